@@ -1,0 +1,337 @@
+"""Throughput benchmark of the IQM metric path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--metric fsim|ssim|flip|msvd]
+                    [--impl ours|reference] [--pairs B] [--no-cpu-baseline]
+
+One step = one pass of the metric over a batch of B synthetic 1080p pairs already resident in
+HBM (distinct buffers; the batch is larger than the 126 MB L2, so no flush is needed between
+steps).  `value` is pairs/s over all ranks; `e2e` is the same metric through the host API
+(pinned host images copied in and scores copied out inside the timed region).  With --impl
+reference the CPU restatement of the reference's arithmetic (oracle/, all host threads) is timed
+on the same workload instead.  Under torchrun each rank evaluates its own batch (independent
+pairs, no collective on the data path): weak scaling.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W1080, H1080 = 1920, 1080
+
+# metric -> (workload name, synthetic generator name, score count per pair)
+WORKLOADS = {
+    "fsim": ("fsim_1080p_rgb", "rgb_gain_pair", 2),
+    "ssim": ("ssim_1080p_grey", "grey_pair", 1),
+    "flip": ("flip_1080p_rgb_67ppd", "rgb_blockquant_pair", 1),
+    "msvd": ("msvd_1080p_rgb", "rgb_blockquant_pair", 1),
+}
+# kernel whose CUDA-event duration the roofline figure uses, per metric
+DOMINANT = {"ssim": "ssim_kernel", "msvd": "msvd_block_kernel", "flip": "flip_kernel", "fsim": "fsim pipeline"}
+
+
+def metric_name(metric):
+    return "1080p image pairs/sec (%s)" % metric.upper()
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--metric", default=None)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--pairs", type=int, default=32)
+    ap.add_argument("--distinct", type=int, default=4, help="distinct synthetic pairs (replicated to --pairs)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def make_pairs(metric, n):
+    from iqm_b200 import synth
+    gen = getattr(synth, WORKLOADS[metric][1])
+    cfg = {"fsim": 1, "ssim": 0, "flip": 2, "msvd": 2}[metric]
+    return [gen(H1080, W1080, config=cfg, pair=i) for i in range(n)]
+
+
+def metric_implemented(metric, device=0):
+    import iqm_b200
+    try:
+        rt = iqm_b200.Runtime(device)
+    except Exception:
+        return False
+    try:
+        a = np.zeros((64, 64, 4), np.uint8)
+        obj = {"fsim": iqm_b200.FSIM, "ssim": iqm_b200.SSIM, "flip": iqm_b200.FLIP, "msvd": iqm_b200.SVD}[metric](rt)
+        obj.compute_metric(a, a)
+        return True
+    except iqm_b200.IQMError as e:
+        return e.code != iqm_b200.IQM_EUNSUPPORTED
+    finally:
+        rt.close()
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        load = [s for s in sm if mx and s > 0.3 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(metric, pairs, seconds, one_pair_only=False):
+    """Times the oracle's reference-faithful FP32 restatement on all host threads."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle
+    o = Oracle("f32")
+    fn = {"ssim": lambda a, b: o.ssim(a, b), "fsim": lambda a, b: o.fsim(a, b),
+          "flip": lambda a, b: o.flip(a, b, ppd=67.0), "msvd": lambda a, b: o.msvd(a, b)}[metric]
+    done = 0
+    t0 = time.perf_counter()
+    while True:
+        a, b = pairs[done % len(pairs)]
+        fn(a, b)
+        done += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or one_pair_only:
+            break
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": done / el, "unit": "pairs/s", "cores": cores, "kind": "port",
+            "sample": "%d pair(s) of the %s workload (%dx%d), %.1f s, oracle FP32 build, OpenMP" % (
+                done, WORKLOADS[metric][0], W1080, H1080, el)}
+
+
+def run_reference(args, metric, rank, world):
+    """--impl reference: the reference's arithmetic on the host CPU (the oracle port)."""
+    if rank != 0:
+        return
+    pairs = make_pairs(metric, 1)
+    for _ in range(max(0, args.warmup)):
+        cpu_baseline(metric, pairs, 0.0, one_pair_only=True)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        cpu_baseline(metric, pairs, 0.0, one_pair_only=True)
+        times.append(time.perf_counter() - t0)
+    per = float(np.mean(times))
+    value = 1.0 / per
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    line = {"impl": "reference", "metric": metric_name(metric), "value": value,
+            "unit": "pairs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded 1/f^2 noise pairs)",
+            "config": {"workload": WORKLOADS[metric][0], "pairs_per_step": 1, "width": W1080, "height": H1080},
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": "port",
+                             "sample": "1 pair per step, oracle FP32 build (reference arithmetic restated), OpenMP"},
+            "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    metric = args.metric or ("fsim" if metric_implemented("fsim", local) else "ssim")
+    if args.impl == "reference":
+        run_reference(args, metric, rank, world)
+        return
+
+    import torch
+    import iqm_b200
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_note = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    B = args.pairs
+    host_pairs = make_pairs(metric, min(args.distinct, B))
+    rt = iqm_b200.Runtime(local)
+    stream = torch.cuda.Stream()
+    rt.set_stream(stream.cuda_stream)
+    obj = {"fsim": iqm_b200.FSIM, "ssim": iqm_b200.SSIM, "flip": iqm_b200.FLIP, "msvd": iqm_b200.SVD}[metric](rt)
+    nscore = WORKLOADS[metric][2]
+
+    # device-resident batch: B distinct buffers (replicas of the distinct synthetic pairs)
+    img_bytes = H1080 * W1080 * 4
+    with torch.cuda.stream(stream):
+        dev = torch.empty((B, 2, img_bytes), dtype=torch.uint8, device="cuda")
+        for i in range(B):
+            a, b = host_pairs[i % len(host_pairs)]
+            dev[i, 0].copy_(torch.from_numpy(a.reshape(-1)))
+            dev[i, 1].copy_(torch.from_numpy(b.reshape(-1)))
+        d_scores = torch.zeros(B * nscore, dtype=torch.float64, device="cuda")
+    stream.synchronize()
+    base = dev.data_ptr()
+    dev_pairs = [(base + (2 * i) * img_bytes, base + (2 * i + 1) * img_bytes, W1080, H1080, W1080 * 4) for i in range(B)]
+
+    def step():
+        obj.compute_dev(dev_pairs, d_scores.data_ptr())
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    launches_per_step = rt.last_launch_count()
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_per_step = ms / args.steps
+    value = world * B / (ms_per_step / 1e3)
+
+    # roofline of the dominant kernel: algorithmic bytes (each RGBA8 input read once) / duration
+    alg_bytes = B * 2 * img_bytes
+    achieved = alg_bytes / (ms_per_step / 1e3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+            "frac": achieved / hbm_peak, "traffic": None, "kernel": DOMINANT[metric],
+            "peak_source": peak_note, "alg_bytes_per_launch": alg_bytes}
+    tr = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tr):
+        try:
+            roof["traffic"] = json.load(open(tr)).get(metric)
+        except Exception:
+            pass
+
+    # end to end: host API with pinned host images and host scores
+    e2e = None
+    pin = []
+    for i in range(B):
+        a, b = host_pairs[i % len(host_pairs)]
+        pa = torch.from_numpy(a).pin_memory()
+        pb = torch.from_numpy(b).pin_memory()
+        pin.append((pa, pb))
+    import ctypes
+    items = [(pa.data_ptr(), pb.data_ptr(), W1080, H1080, W1080 * 4) for pa, pb in pin]
+    arr = iqm_b200._pairs(items)
+    out = np.empty(B * nscore, np.float64)
+    outp = out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    L = rt.L
+
+    def e2e_step():
+        if metric == "ssim":
+            p = obj.params()
+            rt.check(L.iqm_ssim_batch(rt.h, arr, B, ctypes.byref(p), outp))
+        elif metric == "msvd":
+            rt.check(L.iqm_msvd_batch(rt.h, arr, B, outp))
+        elif metric == "flip":
+            p = iqm_b200.FLIPArguments().c()
+            rt.check(L.iqm_flip_batch(rt.h, arr, B, ctypes.byref(p), outp))
+        else:
+            rt.check(L.iqm_fsim_batch(rt.h, arr, B, obj.precision, obj.energy_mode, outp))
+
+    for _ in range(2):
+        e2e_step()
+    e2e_steps = max(3, args.steps // 4)
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ems], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+    e2e = {"value": world * B / (ems / e2e_steps / 1e3), "unit": "pairs/s",
+           "h2d_bytes_per_step": B * 2 * img_bytes, "d2h_bytes_per_step": B * nscore * 8}
+
+    line = {
+        "metric": metric_name(metric), "value": value, "unit": "pairs/s",
+        "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded 1/f^2 noise pairs, %d distinct replicated to %d device buffers)" % (
+            len(host_pairs), B),
+        "config": {"workload": WORKLOADS[metric][0], "pairs_per_step": B, "width": W1080, "height": H1080,
+                   "precision": "fp32", "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (%.0f MB per step), no flush" % (alg_bytes / 1e6)},
+        "roofline": roof, "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(metric, host_pairs, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    rt.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,141 @@
+/*
+ * iqm_cuda.h -- C ABI of the B200 (sm_100a) image-quality-metric library (libiqm_cuda.so).
+ *
+ * This is the drop-in boundary for cadik/IQM's metric-evaluation path.  The reference exposes one
+ * C++ class per metric, each with
+ *     XResult computeMetric(const VulkanRuntime&, const InputImage&, const InputImage&[, args])
+ * (src/gpu/ssim/ssim.h:25-35, src/gpu/fsim/fsim.h:33-36, src/gpu/flip/flip.h:27-30,
+ *  src/gpu/svd/svd.h:25-28), taking RGBA8 host images (src/input_image.h: tightly packed
+ * width*height*4 bytes, src/main.cpp:37-57) and returning scores and maps by value.
+ * Each entry point below replaces one of those calls; the C++ wrappers in iqm_b200/host keep the
+ * reference's class and result shapes on top of it.
+ *
+ * Conventions
+ *   - Plain C types only; no exceptions cross this boundary.  Every call returns IQM_OK (0) or a
+ *     negative IQM_E* code, and iqm_last_error() describes the last failure on that context.
+ *   - Images are RGBA8, row-major, `row_bytes` apart (>= 4*w); the alpha byte is ignored, as in
+ *     the reference's shaders.  "input" is the distorted image, "ref" the reference image
+ *     (the CLI's --input / --ref, src/args.cpp:38-43).
+ *   - Host entry points (iqm_ssim, iqm_fsim, iqm_flip, iqm_msvd and the *_batch forms) take host
+ *     pointers (pageable or pinned), copy to the device, compute, copy results back and return
+ *     when results are in host memory.
+ *   - *_dev entry points take DEVICE pointers, enqueue on the context's stream and return
+ *     immediately; scores are written to device memory.  They never synchronise the host.
+ *   - A context is not thread-safe (neither is the reference's VulkanRuntime, whose single
+ *     command buffer all metric objects share, src/gpu/base/vulkan_runtime.h:54-61).
+ */
+#ifndef IQM_CUDA_H
+#define IQM_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------------- */
+#define IQM_OK 0
+#define IQM_EINVAL (-1)       /* bad argument: null pointer, size, mismatch, parameter range  */
+#define IQM_ECUDA (-2)        /* a CUDA runtime call failed (text in iqm_last_error)            */
+#define IQM_ENOMEM (-3)       /* device or host allocation failed                               */
+#define IQM_EUNSUPPORTED (-4) /* valid request this build does not implement                    */
+
+typedef struct iqm_ctx iqm_ctx;
+
+typedef enum {
+    IQM_FP32 = 0,  /* plain FP32 arithmetic, FP64 pooling sums                                   */
+    IQM_MIXED = 1  /* reduced-precision storage / tensor-core form where a metric provides one   */
+} iqm_precision;
+
+/* ---- context --------------------------------------------------------------------------- */
+/* Replaces VulkanRuntime() (src/gpu/base/vulkan_runtime.cpp:22-67): binds `device`, creates a
+ * stream and a grow-only device arena reused across calls. */
+int iqm_create(int device, iqm_ctx **out);
+int iqm_destroy(iqm_ctx *ctx);
+/* Text of the last error on `ctx` (or of the last iqm_create failure when ctx is NULL). */
+const char *iqm_last_error(const iqm_ctx *ctx);
+/* Run subsequent work on a caller-owned cudaStream_t (NULL restores the context's own stream). */
+int iqm_set_stream(iqm_ctx *ctx, void *cuda_stream);
+int iqm_synchronize(iqm_ctx *ctx);
+/* Device name as the reference prints it with -v ("Selected device: ...", src/main.cpp:80). */
+int iqm_device_name(iqm_ctx *ctx, char *buf, size_t len);
+
+/* ---- SSIM (src/gpu/ssim/ssim.h:25-35, src/gpu/ssim/ssim.cpp:71-243,386-401) ------------- */
+typedef struct {
+    int kernel_size; /* Gaussian window side; radius (kernel_size-1)/2 in [1, 7]; default 11   */
+    float k1;        /* default 0.01 */
+    float k2;        /* default 0.03 */
+    float sigma;     /* default 1.5  */
+} iqm_ssim_params;
+void iqm_ssim_default_params(iqm_ssim_params *p);
+
+/* MSSIM of one pair; `map_out` (nullable, w*h floats) receives the SSIM map
+ * (SSIMResult::imageData, src/gpu/ssim/ssim.h:17-23).  `mssim` must not be NULL. */
+int iqm_ssim(iqm_ctx *ctx, const uint8_t *rgba_in, const uint8_t *rgba_ref, int w, int h,
+             size_t row_bytes, const iqm_ssim_params *params, float *map_out, double *mssim);
+
+/* ---- M-SVD (src/gpu/svd/svd.h:25-28, src/gpu/svd/svd.cpp:39-164) ----------------------- */
+/* `block_map` (nullable, (w/8)*(h/8) floats) receives D/max(D) (SVDResult::imageData). */
+int iqm_msvd(iqm_ctx *ctx, const uint8_t *rgba_in, const uint8_t *rgba_ref, int w, int h,
+             size_t row_bytes, float *block_map, double *msvd);
+
+/* ---- FLIP (src/gpu/flip/flip.h:21-30, src/gpu/flip/flip.cpp:121-172) -------------------- */
+typedef struct {
+    float monitor_resolution_x; /* default 2560 (FLIP_RES)      */
+    float monitor_distance;     /* default 0.7  (FLIP_DISTANCE) */
+    float monitor_width;        /* default 0.6  (FLIP_WIDTH)    */
+} iqm_flip_params;
+void iqm_flip_default_params(iqm_flip_params *p);
+/* pixels per degree exactly as src/gpu/flip/flip.cpp:125 computes it */
+double iqm_flip_ppd(const iqm_flip_params *p);
+/* Mean of the per-pixel FLIP value (shaders/flip/combine_error_maps.glsl:28).  The reference
+ * computes that map but never pools it (FLIPResult::mean_flip is never set); `err_map`
+ * (nullable, w*h floats) receives the map itself. */
+int iqm_flip(iqm_ctx *ctx, const uint8_t *rgba_in, const uint8_t *rgba_ref, int w, int h,
+             size_t row_bytes, const iqm_flip_params *params, float *err_map, double *mean_flip);
+
+/* ---- FSIM / FSIMc (src/gpu/fsim/fsim.h:27-36, src/gpu/fsim/fsim.cpp:80-163) ------------- */
+/* energy_mode selects how the noise-energy estimates are pooled:
+ *   0 = as the reference (only the first ceil(N/2) pixels contribute, the rest read as 0);
+ *   1 = over all N pixels. */
+int iqm_fsim(iqm_ctx *ctx, const uint8_t *rgba_in, const uint8_t *rgba_ref, int w, int h,
+             size_t row_bytes, iqm_precision precision, int energy_mode, double *fsim,
+             double *fsimc);
+
+/* ---- batches: many pairs (uneven sizes allowed) in one launch sequence -------------------- */
+typedef struct {
+    const uint8_t *input; /* RGBA8 distorted image */
+    const uint8_t *ref;   /* RGBA8 reference image */
+    int w, h;
+    size_t row_bytes;
+} iqm_pair;
+
+/* Device-resident forms: `pairs` is a HOST array of n descriptors whose pointers are DEVICE
+ * pointers; scores go to DEVICE memory (`d_scores`, n doubles; FSIM writes 2n: fsim then fsimc
+ * per pair).  Enqueued on the context stream; no host synchronisation. */
+int iqm_ssim_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_ssim_params *params,
+                 double *d_scores);
+int iqm_msvd_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, double *d_scores);
+int iqm_flip_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_flip_params *params,
+                 double *d_scores);
+int iqm_fsim_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, iqm_precision precision,
+                 int energy_mode, double *d_scores);
+
+/* Host forms of the same: HOST image pointers and HOST score arrays; synchronous. */
+int iqm_ssim_batch(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_ssim_params *params,
+                   double *scores);
+int iqm_msvd_batch(iqm_ctx *ctx, const iqm_pair *pairs, int n, double *scores);
+int iqm_flip_batch(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_flip_params *params,
+                   double *scores);
+int iqm_fsim_batch(iqm_ctx *ctx, const iqm_pair *pairs, int n, iqm_precision precision,
+                   int energy_mode, double *scores);
+
+/* Number of kernel launches the last *_dev / host call enqueued on this context (for the
+ * benchmark's launch accounting). */
+int iqm_last_launch_count(const iqm_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IQM_CUDA_H */

@@ -1,0 +1,190 @@
+// Internal declarations shared by the library's translation units (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "iqm_cuda.h"
+
+namespace iqm {
+
+// Failure carried from deep inside an entry point to its C-ABI wrapper.
+struct Error {
+    int code;
+    std::string msg;
+};
+
+#define IQM_CHECK_CUDA(expr)                                                              \
+    do {                                                                                  \
+        cudaError_t e_ = (expr);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            throw ::iqm::Error{IQM_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+
+#define IQM_REQUIRE(cond, text)                                   \
+    do {                                                          \
+        if (!(cond)) throw ::iqm::Error{IQM_EINVAL, (text)};      \
+    } while (0)
+
+// Grow-only device buffer: reused across calls, reallocated (after a stream sync) only when a
+// request exceeds its capacity.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t cap = 0;
+    void *get(size_t bytes, cudaStream_t s) {
+        if (bytes <= cap) return ptr;
+        if (ptr) {
+            IQM_CHECK_CUDA(cudaStreamSynchronize(s));
+            cudaFree(ptr);
+            ptr = nullptr;
+            cap = 0;
+        }
+        size_t want = bytes < 4096 ? 4096 : bytes;
+        want = (want + 255) & ~size_t(255);
+        if (cudaMalloc(&ptr, want) != cudaSuccess) {
+            cudaGetLastError();
+            throw Error{IQM_ENOMEM, "device allocation of " + std::to_string(want) + " bytes failed"};
+        }
+        cap = want;
+        return ptr;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        cap = 0;
+    }
+};
+
+// Pinned host staging buffer (grow-only), for small descriptor uploads and score readback.
+struct PinnedBuf {
+    void *ptr = nullptr;
+    size_t cap = 0;
+    void *get(size_t bytes, cudaStream_t s) {
+        if (bytes <= cap) return ptr;
+        if (ptr) {
+            IQM_CHECK_CUDA(cudaStreamSynchronize(s));
+            cudaFreeHost(ptr);
+            ptr = nullptr;
+            cap = 0;
+        }
+        size_t want = bytes < 4096 ? 4096 : bytes;
+        if (cudaMallocHost(&ptr, want) != cudaSuccess) {
+            cudaGetLastError();
+            throw Error{IQM_ENOMEM, "pinned host allocation failed"};
+        }
+        cap = want;
+        return ptr;
+    }
+    void release() {
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        cap = 0;
+    }
+};
+
+// Small host->device uploads (descriptors, parameters) through a ring of pinned slots.  Each slot
+// is reused only after the event recorded behind its copy has completed, so callers never block
+// on the stream and never overwrite bytes a pending copy still reads.
+struct UploadRing {
+    static constexpr int SLOTS = 8;
+    void *host[SLOTS] = {};
+    size_t cap[SLOTS] = {};
+    cudaEvent_t ev[SLOTS] = {};
+    int next = 0;
+    void release() {
+        for (int i = 0; i < SLOTS; i++) {
+            if (ev[i]) cudaEventDestroy(ev[i]);
+            if (host[i]) cudaFreeHost(host[i]);
+            ev[i] = nullptr;
+            host[i] = nullptr;
+            cap[i] = 0;
+        }
+    }
+};
+
+struct FsimPlan;  // per plane-size FSIM constants (fsim.cu)
+struct FftPlan;   // per-length FFT tables (fft.cu)
+
+}  // namespace iqm
+
+struct iqm_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    int launches = 0;  // kernel launches enqueued by the last entry point
+
+    // named scratch areas (each grow-only)
+    iqm::DevBuf desc;      // per-call pair descriptors
+    iqm::DevBuf scratch;   // per-call kernel scratch (partials, counters, planes)
+    iqm::DevBuf images;    // device copies of host images (host entry points)
+    iqm::DevBuf maps;      // device map outputs (host entry points)
+    iqm::DevBuf scores;    // device scores (host entry points)
+    iqm::PinnedBuf pinned; // staging
+    iqm::UploadRing ring;  // small async uploads
+
+    std::map<std::pair<int, int>, iqm::FsimPlan *> fsim_plans;  // owned; freed by iqm_release_fsim_plans
+    std::map<int, iqm::FftPlan *> fft_plans;  // owned; freed by iqm_release_fft_plans
+};
+
+namespace iqm {
+
+// Run `fn` and convert any failure into a status code recorded on the context.
+template <class F>
+int guarded(iqm_ctx *ctx, F &&fn) {
+    if (!ctx) return IQM_EINVAL;
+    try {
+        ctx->launches = 0;
+        IQM_CHECK_CUDA(cudaSetDevice(ctx->device));
+        fn();
+        ctx->last_error.clear();
+        return IQM_OK;
+    } catch (const Error &e) {
+        ctx->last_error = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        ctx->last_error = "host allocation failed";
+        return IQM_ENOMEM;
+    } catch (const std::exception &e) {
+        ctx->last_error = e.what();
+        return IQM_EINVAL;
+    }
+}
+
+inline void check_launch(iqm_ctx *ctx, const char *what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw Error{IQM_ECUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+    ctx->launches++;
+}
+
+// Validate a batch of pair descriptors.
+inline void check_pairs(const iqm_pair *pairs, int n, int min_w, int min_h) {
+    IQM_REQUIRE(pairs != nullptr, "pairs is NULL");
+    IQM_REQUIRE(n >= 1, "pair count must be >= 1");
+    for (int i = 0; i < n; i++) {
+        const iqm_pair &p = pairs[i];
+        IQM_REQUIRE(p.input && p.ref, "pair " + std::to_string(i) + ": image pointer is NULL");
+        IQM_REQUIRE(p.w >= min_w && p.h >= min_h,
+                    "pair " + std::to_string(i) + ": image too small (" + std::to_string(p.w) + "x" +
+                        std::to_string(p.h) + ")");
+        IQM_REQUIRE(p.w <= 65536 && p.h <= 65536, "pair " + std::to_string(i) + ": image too large");
+        IQM_REQUIRE(p.row_bytes >= size_t(p.w) * 4, "pair " + std::to_string(i) + ": row_bytes < 4*w");
+    }
+}
+
+// Copies `bytes` from host memory to `dst` (grown as needed) on the context stream, staging
+// through the pinned ring; returns the device pointer.
+void *upload_bytes(iqm_ctx *ctx, DevBuf &dst, const void *src, size_t bytes);
+
+// Copies host pairs to device memory (inside ctx->images) and rewrites the pointers.
+std::vector<iqm_pair> upload_pairs(iqm_ctx *ctx, const iqm_pair *pairs, int n);
+
+inline unsigned ceil_div(long a, long b) { return unsigned((a + b - 1) / b); }
+
+}  // namespace iqm
