@@ -1,0 +1,306 @@
+// M-SVD on sm_100a.
+//
+// Reference path (cadik/IQM, src/gpu/svd/svd.cpp:39-164): on the host, OpenCV grey conversion
+// (cv::cvtColor RGB2GRAY, uint8) and cv::SVD(NO_UV) of every 8x8 block of both images, for blocks
+// with x+8 < W and y+8 < H only; on the GPU, the per-block distance D = sqrt(sum_k (s_k - r_k)^2)
+// (shaders/svd/svd.glsl:24-54); on the host again a sort, the median D[n/2] and
+// msvd = sum |D - median| / n with n = (W/8)*(H/8) (skipped slots count as D = 0).
+//
+// Here everything runs on the device in two kernels:
+//   msvd_block_kernel  one thread per block slot: 8 rows x 8 RGBA8 pixels of both images straight
+//                      into registers (two 16-byte loads per row and image, coalesced across a
+//                      warp of horizontally adjacent blocks), OpenCV's 15-bit fixed-point grey,
+//                      one-sided Jacobi SVD in registers (FP32 rotations, FP64 column norms and
+//                      inner products driving the convergence test), D in FP32 as the shader does;
+//   msvd_pool_kernel   one CTA per pair: exact median by radix select (select.cuh), then the mean
+//                      absolute deviation summed in FP64, and the optional D/max(D) map.
+#include <cfloat>
+#include <cmath>
+
+#include "iqm_internal.cuh"
+#include "select.cuh"
+
+namespace {
+
+constexpr int BLOCK_THREADS = 128;
+constexpr int POOL_THREADS = 1024;
+
+struct MsvdPairDev {
+    const uint8_t *a;
+    const uint8_t *b;
+    float *map;          // nullable, bw*bh
+    long long pitch;
+    int w, h;
+    int bw, bh;          // W/8, H/8 block slots
+    int vx, vy;          // computed blocks per row / column (x+8 < W, y+8 < H)
+    int slot_base;       // first global slot of this pair
+    int vec_ok;
+};
+
+struct MsvdArgs {
+    const MsvdPairDev *pairs;
+    int npairs;
+    int total_slots;
+    float *dist;         // total_slots
+    double *scores;      // npairs
+};
+
+__device__ __forceinline__ float gray_u8(uint32_t px) {
+    // cv::cvtColor(COLOR_RGB2GRAY) on 8-bit data: (R*9798 + G*19235 + B*3735 + 2^14) >> 15
+    const uint32_t r = px & 0xffu, g = (px >> 8) & 0xffu, b = (px >> 16) & 0xffu;
+    return float((r * 9798u + g * 19235u + b * 3735u + 16384u) >> 15);
+}
+
+__device__ __forceinline__ int find_pair(const MsvdPairDev *p, int n, int slot) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (p[mid].slot_base <= slot) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Loads one 8x8 grey block (column-major in registers: c[col][row]).
+__device__ __forceinline__ void load_block(const uint8_t *img, long long pitch, int x, int y, bool vec,
+                                           float c[8][8]) {
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        const uint8_t *row = img + (long long)(y + r) * pitch + 4LL * x;
+        uint32_t px[8];
+        if (vec) {
+            const uint4 lo = __ldg(reinterpret_cast<const uint4 *>(row));
+            const uint4 hi = __ldg(reinterpret_cast<const uint4 *>(row) + 1);
+            px[0] = lo.x; px[1] = lo.y; px[2] = lo.z; px[3] = lo.w;
+            px[4] = hi.x; px[5] = hi.y; px[6] = hi.z; px[7] = hi.w;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 8; q++) px[q] = __ldg(reinterpret_cast<const uint32_t *>(row) + q);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) c[q][r] = gray_u8(px[q]);
+    }
+}
+
+// Singular values (descending) of the 8x8 matrix whose columns are c[0..7]; c is destroyed.
+// One-sided Jacobi: each (i, j) column pair is rotated so the columns become orthogonal; the
+// rotation is applied in FP32, the inner product and the squared norms are accumulated in FP64
+// and a pair is skipped once |<ci,cj>| <= eps * |ci| |cj| (compared squared, eps = FLT_EPSILON).
+__device__ __forceinline__ void svd8_values(float c[8][8], float s[8]) {
+    double nrm[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        double q = 0.0;
+#pragma unroll
+        for (int r = 0; r < 8; r++) q = fma(double(c[i][r]), double(c[i][r]), q);
+        nrm[i] = q;
+    }
+    const double eps2 = double(FLT_EPSILON) * double(FLT_EPSILON);
+    for (int sweep = 0; sweep < 60; sweep++) {
+        bool changed = false;
+#pragma unroll
+        for (int i = 0; i < 7; i++) {
+#pragma unroll
+            for (int j = i + 1; j < 8; j++) {
+                double p = 0.0;
+#pragma unroll
+                for (int r = 0; r < 8; r++) p = fma(double(c[i][r]), double(c[j][r]), p);
+                if (p * p > eps2 * nrm[i] * nrm[j]) {
+                    // rotation zeroing <ci, cj>: tan(theta) = t, smaller root of t^2 + 2 zeta t - 1 = 0
+                    const float zeta = float((nrm[j] - nrm[i]) / (2.0 * p));
+                    const float t = copysignf(1.0f, zeta) / (fabsf(zeta) + sqrtf(fmaf(zeta, zeta, 1.0f)));
+                    const float cs = rsqrtf(fmaf(t, t, 1.0f));
+                    const float sn = cs * t;
+                    double ni = 0.0, nj = 0.0;
+#pragma unroll
+                    for (int r = 0; r < 8; r++) {
+                        const float xi = c[i][r], xj = c[j][r];
+                        const float yi = fmaf(cs, xi, -sn * xj);
+                        const float yj = fmaf(sn, xi, cs * xj);
+                        c[i][r] = yi;
+                        c[j][r] = yj;
+                        ni = fma(double(yi), double(yi), ni);
+                        nj = fma(double(yj), double(yj), nj);
+                    }
+                    nrm[i] = ni;
+                    nrm[j] = nj;
+                    changed = true;
+                }
+            }
+        }
+        if (!changed) break;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) s[i] = float(sqrt(nrm[i]));
+    // descending order (sorting network on 8 registers)
+#define IQM_CSWAP(a, b)                         \
+    do {                                        \
+        const float hi_ = fmaxf(s[a], s[b]);    \
+        const float lo_ = fminf(s[a], s[b]);    \
+        s[a] = hi_;                             \
+        s[b] = lo_;                             \
+    } while (0)
+    IQM_CSWAP(0, 1); IQM_CSWAP(2, 3); IQM_CSWAP(4, 5); IQM_CSWAP(6, 7);
+    IQM_CSWAP(0, 2); IQM_CSWAP(1, 3); IQM_CSWAP(4, 6); IQM_CSWAP(5, 7);
+    IQM_CSWAP(1, 2); IQM_CSWAP(5, 6); IQM_CSWAP(0, 4); IQM_CSWAP(3, 7);
+    IQM_CSWAP(1, 5); IQM_CSWAP(2, 6);
+    IQM_CSWAP(1, 4); IQM_CSWAP(3, 6);
+    IQM_CSWAP(2, 4); IQM_CSWAP(3, 5);
+    IQM_CSWAP(3, 4);
+#undef IQM_CSWAP
+}
+
+__global__ void __launch_bounds__(BLOCK_THREADS) msvd_block_kernel(MsvdArgs args) {
+    const int slot = blockIdx.x * BLOCK_THREADS + threadIdx.x;
+    if (slot >= args.total_slots) return;
+    const int pi = find_pair(args.pairs, args.npairs, slot);
+    const MsvdPairDev &P = args.pairs[pi];
+    const int local = slot - P.slot_base;
+    const int bx = local % P.bw, by = local / P.bw;
+    float d = 0.0f;  // slots the reference never computes stay 0 (src/gpu/svd/svd.cpp:44,68-74)
+    if (bx < P.vx && by < P.vy) {
+        float c[8][8], si[8], sr[8];
+        load_block(P.a, P.pitch, 8 * bx, 8 * by, P.vec_ok, c);
+        svd8_values(c, si);
+        load_block(P.b, P.pitch, 8 * bx, 8 * by, P.vec_ok, c);
+        svd8_values(c, sr);
+        float acc = 0.0f;  // shaders/svd/svd.glsl:41-52: float, k = 0..7 in order
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const float t = si[k] - sr[k];
+            acc = fmaf(t, t, acc);
+        }
+        d = sqrtf(acc);
+    }
+    args.dist[slot] = d;
+}
+
+__global__ void __launch_bounds__(POOL_THREADS) msvd_pool_kernel(MsvdArgs args) {
+    __shared__ unsigned hist[iqm::SELECT_BINS];
+    __shared__ double red_s[POOL_THREADS / 32];
+    __shared__ float red_m[POOL_THREADS / 32];
+    const MsvdPairDev &P = args.pairs[blockIdx.x];
+    const int n = P.bw * P.bh;
+    const float *D = args.dist + P.slot_base;
+    const float med = iqm::block_select_kth(D, n, n / 2, hist);
+    double s = 0.0;
+    float mx = 0.0f;
+    for (int i = threadIdx.x; i < n; i += POOL_THREADS) {
+        const float v = __ldcg(D + i);
+        s += double(fabsf(v - med));
+        mx = fmaxf(mx, v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        mx = fmaxf(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        red_s[wid] = s;
+        red_m[wid] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        float m = 0.0f;
+        for (int w = 0; w < POOL_THREADS / 32; w++) {
+            t += red_s[w];
+            m = fmaxf(m, red_m[w]);
+        }
+        args.scores[blockIdx.x] = t / double(n);
+        red_m[0] = m;
+    }
+    __syncthreads();
+    if (P.map) {
+        const float m = red_m[0];
+        for (int i = threadIdx.x; i < n; i += POOL_THREADS) P.map[i] = __ldcg(D + i) / m;
+    }
+}
+
+void msvd_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const std::vector<float *> &maps,
+                  double *d_scores) {
+    const int n = int(pairs.size());
+    std::vector<MsvdPairDev> hd(n);
+    long total = 0;
+    for (int i = 0; i < n; i++) {
+        const iqm_pair &q = pairs[i];
+        MsvdPairDev &d = hd[i];
+        d.a = q.input;
+        d.b = q.ref;
+        d.map = maps.empty() ? nullptr : maps[i];
+        d.pitch = (long long)q.row_bytes;
+        d.w = q.w;
+        d.h = q.h;
+        d.bw = q.w / 8;
+        d.bh = q.h / 8;
+        d.vx = q.w >= 9 ? (q.w - 1) / 8 : 0;  // x = 8*bx with x + 8 < W
+        d.vy = q.h >= 9 ? (q.h - 1) / 8 : 0;
+        d.slot_base = int(total);
+        d.vec_ok = ((reinterpret_cast<uintptr_t>(q.input) | reinterpret_cast<uintptr_t>(q.ref) |
+                     uintptr_t(q.row_bytes)) & 15u) == 0;
+        total += long(d.bw) * d.bh;
+    }
+    IQM_REQUIRE(total < (1L << 31), "too many blocks in one batch");
+    auto *d_desc = static_cast<MsvdPairDev *>(iqm::upload_bytes(ctx, ctx->desc, hd.data(), sizeof(MsvdPairDev) * n));
+    MsvdArgs a{};
+    a.pairs = d_desc;
+    a.npairs = n;
+    a.total_slots = int(total);
+    a.dist = static_cast<float *>(ctx->scratch.get(sizeof(float) * size_t(total), ctx->stream));
+    a.scores = d_scores;
+    msvd_block_kernel<<<iqm::ceil_div(total, BLOCK_THREADS), BLOCK_THREADS, 0, ctx->stream>>>(a);
+    iqm::check_launch(ctx, "msvd_block_kernel");
+    msvd_pool_kernel<<<n, POOL_THREADS, 0, ctx->stream>>>(a);
+    iqm::check_launch(ctx, "msvd_pool_kernel");
+}
+
+}  // namespace
+
+// The reference needs at least one 8x8 block slot: n = (W/8)*(H/8) > 0 (it divides by n).
+static void check_msvd_pairs(const iqm_pair *pairs, int n) { iqm::check_pairs(pairs, n, 8, 8); }
+
+extern "C" __attribute__((visibility("default"))) int iqm_msvd_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n,
+                                                                  double *d_scores) {
+    return iqm::guarded(ctx, [&] {
+        check_msvd_pairs(pairs, n);
+        IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
+        msvd_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), {}, d_scores);
+    });
+}
+
+extern "C" __attribute__((visibility("default"))) int iqm_msvd_batch(iqm_ctx *ctx, const iqm_pair *pairs, int n,
+                                                                    double *scores) {
+    return iqm::guarded(ctx, [&] {
+        check_msvd_pairs(pairs, n);
+        IQM_REQUIRE(scores != nullptr, "scores is NULL");
+        auto dev = iqm::upload_pairs(ctx, pairs, n);
+        auto *d_scores = static_cast<double *>(ctx->scores.get(sizeof(double) * n, ctx->stream));
+        msvd_enqueue(ctx, dev, {}, d_scores);
+        IQM_CHECK_CUDA(cudaMemcpyAsync(scores, d_scores, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        IQM_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+extern "C" __attribute__((visibility("default"))) int iqm_msvd(iqm_ctx *ctx, const uint8_t *rgba_in,
+                                                              const uint8_t *rgba_ref, int w, int h,
+                                                              size_t row_bytes, float *block_map, double *msvd) {
+    return iqm::guarded(ctx, [&] {
+        IQM_REQUIRE(msvd != nullptr, "msvd is NULL");
+        iqm_pair hp{rgba_in, rgba_ref, w, h, row_bytes};
+        check_msvd_pairs(&hp, 1);
+        auto dev = iqm::upload_pairs(ctx, &hp, 1);
+        auto *d_score = static_cast<double *>(ctx->scores.get(sizeof(double), ctx->stream));
+        const size_t nb = size_t(w / 8) * size_t(h / 8);
+        std::vector<float *> maps;
+        float *d_map = nullptr;
+        if (block_map) {
+            d_map = static_cast<float *>(ctx->maps.get(sizeof(float) * nb, ctx->stream));
+            maps.push_back(d_map);
+        }
+        msvd_enqueue(ctx, dev, maps, d_score);
+        IQM_CHECK_CUDA(cudaMemcpyAsync(msvd, d_score, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        if (block_map)
+            IQM_CHECK_CUDA(cudaMemcpyAsync(block_map, d_map, sizeof(float) * nb, cudaMemcpyDeviceToHost, ctx->stream));
+        IQM_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}

@@ -15,18 +15,13 @@ extern "C" __attribute__((visibility("default"))) void iqm_flip_default_params(i
     p->monitor_width = 0.6f;
 }
 extern "C" __attribute__((visibility("default"))) double iqm_flip_ppd(const iqm_flip_params *p) { return 0; }
-extern "C" __attribute__((visibility("default"))) int iqm_msvd(iqm_ctx *ctx, const uint8_t *, const uint8_t *, int, int, size_t, float *, double *) {
-    return iqm::guarded(ctx, [&] { IQM_PENDING("iqm_msvd"); });
-}
 extern "C" __attribute__((visibility("default"))) int iqm_flip(iqm_ctx *ctx, const uint8_t *, const uint8_t *, int, int, size_t, const iqm_flip_params *, float *, double *) {
     return iqm::guarded(ctx, [&] { IQM_PENDING("iqm_flip"); });
 }
 extern "C" __attribute__((visibility("default"))) int iqm_fsim(iqm_ctx *ctx, const uint8_t *, const uint8_t *, int, int, size_t, iqm_precision, int, double *, double *) {
     return iqm::guarded(ctx, [&] { IQM_PENDING("iqm_fsim"); });
 }
-extern "C" __attribute__((visibility("default"))) int iqm_msvd_dev(iqm_ctx *ctx, const iqm_pair *, int, double *) { return iqm::guarded(ctx, [&] { IQM_PENDING("iqm_msvd_dev"); }); }
 extern "C" __attribute__((visibility("default"))) int iqm_flip_dev(iqm_ctx *ctx, const iqm_pair *, int, const iqm_flip_params *, double *) { return iqm::guarded(ctx, [&] { IQM_PENDING("iqm_flip_dev"); }); }
 extern "C" __attribute__((visibility("default"))) int iqm_fsim_dev(iqm_ctx *ctx, const iqm_pair *, int, iqm_precision, int, double *) { return iqm::guarded(ctx, [&] { IQM_PENDING("iqm_fsim_dev"); }); }
-extern "C" __attribute__((visibility("default"))) int iqm_msvd_batch(iqm_ctx *ctx, const iqm_pair *, int, double *) { return iqm::guarded(ctx, [&] { IQM_PENDING("iqm_msvd_batch"); }); }
 extern "C" __attribute__((visibility("default"))) int iqm_flip_batch(iqm_ctx *ctx, const iqm_pair *, int, const iqm_flip_params *, double *) { return iqm::guarded(ctx, [&] { IQM_PENDING("iqm_flip_batch"); }); }
 extern "C" __attribute__((visibility("default"))) int iqm_fsim_batch(iqm_ctx *ctx, const iqm_pair *, int, iqm_precision, int, double *) { return iqm::guarded(ctx, [&] { IQM_PENDING("iqm_fsim_batch"); }); }
