@@ -15,8 +15,12 @@
 //     cov_ab = (var_u - var_v)/4, var_a + var_b = (var_u + var_v)/2;
 //   * the second moments are taken about a per-tile constant (the u, v of the tile's centre
 //     pixel), var = E[(x-c)^2] - E[x-c]^2, which keeps FP32 cancellation ~1e-7 on MSSIM;
-//   * horizontal taps are read from a shared-memory tile (128 output columns + halo, one CTA),
-//     vertical taps live in a register ring of 2R+1 rows: each thread slides down its two columns;
+//   * each CTA owns a 128-column strip of ~120 output rows and streams down it: raw RGBA8 rows
+//     (plus a 5-pixel halo) are prefetched PF rows ahead with cp.async into a small shared ring,
+//     converted once to shifted (u, v), filtered horizontally from shared memory and pushed into a
+//     register ring of 2R+1 rows that carries the vertical taps (one barrier per row, ~11 KB of
+//     shared memory per CTA, so many CTAs overlap their loads with arithmetic);
+//   * (u, v) pairs are processed with packed FP32x2 instructions (__ffma2_rn and friends);
 //   * MSSIM partials go to per-tile FP64 slots; the last CTA of a pair sums them in a fixed order
 //     (deterministic, no second launch).
 #include <cmath>
@@ -26,17 +30,23 @@
 
 namespace {
 
-constexpr int TW = 128;          // output columns per CTA
-constexpr int NT = 64;           // threads per CTA; each owns 2 adjacent columns
-constexpr int SMEM_COLS = TW + 16;  // tile columns x0-8 .. x0+TW+7 (16-byte aligned start)
+constexpr int TW = 128;             // output columns per CTA (one vertical strip)
+constexpr int NT = 64;              // threads per CTA; each owns 2 adjacent columns
+constexpr int SMEM_COLS = TW + 16;  // staged columns x0-8 .. x0+TW+7 (16-byte aligned start)
+constexpr int NRAW = 8;             // raw RGBA row ring
+constexpr int PF = 6;               // rows prefetched ahead (< NRAW)
 
 template <int R>
 struct Geom {
     static constexpr int K = 2 * R + 1;
     // strip height: S + 2R is a multiple of K so the register ring indexes statically
-    static constexpr int S = K * ((32 + 2 * R + K - 1) / K) - 2 * R;
+    static constexpr int S = K * ((120 + 2 * R + K - 1) / K) - 2 * R;
     static constexpr int ROWS = S + 2 * R;
-    static constexpr size_t SMEM = size_t(ROWS) * SMEM_COLS * sizeof(float2);
+};
+
+struct Smem {
+    uint32_t raw[NRAW][2][SMEM_COLS];  // RGBA8 rows of both images, as loaded
+    float2 uv[2][SMEM_COLS];           // shifted (u, v) of the row being filtered
 };
 
 struct SsimPairDev {
@@ -78,12 +88,65 @@ __device__ __forceinline__ int find_pair(const SsimPairDev *pairs, int n, int ti
     return lo;
 }
 
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int src_bytes) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Issue the copies of image row y (both images, staged columns) into raw ring slot `slot`.
+// Columns or rows outside the image are not fetched: the conversion step zeroes them.
+__device__ __forceinline__ void issue_row(Smem &sm, const SsimPairDev &P, int x0, int y, int slot) {
+    if (y < 0 || y >= P.h) return;
+    const int xs = x0 - 8;
+    if (P.vec_ok) {
+        constexpr int CH = SMEM_COLS / 4;  // 16-byte chunks per image row
+        for (int c = threadIdx.x; c < 2 * CH; c += NT) {
+            const int img = c / CH, q = c - img * CH;
+            const int x = xs + 4 * q;
+            if (x < 0 || x >= P.w) continue;
+            const int valid = min(4, P.w - x);
+            const uint8_t *src = (img ? P.b : P.a) + (long long)y * P.pitch + 4LL * x;
+            cp_async16(&sm.raw[slot][img][4 * q], src, 4 * valid);
+        }
+    } else {
+        for (int c = threadIdx.x; c < 2 * SMEM_COLS; c += NT) {
+            const int img = c / SMEM_COLS, q = c - img * SMEM_COLS;
+            const int x = xs + q;
+            if (x < 0 || x >= P.w) continue;
+            const uint8_t *src = (img ? P.b : P.a) + (long long)y * P.pitch + 4LL * x;
+            cp_async4(&sm.raw[slot][img][q], src);
+        }
+    }
+}
+
+// Raw RGBA row -> shifted (u, v) row; positions outside the image become (0, 0), which removes
+// them from every window sum (the reference skips out-of-image taps).
+__device__ __forceinline__ void convert_row(Smem &sm, const SsimPairDev &P, int x0, int y, int slot,
+                                            float2 *dst, float cu, float cv) {
+    const bool row_ok = y >= 0 && y < P.h;
+    for (int q = threadIdx.x; q < SMEM_COLS; q += NT) {
+        const int x = x0 - 8 + q;
+        float2 o = make_float2(0.f, 0.f);
+        if (row_ok && x >= 0 && x < P.w) {
+            const float la = luma_u8(sm.raw[slot][0][q]), lb = luma_u8(sm.raw[slot][1][q]);
+            o = make_float2((la + lb) - cu, (la - lb) - cv);
+        }
+        dst[q] = o;
+    }
+}
+
 template <int R>
-__global__ void __launch_bounds__(NT, 4) ssim_kernel(SsimArgs args) {
+__global__ void __launch_bounds__(NT, 8) ssim_kernel(SsimArgs args) {
     using G = Geom<R>;
     constexpr int K = G::K, S = G::S, ROWS = G::ROWS;
-    extern __shared__ float4 smem_raw[];
-    float2 *tile = reinterpret_cast<float2 *>(smem_raw);
+    __shared__ __align__(16) Smem sm;
     __shared__ double red[NT / 32];
     __shared__ int is_last;
 
@@ -96,162 +159,133 @@ __global__ void __launch_bounds__(NT, 4) ssim_kernel(SsimArgs args) {
     const int W = P.w, H = P.h;
     const int tid = threadIdx.x;
 
-    // per-tile shift constants: u, v of the tile's centre pixel
+    // prefetch the first PF rows (tile row r = image row y0 - R + r)
+#pragma unroll
+    for (int r = 0; r < PF; r++) {
+        issue_row(sm, P, x0, y0 - R + r, r % NRAW);
+        cp_async_commit();
+    }
+
+    // per-tile shift constants: u, v of the tile's centre pixel (keeps FP32 cancellation small)
     float cu, cv;
     {
-        int cx = min(x0 + TW / 2, W - 1), cy = min(y0 + S / 2, H - 1);
-        uint32_t pa = __ldg(reinterpret_cast<const uint32_t *>(P.a + (long long)cy * P.pitch) + cx);
-        uint32_t pb = __ldg(reinterpret_cast<const uint32_t *>(P.b + (long long)cy * P.pitch) + cx);
-        float la = luma_u8(pa), lb = luma_u8(pb);
+        const int cx = min(x0 + TW / 2, W - 1), cy = min(y0 + S / 2, H - 1);
+        const uint32_t pa = __ldg(reinterpret_cast<const uint32_t *>(P.a + (long long)cy * P.pitch) + cx);
+        const uint32_t pb = __ldg(reinterpret_cast<const uint32_t *>(P.b + (long long)cy * P.pitch) + cx);
+        const float la = luma_u8(pa), lb = luma_u8(pb);
         cu = la + lb;
         cv = la - lb;
     }
 
-    // ---- stage RGBA8 -> shifted (u, v) for rows y0-R .. y0+S+R-1, columns x0-8 .. x0+TW+7 ----
-    {
-        constexpr int GROUPS = SMEM_COLS / 4;  // 4-pixel groups per row
-        const int xs = x0 - 8;
-        for (int idx = tid; idx < ROWS * GROUPS; idx += NT) {
-            const int r = idx / GROUPS, gq = idx - r * GROUPS;
-            const int y = y0 - R + r, x = xs + 4 * gq;
-            float2 out[4];
-            if (y < 0 || y >= H || x >= W || x + 3 < 0) {
-#pragma unroll
-                for (int q = 0; q < 4; q++) out[q] = make_float2(0.f, 0.f);
-            } else {
-                const uint8_t *ra = P.a + (long long)y * P.pitch;
-                const uint8_t *rb = P.b + (long long)y * P.pitch;
-                uint32_t pa[4], pb[4];
-                if (P.vec_ok && x >= 0 && x + 3 < W) {
-                    uint4 va = __ldg(reinterpret_cast<const uint4 *>(ra) + (x >> 2));
-                    uint4 vb = __ldg(reinterpret_cast<const uint4 *>(rb) + (x >> 2));
-                    pa[0] = va.x; pa[1] = va.y; pa[2] = va.z; pa[3] = va.w;
-                    pb[0] = vb.x; pb[1] = vb.y; pb[2] = vb.z; pb[3] = vb.w;
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        int xx = x + q;
-                        bool ok = xx >= 0 && xx < W;
-                        pa[q] = ok ? __ldg(reinterpret_cast<const uint32_t *>(ra) + xx) : 0u;
-                        pb[q] = ok ? __ldg(reinterpret_cast<const uint32_t *>(rb) + xx) : 0u;
-                    }
-                }
-#pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    int xx = x + q;
-                    if (xx >= 0 && xx < W) {
-                        float la = luma_u8(pa[q]), lb = luma_u8(pb[q]);
-                        out[q] = make_float2((la + lb) - cu, (la - lb) - cv);
-                    } else {
-                        out[q] = make_float2(0.f, 0.f);
-                    }
-                }
-            }
-            float4 *dst = reinterpret_cast<float4 *>(tile + r * SMEM_COLS + 4 * gq);
-            dst[0] = make_float4(out[0].x, out[0].y, out[1].x, out[1].y);
-            dst[1] = make_float4(out[2].x, out[2].y, out[3].x, out[3].y);
-        }
-    }
+    cp_async_wait<PF - 1>();
     __syncthreads();
+    convert_row(sm, P, x0, y0 - R, 0, sm.uv[0], cu, cv);
+    issue_row(sm, P, x0, y0 - R + PF, PF % NRAW);
+    cp_async_commit();
 
-    // ---- sliding separable window ----
-    constexpr int OFF = (8 - R) & 1;        // parity fix so float4 reads stay 16-byte aligned
-    constexpr int NV = (2 * R + 4) / 2;     // float4 reads per row (2R+4 float2 values)
-    const int col0 = 2 * tid;               // first of this thread's two tile columns
-    const int start = col0 + 8 - R - OFF;   // even
+    constexpr int OFF = (8 - R) & 1;     // parity fix so float4 reads stay 16-byte aligned
+    constexpr int NV = (2 * R + 4) / 2;  // float4 reads per row (2R+4 float2 values)
+    const int col0 = 2 * tid;            // first of this thread's two tile columns
+    const int start = col0 + 8 - R - OFF;
     float gsum = 0.f;
 #pragma unroll
     for (int k = 0; k < K; k++) gsum += args.g[k];
-    float wxv[2];
+    float rwx[2];
 #pragma unroll
     for (int c = 0; c < 2; c++) {
         const int x = x0 + col0 + c;
         float s = 0.f;
 #pragma unroll
         for (int k = 0; k < K; k++) {
-            int xx = x + k - R;
+            const int xx = x + k - R;
             s += (xx >= 0 && xx < W) ? args.g[k] : 0.f;
         }
-        wxv[c] = s;
+        rwx[c] = 1.0f / s;
     }
 
-    float ring[2][K][4];
-    float acc = 0.f;  // pooled SSIM of this thread (<= 2*S terms)
-    const int pool_x_lo = R, pool_x_hi = W - R, pool_y_lo = R, pool_y_hi = H - R;
+    float2 ring_m[2][K];  // (sum g u, sum g v) of the last K rows, per column
+    float2 ring_s[2][K];  // (sum g u^2, sum g v^2)
+    float acc = 0.f;      // pooled SSIM of this thread
+    const bool col_in[2] = {x0 + col0 < W, x0 + col0 + 1 < W};
 
     for (int jb = 0; jb < ROWS; jb += K) {
 #pragma unroll
         for (int t = 0; t < K; t++) {
-            const int j = jb + t;  // tile row; image row y0 - R + j
-            // horizontal taps
+            const int j = jb + t;
+            // make row j+1 available: wait for its copies, convert it, prefetch row j+1+PF
+            cp_async_wait<PF - 1>();
+            __syncthreads();
+            if (j + 1 < ROWS) convert_row(sm, P, x0, y0 - R + j + 1, (j + 1) % NRAW, sm.uv[(j + 1) & 1], cu, cv);
+            if (j + 1 + PF < ROWS) issue_row(sm, P, x0, y0 - R + j + 1 + PF, (j + 1 + PF) % NRAW);
+            cp_async_commit();
+
+            // horizontal taps of row j
             float2 v[2 * R + 4];
-            const float4 *src = reinterpret_cast<const float4 *>(tile + j * SMEM_COLS + start);
+            const float4 *src = reinterpret_cast<const float4 *>(sm.uv[j & 1] + start);
 #pragma unroll
             for (int q = 0; q < NV; q++) {
-                float4 f = src[q];
+                const float4 f = src[q];
                 v[2 * q] = make_float2(f.x, f.y);
                 v[2 * q + 1] = make_float2(f.z, f.w);
             }
 #pragma unroll
             for (int c = 0; c < 2; c++) {
-                float hu = 0.f, hv = 0.f, huu = 0.f, hvv = 0.f;
+                float2 hm = make_float2(0.f, 0.f), hs = make_float2(0.f, 0.f);
 #pragma unroll
                 for (int k = 0; k < K; k++) {
-                    const float2 s = v[OFF + c + k];
-                    const float gu = args.g[k] * s.x, gv = args.g[k] * s.y;
-                    hu += gu;
-                    hv += gv;
-                    huu = fmaf(gu, s.x, huu);
-                    hvv = fmaf(gv, s.y, hvv);
+                    const float2 sv = v[OFF + c + k];
+                    const float2 gs = __fmul2_rn(make_float2(args.g[k], args.g[k]), sv);
+                    hm = __fadd2_rn(hm, gs);
+                    hs = __ffma2_rn(gs, sv, hs);
                 }
-                ring[c][t][0] = hu;
-                ring[c][t][1] = hv;
-                ring[c][t][2] = huu;
-                ring[c][t][3] = hvv;
+                ring_m[c][t] = hm;
+                ring_s[c][t] = hs;
             }
             if (j >= 2 * R) {
                 // vertical taps: output row i = j - 2R uses tile rows i .. i + 2R
                 const int y = y0 + j - 2 * R;
                 if (y < H) {
-                    float wy;
-                    if (y >= R && y < H - R) {
-                        wy = gsum;
-                    } else {
+                    float wy = gsum;
+                    if (y < R || y >= H - R) {
                         wy = 0.f;
 #pragma unroll
                         for (int k = 0; k < K; k++) {
-                            int yy = y + k - R;
+                            const int yy = y + k - R;
                             wy += (yy >= 0 && yy < H) ? args.g[k] : 0.f;
                         }
                     }
+                    const float rwy = 1.0f / wy;
+                    const bool pool_y = y >= R && y <= H - R;
 #pragma unroll
                     for (int c = 0; c < 2; c++) {
-                        float m[4] = {0.f, 0.f, 0.f, 0.f};
+                        float2 mm = make_float2(0.f, 0.f), ms = make_float2(0.f, 0.f);
 #pragma unroll
                         for (int k = 0; k < K; k++) {
                             const int slot = (t + 1 + k) % K;
-#pragma unroll
-                            for (int q = 0; q < 4; q++) m[q] = fmaf(args.g[k], ring[c][slot][q], m[q]);
+                            const float2 gk = make_float2(args.g[k], args.g[k]);
+                            mm = __ffma2_rn(gk, ring_m[c][slot], mm);
+                            ms = __ffma2_rn(gk, ring_s[c][slot], ms);
                         }
-                        const int x = x0 + col0 + c;
-                        if (x < W) {
-                            const float inv = 1.0f / (wxv[c] * wy);
-                            const float su = m[0] * inv, sv = m[1] * inv;  // shifted means
-                            const float varu = m[2] * inv - su * su;
-                            const float varv = m[3] * inv - sv * sv;
+                        if (col_in[c]) {
+                            const int x = x0 + col0 + c;
+                            const float inv = rwx[c] * rwy;
+                            const float su = mm.x * inv, sv = mm.y * inv;  // shifted means
+                            const float varu = fmaf(ms.x, inv, -su * su);
+                            const float varv = fmaf(ms.y, inv, -sv * sv);
                             const float mu = su + cu, mv = sv + cv;
                             const float mu2 = mu * mu, mv2 = mv * mv;
                             const float num = (0.5f * (mu2 - mv2) + args.c1) * (0.5f * (varu - varv) + args.c2);
                             const float den = (0.5f * (mu2 + mv2) + args.c1) * (0.5f * (varu + varv) + args.c2);
-                            const float ssim = num / den;
+                            const float ssim = __fdividef(num, den);
                             if (P.map) P.map[(long long)y * W + x] = ssim;
-                            if (x >= pool_x_lo && x <= pool_x_hi && y >= pool_y_lo && y <= pool_y_hi) acc += ssim;
+                            if (pool_y && x >= R && x <= W - R) acc += ssim;
                         }
                     }
                 }
             }
         }
     }
+    cp_async_wait<0>();
 
     // ---- deterministic pooling: CTA partial -> per-tile slot -> last CTA of the pair ----
     double d = double(acc);
@@ -265,7 +299,7 @@ __global__ void __launch_bounds__(NT, 4) ssim_kernel(SsimArgs args) {
         for (int i = 0; i < NT / 32; i++) s += red[i];
         args.partials[gt] = s;
         __threadfence();
-        unsigned prev = atomicAdd(&args.counters[pi], 1u);
+        const unsigned prev = atomicAdd(&args.counters[pi], 1u);
         is_last = (prev == unsigned(P.ntiles - 1));
     }
     __syncthreads();
@@ -290,13 +324,7 @@ __global__ void __launch_bounds__(NT, 4) ssim_kernel(SsimArgs args) {
 
 template <int R>
 void launch_ssim(const SsimArgs &a, int total_tiles, cudaStream_t s) {
-    using G = Geom<R>;
-    static bool attr_set = false;  // per process; the attribute is per device function
-    if (!attr_set) {
-        cudaFuncSetAttribute(ssim_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::SMEM));
-        attr_set = true;
-    }
-    ssim_kernel<R><<<total_tiles, NT, G::SMEM, s>>>(a);
+    ssim_kernel<R><<<total_tiles, NT, 0, s>>>(a);
 }
 
 int strip_rows(int R) {

@@ -1,6 +1,10 @@
 """M-SVD on the GPU through the C ABI.  Pinned against OpenCV (the reference's own library) via
-tests/golden/msvd.npz, and against the FP64 oracle.  Tolerance: relative 1e-5 on the score (the
-reference itself accumulates in float, whose rounding is ~1e-6 relative at 1080p)."""
+tests/golden/msvd.npz, and against the FP64 and FP32 oracle builds.
+
+Tolerance: |delta| <= 1e-5 * max(1, |score|) + 2e-4 / sqrt(n_blocks).  The second term is the
+rounding of FP32 singular values: the reference's cv::SVD runs in float on blocks whose largest
+singular value reaches ~2040 (ulp ~1.2e-4), so two correct FP32 SVDs differ by ~1e-4 in D; the
+score is a mean over n blocks, which averages those differences down by ~sqrt(n)."""
 import os
 
 import numpy as np
@@ -14,8 +18,12 @@ GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 RTOL = 1e-5
 
 
-def close(a, b):
-    return abs(a - b) <= RTOL * max(1.0, abs(b))
+def close(a, b, nblocks=1):
+    return abs(a - b) <= RTOL * max(1.0, abs(b)) + 2e-4 / np.sqrt(max(1, nblocks))
+
+
+def computed_blocks(h, w):
+    return max(0, (w - 1) // 8) * max(0, (h - 1) // 8)
 
 
 def test_msvd_matches_opencv_golden(rt):
@@ -23,7 +31,8 @@ def test_msvd_matches_opencv_golden(rt):
     s = iqm_b200.SVD(rt)
     for i in range(len(d["sizes"])):
         r = s.compute_metric(d["img%d" % i], d["ref%d" % i])
-        assert close(r.msvd, float(d["scores"][i])), (i, r.msvd, d["scores"][i])
+        h, w = d["sizes"][i]
+        assert close(r.msvd, float(d["scores"][i]), computed_blocks(h, w)), (i, r.msvd, d["scores"][i])
         dist = d["dist%d" % i]
         mx = dist.max()
         assert np.allclose(r.image_data, dist / mx, rtol=1e-4, atol=1e-4)
@@ -34,8 +43,9 @@ def test_msvd_matches_oracle(rt, o64, o32, h, w):
     a, b = synth.rgb_blockquant_pair(h, w, config=2, pair=h % 5)
     got = iqm_b200.SVD(rt).compute_metric(a, b).msvd
     want = o64.msvd(a, b)
-    assert close(got, want), (got, want)
-    assert close(got, o32.msvd(a, b))
+    n = computed_blocks(h, w)
+    assert close(got, want, n), (got, want)
+    assert close(got, o32.msvd(a, b), n)
 
 
 def test_msvd_identical_is_zero(rt):
@@ -47,8 +57,8 @@ def test_msvd_batch_uneven(rt, o64):
     sizes = [(64, 64), (33, 130), (250, 17), (128, 300), (1080, 1920)]
     pairs = [synth.rgb_blockquant_pair(h, w, config=2, pair=i) for i, (h, w) in enumerate(sizes)]
     got = iqm_b200.SVD(rt).compute_batch(pairs)
-    for (a, b), g in zip(pairs, got):
-        assert close(g, o64.msvd(a, b))
+    for (a, b), g, (h, w) in zip(pairs, got, sizes):
+        assert close(g, o64.msvd(a, b), computed_blocks(h, w))
 
 
 def test_msvd_rejects_tiny(rt):
