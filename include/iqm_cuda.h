@@ -103,6 +103,12 @@ int iqm_fsim(iqm_ctx *ctx, const uint8_t *rgba_in, const uint8_t *rgba_ref, int 
              size_t row_bytes, iqm_precision precision, int energy_mode, double *fsim,
              double *fsimc);
 
+/* Size-only FSIM constants of a W'xH' plane, as used by the noise model: EM_n(o) (the filter
+ * energy of fsim_filter_combinations.cpp:76-134) and the estimated noise-energy sums EstSumAn2(o),
+ * EstSumAiAj(o) (shaders/fsim/fsim_mult_filters.glsl) pooled per energy_mode; 4 values each. */
+int iqm_fsim_plan_constants(iqm_ctx *ctx, int w2, int h2, int energy_mode, double *em, double *an2,
+                            double *aiaj);
+
 /* ---- batches: many pairs (uneven sizes allowed) in one launch sequence -------------------- */
 typedef struct {
     const uint8_t *input; /* RGBA8 distorted image */

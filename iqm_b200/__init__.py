@@ -33,7 +33,7 @@ EXPORTS = (
     "iqm_device_name", "iqm_ssim_default_params", "iqm_ssim", "iqm_msvd", "iqm_flip_default_params",
     "iqm_flip_ppd", "iqm_flip", "iqm_fsim", "iqm_ssim_dev", "iqm_msvd_dev", "iqm_flip_dev",
     "iqm_fsim_dev", "iqm_ssim_batch", "iqm_msvd_batch", "iqm_flip_batch", "iqm_fsim_batch",
-    "iqm_last_launch_count",
+    "iqm_last_launch_count", "iqm_fsim_plan_constants",
 )
 
 
@@ -98,6 +98,7 @@ def load_library(path=LIB_PATH):
     L.iqm_flip_batch.argtypes = [vp, PP, ip, ctypes.POINTER(FLIPParams), dp]
     L.iqm_fsim_batch.argtypes = [vp, PP, ip, ip, ip, dp]
     L.iqm_last_launch_count.argtypes = [vp]
+    L.iqm_fsim_plan_constants.argtypes = [vp, ip, ip, ip, dp, dp, dp]
     _lib = L
     return L
 
@@ -346,6 +347,13 @@ class FSIM:
         self.rt.check(self.rt.L.iqm_fsim_batch(self.rt.h, arr, len(keep), self.precision, self.energy_mode,
                                                out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return out.reshape(-1, 2)
+
+    def plan_constants(self, w2, h2):
+        """(EM_n, EstSumAn2, EstSumAiAj) per orientation for a W'xH' plane."""
+        em, an2, aiaj = np.empty(4), np.empty(4), np.empty(4)
+        P = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        self.rt.check(self.rt.L.iqm_fsim_plan_constants(self.rt.h, w2, h2, self.energy_mode, P(em), P(an2), P(aiaj)))
+        return em, an2, aiaj
 
     def compute_dev(self, dev_pairs, d_scores):
         arr = _pairs(dev_pairs)

@@ -1,0 +1,237 @@
+// Complex FP32 FFTs in shared memory (sm_100a), the transform engine behind FSIM.
+//
+// The reference delegates its FFTs to VkFFT (src/gpu/fsim/fsim.cpp:201-263 plans, :364 forward
+// with sign -1 and no scaling, :378 inverse with sign +1 and normalize = 1/N).  Here a transform
+// of length n runs inside one CTA as a Stockham auto-sort FFT: log_p stages, each reading one
+// buffer and writing the other, so no bit reversal is needed.  n is factored into radices
+// 8, 4, 2, 3, 5, 7 and other odd primes up to 61 (an O(p^2) butterfly); a length with a larger
+// prime factor is computed with Bluestein's chirp-z algorithm on a power-of-two length m >= 2n-1.
+//
+// Stage s with radix p and stride L (the product of the earlier radices), butterfly j in [0, n/p):
+//   k = j mod L;  v_r = in[j + r n/p] * W^(r k),  W = exp(sign 2 pi i / (L p));
+//   V = DFT_p(v);  out[(j / L) L p + k + q L] = V_q.
+// Twiddles come from a per-length table exp(-2 pi i t / n), t < n, evaluated in double on the host
+// and rounded to float (conjugated for sign = +1).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace iqm {
+
+constexpr int FFT_MAX_STAGES = 16;
+constexpr int FFT_MAX_GENERIC = 61;  // largest prime handled by the direct butterfly
+
+// Device-visible description of one transform length.
+struct FftLen {
+    int n;
+    int nst;
+    int radix[FFT_MAX_STAGES];
+    const float2 *tw;         // n entries, exp(-2 pi i t / n)
+    // Bluestein data (bluestein != 0): x -> c * IFFT_m( FFT_m(c * x) * B ), c = chirp
+    int bluestein;
+    int m;
+    int mst;
+    int mradix[FFT_MAX_STAGES];
+    const float2 *mtw;        // m entries, exp(-2 pi i t / m)
+    const float2 *chirp;      // n entries, exp(-pi i t^2 / n)
+    const float2 *bfwd;       // m entries, FFT_m(conj chirp, wrapped) / m      (sign -1)
+    const float2 *binv;       // m entries, FFT_m(chirp, wrapped) / m           (sign +1)
+};
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// multiply by i*s (s = +-1)
+__device__ __forceinline__ float2 cmul_is(float2 a, float s) { return make_float2(-s * a.y, s * a.x); }
+__device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
+
+__device__ __forceinline__ float2 tw_at(const float2 *tw, int idx, float s) {
+    const float2 w = __ldg(tw + idx);
+    return make_float2(w.x, -s * w.y);  // table holds sign -1; s = sign
+}
+
+// DFT of p points in registers, sign s: V_q = sum_r v_r exp(s 2 pi i r q / p).
+template <int P>
+__device__ __forceinline__ void dft_small(float2 *v, float s);
+
+template <>
+__device__ __forceinline__ void dft_small<2>(float2 *v, float s) {
+    const float2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+}
+template <>
+__device__ __forceinline__ void dft_small<3>(float2 *v, float s) {
+    const float c = 0.86602540378443865f;  // sqrt(3)/2
+    const float2 t1 = cadd(v[1], v[2]);
+    const float2 t2 = make_float2(v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y);
+    const float2 d = csub(v[1], v[2]);
+    const float2 t3 = cmul_is(make_float2(c * d.x, c * d.y), s);
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(t2, t3);
+    v[2] = csub(t2, t3);
+}
+template <>
+__device__ __forceinline__ void dft_small<4>(float2 *v, float s) {
+    const float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+    const float2 b0 = cadd(v[1], v[3]), b1 = cmul_is(csub(v[1], v[3]), s);
+    v[0] = cadd(a0, b0);
+    v[2] = csub(a0, b0);
+    v[1] = cadd(a1, b1);
+    v[3] = csub(a1, b1);
+}
+template <>
+__device__ __forceinline__ void dft_small<5>(float2 *v, float s) {
+    const float c1 = 0.30901699437494742f, c2 = -0.80901699437494742f;
+    const float s1 = 0.95105651629515357f, s2 = 0.58778525229247313f;
+    const float2 p14 = cadd(v[1], v[4]), m14 = csub(v[1], v[4]);
+    const float2 p23 = cadd(v[2], v[3]), m23 = csub(v[2], v[3]);
+    const float2 a0 = v[0];
+    const float2 r1 = make_float2(a0.x + c1 * p14.x + c2 * p23.x, a0.y + c1 * p14.y + c2 * p23.y);
+    const float2 r2 = make_float2(a0.x + c2 * p14.x + c1 * p23.x, a0.y + c2 * p14.y + c1 * p23.y);
+    const float2 i1 = cmul_is(make_float2(s1 * m14.x + s2 * m23.x, s1 * m14.y + s2 * m23.y), s);
+    const float2 i2 = cmul_is(make_float2(s2 * m14.x - s1 * m23.x, s2 * m14.y - s1 * m23.y), s);
+    v[0] = cadd(a0, cadd(p14, p23));
+    v[1] = cadd(r1, i1);
+    v[4] = csub(r1, i1);
+    v[2] = cadd(r2, i2);
+    v[3] = csub(r2, i2);
+}
+template <>
+__device__ __forceinline__ void dft_small<8>(float2 *v, float s) {
+    float2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+    dft_small<4>(e, s);
+    dft_small<4>(o, s);
+    const float h = 0.70710678118654752f;
+    // W8^q for q = 0..3 with W8 = exp(s 2 pi i / 8)
+    const float2 w1 = make_float2(h, s * h), w3 = make_float2(-h, s * h);
+    const float2 t0 = o[0];
+    const float2 t1 = cmul(o[1], w1);
+    const float2 t2 = cmul_is(o[2], s);
+    const float2 t3 = cmul(o[3], w3);
+    v[0] = cadd(e[0], t0); v[4] = csub(e[0], t0);
+    v[1] = cadd(e[1], t1); v[5] = csub(e[1], t1);
+    v[2] = cadd(e[2], t2); v[6] = csub(e[2], t2);
+    v[3] = cadd(e[3], t3); v[7] = csub(e[3], t3);
+}
+
+// One Stockham stage of radix P over `batch` transforms (buffers `stride` apart).
+template <int P>
+__device__ __forceinline__ void stage_fixed(const float2 *in, float2 *out, int n, int L, const float2 *tw,
+                                            float s, int batch, int stride) {
+    const int q = n / P;
+    const int twstep = n / (L * P);
+    const int total = batch * q;
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const int t = idx / q, j = idx - t * q;
+        const float2 *src = in + t * stride;
+        float2 *dst = out + t * stride;
+        const int k = j % L;
+        float2 v[P];
+#pragma unroll
+        for (int r = 0; r < P; r++) v[r] = src[j + r * q];
+        if (k != 0) {
+#pragma unroll
+            for (int r = 1; r < P; r++) v[r] = cmul(v[r], tw_at(tw, r * k * twstep, s));
+        }
+        dft_small<P>(v, s);
+        const int base = (j / L) * L * P + k;
+#pragma unroll
+        for (int r = 0; r < P; r++) dst[base + r * L] = v[r];
+    }
+}
+
+// Radix-p stage for an odd prime p <= FFT_MAX_GENERIC: direct p-point DFT from the table.
+__device__ __forceinline__ void stage_generic(const float2 *in, float2 *out, int n, int L, int p,
+                                              const float2 *tw, float s, int batch, int stride) {
+    const int q = n / p;
+    const int twstep = n / (L * p);
+    const int total = batch * q;
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const int t = idx / q, j = idx - t * q;
+        const float2 *src = in + t * stride;
+        float2 *dst = out + t * stride;
+        const int k = j % L;
+        const int base = (j / L) * L * p + k;
+        for (int qq = 0; qq < p; qq++) {
+            float2 acc = make_float2(0.f, 0.f);
+            for (int r = 0; r < p; r++) {
+                float2 x = src[j + r * q];
+                if (k != 0 && r != 0) x = cmul(x, tw_at(tw, r * k * twstep, s));
+                // exp(s 2 pi i r qq / p) = table entry (r qq mod p) * (n / p)
+                const int e = (r * qq) % p;
+                acc = e ? cadd(acc, cmul(x, tw_at(tw, e * q, s))) : cadd(acc, x);
+            }
+            dst[base + qq * L] = acc;
+        }
+    }
+}
+
+// Stockham FFT of `batch` transforms of length n (no Bluestein), ping-ponging between a and b.
+// Returns the buffer holding the result.  Every thread of the block must call it.
+__device__ inline float2 *fft_stockham(float2 *a, float2 *b, int n, int nst, const int *radix, const float2 *tw,
+                                       float s, int batch, int stride) {
+    int L = 1;
+    float2 *in = a, *out = b;
+    for (int st = 0; st < nst; st++) {
+        const int p = radix[st];
+        __syncthreads();
+        switch (p) {
+            case 2: stage_fixed<2>(in, out, n, L, tw, s, batch, stride); break;
+            case 3: stage_fixed<3>(in, out, n, L, tw, s, batch, stride); break;
+            case 4: stage_fixed<4>(in, out, n, L, tw, s, batch, stride); break;
+            case 5: stage_fixed<5>(in, out, n, L, tw, s, batch, stride); break;
+            case 8: stage_fixed<8>(in, out, n, L, tw, s, batch, stride); break;
+            default: stage_generic(in, out, n, L, p, tw, s, batch, stride); break;
+        }
+        L *= p;
+        float2 *t = in;
+        in = out;
+        out = t;
+    }
+    __syncthreads();
+    return in;
+}
+
+// Shared-memory floats a transform of this length needs per batch entry (two ping-pong buffers).
+__host__ __device__ inline int fft_work_len(const FftLen &P) { return P.bluestein ? P.m : P.n; }
+
+// FFT of `batch` transforms of length P.n stored in a (stride apart, stride >= fft_work_len);
+// b is scratch of the same size.  Result (unscaled) returned in a or b.
+__device__ inline float2 *fft_run(float2 *a, float2 *b, const FftLen &P, float s, int batch, int stride) {
+    if (!P.bluestein) return fft_stockham(a, b, P.n, P.nst, P.radix, P.tw, s, batch, stride);
+    const int n = P.n, m = P.m;
+    // a_j = x_j * c_j (c conjugated for the inverse sign), zero padded to m
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < batch * m; idx += blockDim.x) {
+        const int t = idx / m, j = idx - t * m;
+        float2 *x = a + t * stride;
+        if (j < n) {
+            float2 c = __ldg(P.chirp + j);
+            if (s > 0) c = conjf2(c);
+            x[j] = cmul(x[j], c);
+        } else {
+            x[j] = make_float2(0.f, 0.f);
+        }
+    }
+    float2 *r = fft_stockham(a, b, m, P.mst, P.mradix, P.mtw, -1.f, batch, stride);
+    const float2 *B = s < 0 ? P.bfwd : P.binv;
+    for (int idx = threadIdx.x; idx < batch * m; idx += blockDim.x) {
+        const int t = idx / m, j = idx - t * m;
+        r[t * stride + j] = cmul(r[t * stride + j], __ldg(B + j));
+    }
+    float2 *o = (r == a) ? b : a;
+    float2 *y = fft_stockham(r, o, m, P.mst, P.mradix, P.mtw, 1.f, batch, stride);
+    for (int idx = threadIdx.x; idx < batch * n; idx += blockDim.x) {
+        const int t = idx / n, j = idx - t * n;
+        float2 c = __ldg(P.chirp + j);
+        if (s > 0) c = conjf2(c);
+        y[t * stride + j] = cmul(y[t * stride + j], c);
+    }
+    __syncthreads();
+    return y;
+}
+
+}  // namespace iqm

@@ -1,0 +1,787 @@
+// FSIM / FSIMc on sm_100a.
+//
+// Reference path (cadik/IQM, src/gpu/fsim/fsim.cpp:80-163 and src/gpu/fsim/steps/*): downscale to
+// W'xH' (F = max(1, round(min(W,H)/256))) as YIQ, gradient map, VkFFT forward transform of luma,
+// 48 filtered spectra and 48 inverse transforms, per-orientation response sums, a host round trip
+// for the noise medians, noise-energy estimates, phase congruency, similarity maps and three
+// multi-pass float reductions.
+//
+// Here, per group of pairs with the same W'xH', seven kernels:
+//   fsim_ingest_kernel      full-resolution RGBA8 -> I, Q, Y planes of both images (box F x F)
+//   fsim_fwd_rows_kernel    forward FFT along x of the two luma planes (shared-memory Stockham)
+//   fsim_fwd_cols_kernel    forward FFT along y
+//   fsim_inv_cols_kernel    spectrum x log-Gabor_s x angular_o, inverse FFT along y (32 planes)
+//   fsim_inv_rows_kernel    inverse FFT along x of the 4 scales of one orientation, scaled 1/N,
+//                           fused with the response sums of fsim_sum_filter_responses.glsl and
+//                           the |EO(s=0)|^2 values of fsim_pack_for_median.glsl
+//   fsim_noise_kernel       exact upper median by radix select (no host round trip), noise power
+//                           and the phase-congruency threshold T in FP64
+//   fsim_final_kernel       phase congruency, gradient (3x3 on the fly), similarity terms and the
+//                           three pooled sums in FP64; the last CTA of a pair writes FSIM, FSIMc
+// The 16 filters and the size-only constants (EM_n, EstSumAn2, EstSumAiAj; fsim_filter_noise.glsl,
+// fsim_mult_filters.glsl) are built once per W'xH' with the same kernels and cached on the context.
+// Pairs are processed in chunks whose intermediates fit the 126 MB L2.
+#include <algorithm>
+#include <cmath>
+#include <map>
+
+#include "fft.cuh"
+#include "fft_plan.cuh"
+#include "iqm_internal.cuh"
+#include "select.cuh"
+
+#define GLSL_PI 3.141592653589
+
+namespace iqm {
+
+struct FsimPlan {
+    int w2 = 0, h2 = 0, n = 0;
+    FftLen row{}, col{};
+    float *filters = nullptr;  // 16 planes of n (z = o*4 + s)
+    double *consts = nullptr;  // device: em[4], an2[2][4], aiaj[2][4]
+    double em[4], an2[2][4], aiaj[2][4];
+    ~FsimPlan() {
+        if (filters) cudaFree(filters);
+        if (consts) cudaFree(consts);
+    }
+};
+
+}  // namespace iqm
+
+using iqm::FftLen;
+
+namespace {
+
+constexpr int FT = 256;  // threads per FFT / pointwise CTA
+
+struct FsimPairDev {
+    const uint8_t *a;
+    const uint8_t *b;
+    long long pitch;
+    int w, h, F;
+    int out;  // index of this pair in the caller's score array
+};
+
+struct FsimGroup {
+    const FsimPairDev *pairs;
+    int G;          // pairs in this launch
+    int w2, h2, n;
+    float *yiq;     // G x 2 x 3 x n   (I, Q, Y)
+    float2 *spec;   // G x 2 x n
+    float2 *T;      // G x 2 x 16 x n  (after the column pass of the inverse transform)
+    float *amp;     // G x 8 x n       (img*4 + o)
+    float *energy;  // G x 8 x n
+    float *eo0;     // G x 8 x n       |EO(s=0, o)|^2
+    float *thr;     // G x 8
+    double *partials;  // G x tiles x 3
+    unsigned *counters;
+    int tiles;
+    double *scores;    // 2 per pair: fsim, fsimc
+    const float *filters;
+    const double *consts;
+    int energy_mode;
+};
+
+// ---------------------------------------------------------------------------------------------
+// filters -- shaders/fsim/fsim_lowpassfilter.glsl:21-42 (cutoff 0.45, order 15),
+// fsim_log_gabor.glsl:16-49 (minWaveLength 6, mult 2, sigmaOnf 0.55), fsim_angular.glsl:16-48,
+// combined as in fsim_filter_combinations.glsl:44-51 (z = o*4 + s)
+__device__ __forceinline__ float freq_coord(int i, int n) {
+    const int shifted = (i + n / 2) % n;
+    return float(shifted - n / 2) / float(n);
+}
+
+__global__ void fsim_filters_kernel(float *filters, int w2, int h2) {
+    const int n = w2 * h2;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int x = p % w2, y = p / w2;
+    const float sx = freq_coord(x, w2), sy = freq_coord(y, h2);
+    const float radius = sqrtf(sx * sx + sy * sy);
+    const float lp = 1.0f / (1.0f + powf(radius / 0.45f, 2.0f * 15.0f));
+    float lg[4];
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+        const float wavelength = 6.0f * powf(2.0f, float(s));
+        const float freq = 1.0f / wavelength;
+        const float lr = logf(radius / freq);
+        const float ls = logf(0.55f);
+        const float v = expf(-(lr * lr) / (2.0f * (ls * ls)));
+        lg[s] = (x == 0 && y == 0) ? 0.0f : v * lp;
+    }
+    const float theta_sigma = float(GLSL_PI) / 4.0f / 1.2f;
+    const float theta = atan2f(-sy, sx);
+    const float st = sinf(theta), ct = cosf(theta);
+#pragma unroll
+    for (int o = 0; o < 4; o++) {
+        const float angle = (float(o) * float(GLSL_PI)) / 4.0f;
+        const float ds = st * cosf(angle) - ct * sinf(angle);
+        const float dc = ct * cosf(angle) + st * sinf(angle);
+        const float dtheta = fabsf(atan2f(ds, dc));
+        const float a = expf(-(dtheta * dtheta) / (2.0f * (theta_sigma * theta_sigma)));
+#pragma unroll
+        for (int s = 0; s < 4; s++) filters[(o * 4 + s) * n + p] = lg[s] * a;
+    }
+}
+
+// EM_n(o) = sum_p H[o*4+0](p)^2 (fsim_filter_combinations.cpp:76-134 with fsim_filter_noise.glsl)
+__global__ void fsim_em_kernel(const float *filters, int n, double *consts) {
+    __shared__ double red[FT / 32];
+    const int o = blockIdx.x;
+    const float *f = filters + (o * 4) * n;
+    double s = 0.0;
+    for (int p = threadIdx.x; p < n; p += FT) {
+        const float v = f[p];
+        s += double(v * v);
+    }
+    for (int d = 16; d > 0; d >>= 1) s += __shfl_down_sync(0xffffffffu, s, d);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < FT / 32; i++) t += red[i];
+        consts[o] = t;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// ingest -- shaders/fsim/fsim_downsample.glsl:21-55: RGB x 255 -> (I, Q, Y), F x F box starting
+// at (x F - F/2, y F - F/2), out-of-image samples contribute 0, divided by F^2 always.
+__global__ void __launch_bounds__(FT) fsim_ingest_kernel(FsimGroup g) {
+    __shared__ float u8f[256];  // (b / 255) * 255 in float, as the unorm load followed by * 255.0
+    for (int i = threadIdx.x; i < 256; i += FT) u8f[i] = __fdiv_rn(float(i), 255.0f) * 255.0f;
+    __syncthreads();
+    const int pi = blockIdx.y;
+    const int p = blockIdx.x * FT + threadIdx.x;
+    if (p >= g.n) return;
+    const FsimPairDev P = g.pairs[pi];
+    const int x = p % g.w2, y = p / g.w2;
+    const int F = P.F;
+    const int xs = x * F - F / 2, ys = y * F - F / 2;
+    const float scaler = float(F * F);
+#pragma unroll
+    for (int img = 0; img < 2; img++) {
+        const uint8_t *base = img ? P.b : P.a;
+        float sI = 0.f, sQ = 0.f, sY = 0.f;
+        for (int j = xs; j < xs + F; j++) {
+            if (j < 0 || j >= P.w) continue;
+            for (int k = ys; k < ys + F; k++) {
+                if (k < 0 || k >= P.h) continue;
+                const uint32_t px = __ldg(reinterpret_cast<const uint32_t *>(base + (long long)k * P.pitch) + j);
+                const float r = u8f[px & 0xffu], gg = u8f[(px >> 8) & 0xffu], b = u8f[(px >> 16) & 0xffu];
+                sI += r * 0.596f - gg * 0.274f - b * 0.322f;
+                sQ += r * 0.211f - gg * 0.523f + b * 0.312f;
+                sY += r * 0.299f + gg * 0.587f + b * 0.114f;
+            }
+        }
+        float *dst = g.yiq + size_t(pi * 2 + img) * 3 * g.n;
+        dst[p] = sI / scaler;
+        dst[g.n + p] = sQ / scaler;
+        dst[2 * g.n + p] = sY / scaler;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// forward transform (src/gpu/fsim/fsim.cpp:270-368: luma as complex (Y, 0), sign -1, unscaled)
+__global__ void __launch_bounds__(FT) fsim_fwd_rows_kernel(FsimGroup g, FftLen L, int rows, int wl) {
+    extern __shared__ float2 sm[];
+    float2 *a = sm, *b = sm + rows * wl;
+    const int plane = blockIdx.y;  // pair*2 + img
+    const int y0 = blockIdx.x * rows;
+    const int nr = min(rows, g.h2 - y0);
+    const float *Y = g.yiq + (size_t(plane) * 3 + 2) * g.n;
+    for (int idx = threadIdx.x; idx < nr * g.w2; idx += FT) {
+        const int r = idx / g.w2, x = idx - r * g.w2;
+        a[r * wl + x] = make_float2(Y[(y0 + r) * g.w2 + x], 0.f);
+    }
+    const float2 *res = iqm::fft_run(a, b, L, -1.f, nr, wl);
+    float2 *S = g.spec + size_t(plane) * g.n;
+    for (int idx = threadIdx.x; idx < nr * g.w2; idx += FT) {
+        const int r = idx / g.w2, x = idx - r * g.w2;
+        S[(y0 + r) * g.w2 + x] = res[r * wl + x];
+    }
+}
+
+__global__ void __launch_bounds__(FT) fsim_fwd_cols_kernel(FsimGroup g, FftLen L, int cols, int wl) {
+    extern __shared__ float2 sm[];
+    float2 *a = sm, *b = sm + cols * wl;
+    const int plane = blockIdx.y;
+    const int x0 = blockIdx.x * cols;
+    const int nc = min(cols, g.w2 - x0);
+    float2 *S = g.spec + size_t(plane) * g.n;
+    for (int idx = threadIdx.x; idx < nc * g.h2; idx += FT) {
+        const int y = idx / nc, c = idx - y * nc;
+        a[c * wl + y] = S[y * g.w2 + x0 + c];
+    }
+    const float2 *res = iqm::fft_run(a, b, L, -1.f, nc, wl);
+    for (int idx = threadIdx.x; idx < nc * g.h2; idx += FT) {
+        const int y = idx / nc, c = idx - y * nc;
+        S[y * g.w2 + x0 + c] = res[c * wl + y];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// inverse transform, pass 1 (along y) of the 16 filtered spectra of one orientation:
+// spectrum x H[o*4+s] (fsim_filter_combinations.glsl:53-56), sign +1.  consts_mode uses a
+// spectrum of ones, i.e. transforms the filters themselves (block 0 of the reference's buffer).
+__global__ void __launch_bounds__(FT) fsim_inv_cols_kernel(FsimGroup g, FftLen L, int cols, int wl, int consts_mode) {
+    extern __shared__ float2 sm[];
+    float2 *S = sm;                 // cols x h2 spectrum slice
+    float2 *a = sm + cols * g.h2;   // cols x wl
+    float2 *b = a + cols * wl;
+    const int o = blockIdx.y;
+    const int plane = blockIdx.z;  // pair*2 + img (0 in consts mode)
+    const int x0 = blockIdx.x * cols;
+    const int nc = min(cols, g.w2 - x0);
+    const float2 *src = g.spec + size_t(plane) * g.n;
+    for (int idx = threadIdx.x; idx < nc * g.h2; idx += FT) {
+        const int y = idx / nc, c = idx - y * nc;
+        S[c * g.h2 + y] = consts_mode ? make_float2(1.f, 0.f) : src[y * g.w2 + x0 + c];
+    }
+    __syncthreads();
+    for (int s = 0; s < 4; s++) {
+        const int z = o * 4 + s;
+        const float *H = g.filters + size_t(z) * g.n;
+        for (int idx = threadIdx.x; idx < nc * g.h2; idx += FT) {
+            const int y = idx / nc, c = idx - y * nc;
+            const float h = __ldg(H + y * g.w2 + x0 + c);
+            const float2 v = S[c * g.h2 + y];
+            a[c * wl + y] = make_float2(h * v.x, h * v.y);
+        }
+        const float2 *res = iqm::fft_run(a, b, L, 1.f, nc, wl);
+        float2 *dst = g.T + (size_t(plane) * 16 + z) * g.n;
+        for (int idx = threadIdx.x; idx < nc * g.h2; idx += FT) {
+            const int y = idx / nc, c = idx - y * nc;
+            dst[y * g.w2 + x0 + c] = res[c * wl + y];
+        }
+        __syncthreads();
+    }
+}
+
+// inverse transform, pass 2 (along x) of the 4 scales of orientation o for one row, scaled 1/N,
+// then per pixel (shaders/fsim/fsim_sum_filter_responses.glsl:43-80):
+//   sumAn = sum_s |EO_s|;  (MeanE, MeanO) = (sum E, sum O) / (|(sum E, sum O)| + 1e-4)
+//   Energy = sum_s E MeanE + O MeanO - |E MeanO - O MeanE|
+// and |EO_0|^2 for the noise median (shaders/fsim/fsim_pack_for_median.glsl:39-43).
+// consts_mode instead accumulates, per row, sum_s Re_s^2 N and sum_{i<j} Re_i Re_j N
+// (shaders/fsim/fsim_mult_filters.glsl:37-58) over p < ceil(N/2) and over all p.
+__global__ void __launch_bounds__(FT) fsim_inv_rows_kernel(FsimGroup g, FftLen L, int wl, int seq,
+                                                           int consts_mode, double *rowsums) {
+    extern __shared__ float2 sm[];
+    const int y = blockIdx.x, o = blockIdx.y, plane = blockIdx.z;
+    const int w2 = g.w2;
+    const float2 *src = g.T + (size_t(plane) * 16 + o * 4) * g.n + size_t(y) * w2;
+    float2 *keep;  // 4 x w2 results
+    if (!seq) {
+        float2 *a = sm, *b = sm + 4 * wl;
+        for (int idx = threadIdx.x; idx < 4 * w2; idx += FT) {
+            const int s = idx / w2, x = idx - s * w2;
+            a[s * wl + x] = src[size_t(s) * g.n + x];
+        }
+        float2 *res = iqm::fft_run(a, b, L, 1.f, 4, wl);
+        // compact to stride w2 is unnecessary: index with stride wl below
+        keep = res;
+    } else {
+        keep = sm;                      // 4 x w2
+        float2 *a = sm + 4 * w2, *b = a + wl;
+        for (int s = 0; s < 4; s++) {
+            for (int x = threadIdx.x; x < w2; x += FT) a[x] = src[size_t(s) * g.n + x];
+            const float2 *res = iqm::fft_run(a, b, L, 1.f, 1, wl);
+            for (int x = threadIdx.x; x < w2; x += FT) keep[s * w2 + x] = res[x];
+            __syncthreads();
+        }
+    }
+    const int ks = seq ? w2 : wl;
+    const float invN = 1.0f / float(g.n);
+    if (!consts_mode) {
+        const size_t off = (size_t(plane) * 4 + o) * g.n + size_t(y) * w2;
+        for (int x = threadIdx.x; x < w2; x += FT) {
+            float re[4], im[4];
+            float sA = 0.f, sE = 0.f, sO = 0.f;
+#pragma unroll
+            for (int s = 0; s < 4; s++) {
+                const float2 v = keep[s * ks + x];
+                re[s] = v.x * invN;
+                im[s] = v.y * invN;
+                sA += sqrtf(re[s] * re[s] + im[s] * im[s]);
+                sE += re[s];
+                sO += im[s];
+            }
+            const float xe = sqrtf(sE * sE + sO * sO) + 0.0001f;
+            const float mE = sE / xe, mO = sO / xe;
+            float en = 0.f;
+#pragma unroll
+            for (int s = 0; s < 4; s++) en += re[s] * mE + im[s] * mO - fabsf(re[s] * mO - im[s] * mE);
+            g.amp[off + x] = sA;
+            g.energy[off + x] = en;
+            g.eo0[off + x] = re[0] * re[0] + im[0] * im[0];
+        }
+    } else {
+        __shared__ double red[4][FT / 32];
+        const long lim = (long(g.n) + 1) / 2;
+        const float fn = float(g.n);
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};  // an2 (ref), aiaj (ref), an2 (full), aiaj (full)
+        for (int x = threadIdx.x; x < w2; x += FT) {
+            float re[4];
+#pragma unroll
+            for (int s = 0; s < 4; s++) re[s] = keep[s * ks + x].x * invN;
+            float q2 = 0.f, qx = 0.f;
+#pragma unroll
+            for (int s = 0; s < 4; s++) q2 += (re[s] * re[s]) * fn;
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = i + 1; j < 4; j++) qx += re[i] * re[j] * fn;
+            const long p = long(y) * w2 + x;
+            if (p < lim) {
+                acc[0] += q2;
+                acc[1] += qx;
+            }
+            acc[2] += q2;
+            acc[3] += qx;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            double v = acc[q];
+            for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
+            if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < 4) {
+            double t = 0.0;
+            for (int i = 0; i < FT / 32; i++) t += red[threadIdx.x][i];
+            rowsums[(size_t(o) * g.h2 + y) * 4 + threadIdx.x] = t;
+        }
+    }
+}
+
+// sum the per-row constants in row order -> an2[mode][o], aiaj[mode][o]
+__global__ void fsim_consts_reduce_kernel(const double *rowsums, int h2, double *consts) {
+    const int o = threadIdx.x;  // 4 threads
+    if (o >= 4) return;
+    double t[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int y = 0; y < h2; y++)
+        for (int q = 0; q < 4; q++) t[q] += rowsums[(size_t(o) * h2 + y) * 4 + q];
+    consts[4 + 0 * 4 + o] = t[0];   // an2 [ref]
+    consts[12 + 0 * 4 + o] = t[1];  // aiaj[ref]
+    consts[4 + 1 * 4 + o] = t[2];   // an2 [full]
+    consts[12 + 1 * 4 + o] = t[3];  // aiaj[full]
+}
+
+// ---------------------------------------------------------------------------------------------
+// noise power and threshold -- src/gpu/fsim/steps/fsim_noise_power.cpp:193-205 (upper median of a
+// full sort, mean = -median/ln 0.5, divided by EM_n(o)) and shaders/fsim/fsim_phase_congruency.glsl:
+// 42-53 (estimated noise energy, tau, T = (mu + k sigma)/1.7 with k = 2); evaluated in FP64.
+__global__ void __launch_bounds__(1024) fsim_noise_kernel(FsimGroup g) {
+    __shared__ unsigned hist[iqm::SELECT_BINS];
+    const int q = blockIdx.x;   // img*4 + o
+    const int pi = blockIdx.y;
+    const int o = q & 3;
+    const float *v = g.eo0 + (size_t(pi) * 8 + q) * g.n;
+    const float med = iqm::block_select_kth(v, g.n, g.n / 2, hist);
+    if (threadIdx.x == 0) {
+        const double mean = -double(med) / log(0.5);
+        const double np = mean / g.consts[o];
+        const double an2 = g.consts[4 + g.energy_mode * 4 + o];
+        const double aiaj = g.consts[12 + g.energy_mode * 4 + o];
+        const double e2 = 2.0 * np * an2 + 4.0 * np * aiaj;
+        const double tau = sqrt(e2 / 2.0);
+        const double mu = tau * sqrt(GLSL_PI / 2.0);
+        const double sig = sqrt((2.0 - GLSL_PI / 2.0) * (tau * tau));
+        g.thr[size_t(pi) * 8 + q] = float((mu + 2.0 * sig) / 1.7);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// phase congruency (fsim_phase_congruency.glsl:39-64), gradient (fsim_gradientmap.glsl:16-57),
+// similarities (fsim_final_multiply.glsl:18-58; T1 0.85, T2 160, T3 = T4 200, lambda 0.03) and the
+// pooled sums (fsim_final_multiply.cpp:294-300), FP64 accumulation.
+__device__ __forceinline__ float grad_at(const float *Y, int x, int y, int w2, int h2) {
+    const float vert[9] = {3.f, 0.f, -3.f, 10.f, 0.f, -10.f, 3.f, 0.f, -3.f};
+    const float hor[9] = {3.f, 10.f, 3.f, 0.f, 0.f, 0.f, -3.f, -10.f, -3.f};
+    float vs = 0.f, hs = 0.f;
+#pragma unroll
+    for (int j = -1; j < 2; j++)
+#pragma unroll
+        for (int k = -1; k < 2; k++) {
+            const int px = x + j, py = y + k;
+            if (px >= 0 && px < w2 && py >= 0 && py < h2) {
+                const float v = Y[py * w2 + px];
+                const int idx = (j + 1) + (k + 1) * 3;
+                vs += v * vert[idx];
+                hs += v * hor[idx];
+            }
+        }
+    const float a = vs / 16.0f, b = hs / 16.0f;
+    return sqrtf(a * a + b * b);
+}
+
+__global__ void __launch_bounds__(FT) fsim_final_kernel(FsimGroup g) {
+    __shared__ double red[3][FT / 32];
+    __shared__ int is_last;
+    const int pi = blockIdx.y;
+    const int p = blockIdx.x * FT + threadIdx.x;
+    const int n = g.n;
+    double s_pcm = 0.0, s_sim = 0.0, s_simc = 0.0;
+    if (p < n) {
+        float pc[2];
+#pragma unroll
+        for (int img = 0; img < 2; img++) {
+            float et = 0.f, at = 0.f;
+#pragma unroll
+            for (int o = 0; o < 4; o++) {
+                const size_t plane = (size_t(pi) * 8 + img * 4 + o) * n;
+                const float e = g.energy[plane + p] - g.thr[size_t(pi) * 8 + img * 4 + o];
+                et += fmaxf(e, 0.f);
+                at += g.amp[plane + p];
+            }
+            pc[img] = et / at;
+        }
+        const float pc1 = pc[0], pc2 = pc[1];
+        const float pcm = fmaxf(pc1, pc2);
+        const float pcsim = (2.0f * pc1 * pc2 + 0.85f) / (pc1 * pc1 + pc2 * pc2 + 0.85f);
+        const int x = p % g.w2, y = p / g.w2;
+        const float *yiq1 = g.yiq + size_t(pi * 2 + 0) * 3 * n;
+        const float *yiq2 = g.yiq + size_t(pi * 2 + 1) * 3 * n;
+        const float g1 = grad_at(yiq1 + 2 * n, x, y, g.w2, g.h2);
+        const float g2 = grad_at(yiq2 + 2 * n, x, y, g.w2, g.h2);
+        const float gsim = (2.0f * g1 * g2 + 160.0f) / (g1 * g1 + g2 * g2 + 160.0f);
+        const float i1 = yiq1[p], i2 = yiq2[p], q1 = yiq1[n + p], q2 = yiq2[n + p];
+        const float isim = (2.0f * i1 * i2 + 200.0f) / (i1 * i1 + i2 * i2 + 200.0f);
+        const float qsim = (2.0f * q1 * q2 + 200.0f) / (q1 * q1 + q2 * q2 + 200.0f);
+        const float sim = gsim * pcsim * pcm;
+        const float simc = gsim * pcsim * powf(fabsf(isim * qsim), 0.03f) * pcm;
+        s_pcm = pcm;
+        s_sim = sim;
+        s_simc = simc;
+    }
+    double v[3] = {s_pcm, s_sim, s_simc};
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        for (int d = 16; d > 0; d >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], d);
+        if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = v[q];
+    }
+    __syncthreads();
+    double *part = g.partials + (size_t(pi) * g.tiles + blockIdx.x) * 3;
+    if (threadIdx.x < 3) {
+        double t = 0.0;
+        for (int i = 0; i < FT / 32; i++) t += red[threadIdx.x][i];
+        part[threadIdx.x] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(&g.counters[pi], 1u);
+        is_last = prev == unsigned(g.tiles - 1);
+    }
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    if (threadIdx.x < 3) {
+        double t = 0.0;
+        const double *pp = g.partials + size_t(pi) * g.tiles * 3;
+        for (int i = 0; i < g.tiles; i++) t += __ldcg(pp + size_t(i) * 3 + threadIdx.x);
+        red[threadIdx.x][0] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int out = g.pairs[pi].out;
+        g.scores[2 * out] = red[1][0] / red[0][0];
+        g.scores[2 * out + 1] = red[2][0] / red[0][0];
+        g.counters[pi] = 0u;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// host orchestration
+
+int downscale_factor(int w, int h) {  // src/gpu/fsim/fsim.cpp:165-168
+    const int smaller = std::min(w, h);
+    return std::max(1, int(std::round(smaller / 256.0)));
+}
+
+void plane_size(int w, int h, int F, int &w2, int &h2) {  // src/gpu/fsim/fsim.cpp:91-92
+    w2 = int(std::round(float(w) / float(F)));
+    h2 = int(std::round(float(h) / float(F)));
+}
+
+constexpr size_t SMEM_CAP = 200 * 1024;
+
+void set_smem(const void *fn, size_t bytes) {
+    if (bytes > 48 * 1024)
+        IQM_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+}
+
+struct Shapes {
+    int rows_fwd, cols_fwd, cols_inv, seq_rows;
+    size_t sm_rows_fwd, sm_cols_fwd, sm_cols_inv, sm_rows_inv;
+};
+
+Shapes shapes_for(const iqm::FsimPlan &P) {
+    Shapes s{};
+    const int wlr = iqm::fft_work_len(P.row), wlc = iqm::fft_work_len(P.col);
+    const size_t f2 = sizeof(float2);
+    auto round8 = [](int c) { return c >= 8 ? c & ~7 : c; };  // whole 64-byte row segments
+    s.rows_fwd = std::max(1, std::min(8, int((64 * 1024) / (2 * wlr * f2))));
+    s.sm_rows_fwd = 2 * size_t(s.rows_fwd) * wlr * f2;
+    s.cols_fwd = round8(std::max(1, std::min(16, int((64 * 1024) / (2 * wlc * f2)))));
+    s.sm_cols_fwd = 2 * size_t(s.cols_fwd) * wlc * f2;
+    s.cols_inv = round8(std::max(1, std::min(16, int((96 * 1024) / ((P.h2 + 2 * wlc) * f2)))));
+    s.sm_cols_inv = size_t(s.cols_inv) * (P.h2 + 2 * wlc) * f2;
+    const size_t batch4 = 2 * 4 * size_t(wlr) * f2;
+    s.seq_rows = batch4 > 160 * 1024 ? 1 : 0;
+    s.sm_rows_inv = s.seq_rows ? (4 * size_t(P.w2) + 2 * wlr) * f2 : batch4;
+    IQM_REQUIRE(s.sm_rows_fwd <= SMEM_CAP && s.sm_cols_fwd <= SMEM_CAP && s.sm_cols_inv <= SMEM_CAP &&
+                    s.sm_rows_inv <= SMEM_CAP,
+                "FSIM plane too large for the shared-memory FFT");
+    return s;
+}
+
+void configure_kernels(const Shapes &s) {
+    set_smem((const void *)fsim_fwd_rows_kernel, s.sm_rows_fwd);
+    set_smem((const void *)fsim_fwd_cols_kernel, s.sm_cols_fwd);
+    set_smem((const void *)fsim_inv_cols_kernel, s.sm_cols_inv);
+    set_smem((const void *)fsim_inv_rows_kernel, s.sm_rows_inv);
+}
+
+iqm::FsimPlan *get_plan(iqm_ctx *ctx, int w2, int h2) {
+    auto key = std::make_pair(w2, h2);
+    auto it = ctx->fsim_plans.find(key);
+    if (it != ctx->fsim_plans.end()) return it->second;
+    auto *P = new iqm::FsimPlan();
+    P->w2 = w2;
+    P->h2 = h2;
+    P->n = w2 * h2;
+    const int n = P->n;
+    void *tmp = nullptr;
+    try {
+        P->row = iqm::fft_len(ctx, w2);
+        P->col = iqm::fft_len(ctx, h2);
+        IQM_CHECK_CUDA(cudaMalloc(&P->filters, sizeof(float) * 16 * size_t(n)));
+        IQM_CHECK_CUDA(cudaMalloc(&P->consts, sizeof(double) * 20));
+        const Shapes s = shapes_for(*P);
+        configure_kernels(s);
+        cudaStream_t st = ctx->stream;
+        fsim_filters_kernel<<<iqm::ceil_div(n, FT), FT, 0, st>>>(P->filters, w2, h2);
+        IQM_CHECK_CUDA(cudaGetLastError());
+        fsim_em_kernel<<<4, FT, 0, st>>>(P->filters, n, P->consts);
+        IQM_CHECK_CUDA(cudaGetLastError());
+        // transforms of the filters themselves
+        const size_t tbytes = sizeof(float2) * 16 * size_t(n);
+        const size_t rbytes = sizeof(double) * 4 * 4 * size_t(h2);
+        IQM_CHECK_CUDA(cudaMalloc(&tmp, tbytes + rbytes));
+        FsimGroup g{};
+        g.G = 1;
+        g.w2 = w2;
+        g.h2 = h2;
+        g.n = n;
+        g.T = static_cast<float2 *>(tmp);
+        g.filters = P->filters;
+        double *rowsums = reinterpret_cast<double *>(static_cast<uint8_t *>(tmp) + tbytes);
+        const int wlr = iqm::fft_work_len(P->row), wlc = iqm::fft_work_len(P->col);
+        fsim_inv_cols_kernel<<<dim3(iqm::ceil_div(w2, s.cols_inv), 4, 1), FT, s.sm_cols_inv, st>>>(g, P->col, s.cols_inv,
+                                                                                                  wlc, 1);
+        IQM_CHECK_CUDA(cudaGetLastError());
+        fsim_inv_rows_kernel<<<dim3(h2, 4, 1), FT, s.sm_rows_inv, st>>>(g, P->row, wlr, s.seq_rows, 1, rowsums);
+        IQM_CHECK_CUDA(cudaGetLastError());
+        fsim_consts_reduce_kernel<<<1, 32, 0, st>>>(rowsums, h2, P->consts);
+        IQM_CHECK_CUDA(cudaGetLastError());
+        double host[20];
+        IQM_CHECK_CUDA(cudaMemcpyAsync(host, P->consts, sizeof(host), cudaMemcpyDeviceToHost, st));
+        IQM_CHECK_CUDA(cudaStreamSynchronize(st));
+        cudaFree(tmp);
+        tmp = nullptr;
+        for (int o = 0; o < 4; o++) {
+            P->em[o] = host[o];
+            for (int m = 0; m < 2; m++) {
+                P->an2[m][o] = host[4 + m * 4 + o];
+                P->aiaj[m][o] = host[12 + m * 4 + o];
+            }
+        }
+    } catch (...) {
+        if (tmp) cudaFree(tmp);
+        delete P;
+        throw;
+    }
+    ctx->fsim_plans[key] = P;
+    return P;
+}
+
+struct Layout {
+    size_t yiq, spec, T, planes, thr, partials, counters, total;
+};
+
+Layout layout_for(int G, int n, int tiles) {
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    Layout L{};
+    size_t off = 0;
+    L.yiq = off; off += al(sizeof(float) * size_t(G) * 6 * n);
+    L.spec = off; off += al(sizeof(float2) * size_t(G) * 2 * n);
+    L.T = off; off += al(sizeof(float2) * size_t(G) * 32 * n);
+    L.planes = off; off += al(sizeof(float) * size_t(G) * 24 * n);
+    L.thr = off; off += al(sizeof(float) * size_t(G) * 8);
+    L.partials = off; off += al(sizeof(double) * size_t(G) * tiles * 3);
+    L.counters = off; off += al(sizeof(unsigned) * size_t(G));
+    L.total = off;
+    return L;
+}
+
+// Enqueue FSIM for device-resident pairs; scores[2*i], scores[2*i+1] = FSIM, FSIMc of pair i.
+void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_mode, double *d_scores) {
+    const int n_pairs = int(pairs.size());
+    // group by plane size, keeping the caller's order inside each group
+    std::map<std::pair<int, int>, std::vector<int>> groups;
+    std::vector<FsimPairDev> hd(n_pairs);
+    for (int i = 0; i < n_pairs; i++) {
+        const iqm_pair &q = pairs[i];
+        const int F = downscale_factor(q.w, q.h);
+        int w2, h2;
+        plane_size(q.w, q.h, F, w2, h2);
+        IQM_REQUIRE(w2 >= 1 && h2 >= 1, "FSIM plane is empty");
+        groups[{w2, h2}].push_back(i);
+        hd[i] = FsimPairDev{q.input, q.ref, (long long)q.row_bytes, q.w, q.h, F, i};
+    }
+    // descriptors ordered group by group
+    std::vector<FsimPairDev> ordered;
+    ordered.reserve(n_pairs);
+    for (auto &kv : groups)
+        for (int i : kv.second) ordered.push_back(hd[i]);
+    auto *d_desc = static_cast<FsimPairDev *>(
+        iqm::upload_bytes(ctx, ctx->desc, ordered.data(), sizeof(FsimPairDev) * n_pairs));
+    size_t first = 0;
+    for (auto &kv : groups) {
+        const int w2 = kv.first.first, h2 = kv.first.second;
+        const int Gtot = int(kv.second.size());
+        iqm::FsimPlan *P = get_plan(ctx, w2, h2);
+        const Shapes s = shapes_for(*P);
+        configure_kernels(s);
+        const int n = P->n;
+        const int tiles = int(iqm::ceil_div(n, FT));
+        // chunk so that one chunk's intermediates (~400 bytes per plane pixel) stay in L2
+        const size_t per_pair = layout_for(1, n, tiles).total;
+        const int chunk = std::max(1, std::min(Gtot, int((96ull << 20) / per_pair)));
+        const Layout Lc = layout_for(chunk, n, tiles);
+        auto *base = static_cast<uint8_t *>(ctx->scratch.get(Lc.total, ctx->stream));
+        const int wlr = iqm::fft_work_len(P->row), wlc = iqm::fft_work_len(P->col);
+        for (int c0 = 0; c0 < Gtot; c0 += chunk) {
+            const int G = std::min(chunk, Gtot - c0);
+            FsimGroup g{};
+            g.pairs = d_desc + first + c0;
+            g.G = G;
+            g.w2 = w2;
+            g.h2 = h2;
+            g.n = n;
+            g.yiq = reinterpret_cast<float *>(base + Lc.yiq);
+            g.spec = reinterpret_cast<float2 *>(base + Lc.spec);
+            g.T = reinterpret_cast<float2 *>(base + Lc.T);
+            g.amp = reinterpret_cast<float *>(base + Lc.planes);
+            g.energy = g.amp + size_t(G) * 8 * n;
+            g.eo0 = g.energy + size_t(G) * 8 * n;
+            g.thr = reinterpret_cast<float *>(base + Lc.thr);
+            g.partials = reinterpret_cast<double *>(base + Lc.partials);
+            g.counters = reinterpret_cast<unsigned *>(base + Lc.counters);
+            g.tiles = tiles;
+            g.scores = d_scores;
+            g.filters = P->filters;
+            g.consts = P->consts;
+            g.energy_mode = energy_mode;
+            cudaStream_t st = ctx->stream;
+            IQM_CHECK_CUDA(cudaMemsetAsync(g.counters, 0, sizeof(unsigned) * G, st));
+            fsim_ingest_kernel<<<dim3(tiles, G), FT, 0, st>>>(g);
+            iqm::check_launch(ctx, "fsim_ingest_kernel");
+            fsim_fwd_rows_kernel<<<dim3(iqm::ceil_div(h2, s.rows_fwd), 2 * G), FT, s.sm_rows_fwd, st>>>(
+                g, P->row, s.rows_fwd, wlr);
+            iqm::check_launch(ctx, "fsim_fwd_rows_kernel");
+            fsim_fwd_cols_kernel<<<dim3(iqm::ceil_div(w2, s.cols_fwd), 2 * G), FT, s.sm_cols_fwd, st>>>(
+                g, P->col, s.cols_fwd, wlc);
+            iqm::check_launch(ctx, "fsim_fwd_cols_kernel");
+            fsim_inv_cols_kernel<<<dim3(iqm::ceil_div(w2, s.cols_inv), 4, 2 * G), FT, s.sm_cols_inv, st>>>(
+                g, P->col, s.cols_inv, wlc, 0);
+            iqm::check_launch(ctx, "fsim_inv_cols_kernel");
+            fsim_inv_rows_kernel<<<dim3(h2, 4, 2 * G), FT, s.sm_rows_inv, st>>>(g, P->row, wlr, s.seq_rows, 0,
+                                                                                 nullptr);
+            iqm::check_launch(ctx, "fsim_inv_rows_kernel");
+            fsim_noise_kernel<<<dim3(8, G), 1024, 0, st>>>(g);
+            iqm::check_launch(ctx, "fsim_noise_kernel");
+            fsim_final_kernel<<<dim3(tiles, G), FT, 0, st>>>(g);
+            iqm::check_launch(ctx, "fsim_final_kernel");
+        }
+        first += Gtot;
+    }
+}
+
+void check_fsim_args(const iqm_pair *pairs, int n, iqm_precision precision, int energy_mode) {
+    iqm::check_pairs(pairs, n, 1, 1);
+    IQM_REQUIRE(energy_mode == 0 || energy_mode == 1, "energy_mode must be 0 or 1");
+    IQM_REQUIRE(precision == IQM_FP32 || precision == IQM_MIXED, "unknown precision");
+    for (int i = 0; i < n; i++) {
+        const int F = downscale_factor(pairs[i].w, pairs[i].h);
+        int w2, h2;
+        plane_size(pairs[i].w, pairs[i].h, F, w2, h2);
+        IQM_REQUIRE(w2 >= 2 && h2 >= 2 && w2 <= 4096 && h2 <= 4096,
+                    "pair " + std::to_string(i) + ": FSIM plane size out of range");
+    }
+}
+
+}  // namespace
+
+void iqm_release_fsim_plans(iqm_ctx *ctx) {
+    for (auto &kv : ctx->fsim_plans) delete kv.second;
+    ctx->fsim_plans.clear();
+}
+
+#define IQM_API extern "C" __attribute__((visibility("default")))
+
+IQM_API int iqm_fsim_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, iqm_precision precision, int energy_mode,
+                         double *d_scores) {
+    return iqm::guarded(ctx, [&] {
+        check_fsim_args(pairs, n, precision, energy_mode);
+        IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
+        fsim_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), energy_mode, d_scores);
+    });
+}
+
+IQM_API int iqm_fsim_batch(iqm_ctx *ctx, const iqm_pair *pairs, int n, iqm_precision precision, int energy_mode,
+                           double *scores) {
+    return iqm::guarded(ctx, [&] {
+        check_fsim_args(pairs, n, precision, energy_mode);
+        IQM_REQUIRE(scores != nullptr, "scores is NULL");
+        auto dev = iqm::upload_pairs(ctx, pairs, n);
+        auto *d_scores = static_cast<double *>(ctx->scores.get(sizeof(double) * 2 * n, ctx->stream));
+        fsim_enqueue(ctx, dev, energy_mode, d_scores);
+        IQM_CHECK_CUDA(cudaMemcpyAsync(scores, d_scores, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, ctx->stream));
+        IQM_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+IQM_API int iqm_fsim(iqm_ctx *ctx, const uint8_t *rgba_in, const uint8_t *rgba_ref, int w, int h, size_t row_bytes,
+                     iqm_precision precision, int energy_mode, double *fsim, double *fsimc) {
+    return iqm::guarded(ctx, [&] {
+        IQM_REQUIRE(fsim && fsimc, "fsim/fsimc is NULL");
+        iqm_pair hp{rgba_in, rgba_ref, w, h, row_bytes};
+        check_fsim_args(&hp, 1, precision, energy_mode);
+        auto dev = iqm::upload_pairs(ctx, &hp, 1);
+        auto *d_scores = static_cast<double *>(ctx->scores.get(sizeof(double) * 2, ctx->stream));
+        fsim_enqueue(ctx, dev, energy_mode, d_scores);
+        double out[2];
+        IQM_CHECK_CUDA(cudaMemcpyAsync(out, d_scores, sizeof(out), cudaMemcpyDeviceToHost, ctx->stream));
+        IQM_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+        *fsim = out[0];
+        *fsimc = out[1];
+    });
+}
+
+IQM_API int iqm_fsim_plan_constants(iqm_ctx *ctx, int w2, int h2, int energy_mode, double *em, double *an2,
+                                    double *aiaj) {
+    return iqm::guarded(ctx, [&] {
+        IQM_REQUIRE(w2 >= 2 && h2 >= 2 && w2 <= 4096 && h2 <= 4096, "plane size out of range");
+        IQM_REQUIRE(energy_mode == 0 || energy_mode == 1, "energy_mode must be 0 or 1");
+        IQM_REQUIRE(em && an2 && aiaj, "output pointer is NULL");
+        iqm::FsimPlan *P = get_plan(ctx, w2, h2);
+        for (int o = 0; o < 4; o++) {
+            em[o] = P->em[o];
+            an2[o] = P->an2[energy_mode][o];
+            aiaj[o] = P->aiaj[energy_mode][o];
+        }
+    });
+}

@@ -1,0 +1,73 @@
+"""FSIM / FSIMc on the GPU through the C ABI, against the CPU oracle (FP64 and the
+reference-faithful FP32 build).  Tolerance |delta| <= 1e-5 on both scores."""
+import numpy as np
+import pytest
+
+import iqm_b200
+from iqm_b200 import synth
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+@pytest.mark.parametrize("w2,h2", [(128, 96), (480, 270), (263, 131), (200, 130), (64, 64)])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_plan_constants_match_oracle(rt, o64, w2, h2, mode):
+    em, an2, aiaj = iqm_b200.FSIM(rt, energy_mode=mode).plan_constants(w2, h2)
+    oem, oan2, oaiaj = o64.fsim_constants(w2, h2, energy_full=bool(mode))
+    assert np.allclose(em, oem, rtol=1e-5)
+    assert np.allclose(an2, oan2, rtol=1e-4, atol=1e-6 * np.abs(oan2).max())
+    assert np.allclose(aiaj, oaiaj, rtol=1e-4, atol=1e-6 * np.abs(oan2).max())
+
+
+@pytest.mark.parametrize("h,w", [(96, 128), (130, 200), (270, 480), (600, 800), (1080, 1920), (131, 263), (57, 61)])
+def test_fsim_matches_oracle(rt, o64, o32, h, w):
+    a, b = synth.rgb_gain_pair(h, w, config=1, pair=w % 7)
+    r = iqm_b200.FSIM(rt).compute_metric(a, b)
+    f64, fc64 = o64.fsim(a, b)
+    f32, fc32 = o32.fsim(a, b)
+    assert abs(r.fsim - f64) <= TOL and abs(r.fsimc - fc64) <= TOL, (r, f64, fc64)
+    assert abs(r.fsim - f32) <= TOL and abs(r.fsimc - fc32) <= TOL, (r, f32, fc32)
+
+
+def test_fsim_full_energy_mode(rt, o64):
+    a, b = synth.rgb_gain_pair(200, 260, config=1, pair=3)
+    r = iqm_b200.FSIM(rt, energy_mode=1).compute_metric(a, b)
+    f, fc = o64.fsim(a, b, energy_full=True)
+    assert abs(r.fsim - f) <= TOL and abs(r.fsimc - fc) <= TOL
+
+
+def test_fsim_identical_is_one(rt):
+    a, b = synth.rgb_gain_pair(120, 160, config=1, pair=2)
+    r = iqm_b200.FSIM(rt).compute_metric(b, b)
+    assert r.fsim == pytest.approx(1.0, abs=1e-6) and r.fsimc == pytest.approx(1.0, abs=1e-6)
+
+
+def test_fsim_batch_uneven_matches_single(rt, o64):
+    sizes = [(96, 128), (270, 480), (96, 128), (130, 200), (600, 800)]
+    pairs = [synth.rgb_gain_pair(h, w, config=1, pair=i) for i, (h, w) in enumerate(sizes)]
+    f = iqm_b200.FSIM(rt)
+    got = f.compute_batch(pairs)
+    for (a, b), g in zip(pairs, got):
+        single = f.compute_metric(a, b)
+        assert g[0] == single.fsim and g[1] == single.fsimc
+        w64 = o64.fsim(a, b)
+        assert abs(g[0] - w64[0]) <= TOL and abs(g[1] - w64[1]) <= TOL
+
+
+def test_fsim_deterministic(rt):
+    a, b = synth.rgb_gain_pair(270, 480, config=1, pair=5)
+    f = iqm_b200.FSIM(rt)
+    v = [f.compute_metric(a, b) for _ in range(3)]
+    assert v[0] == v[1] == v[2]
+
+
+def test_fsim_errors(rt):
+    f = iqm_b200.FSIM(rt)
+    a = np.zeros((40, 40, 4), np.uint8)
+    with pytest.raises(iqm_b200.IQMError):
+        f.compute_metric(a, np.zeros((40, 41, 4), np.uint8))
+    f.energy_mode = 3
+    with pytest.raises(iqm_b200.IQMError) as e:
+        f.compute_metric(a, a)
+    assert e.value.code == iqm_b200.IQM_EINVAL
