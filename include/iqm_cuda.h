@@ -75,6 +75,23 @@ void iqm_ssim_default_params(iqm_ssim_params *p);
 int iqm_ssim(iqm_ctx *ctx, const uint8_t *rgba_in, const uint8_t *rgba_ref, int w, int h,
              size_t row_bytes, const iqm_ssim_params *params, float *map_out, double *mssim);
 
+/* Allocation-free SSIM.  This entry point has no counterpart in the reference.  It is for callers
+ * that cannot let a library allocate device memory -- a host application that reserves the whole
+ * GPU for its own allocator, or a plugin host that accounts for every byte it hands out.  It calls
+ * no cudaMalloc/cudaFree and creates no context: the caller passes DEVICE pointers for the two
+ * images (`d_in`, `d_ref`), the score (`d_mssim`, one double) and optionally the map (`d_map`,
+ * w*h floats), plus the stream to run on (NULL = the default stream); the call returns without
+ * synchronising.  The kernel's scratch is a fixed array inside the library (about 33 KB) that every
+ * GPU which loads the library holds until the process exits, so the image may span at most
+ * IQM_SSIM_NOALLOC_MAX_TILES tiles of 128 columns x 122 rows (11-tap window; e.g. 7680x4320 uses
+ * 2160); larger images return IQM_EINVAL.  The first call on a device looks up that array's device
+ * address with the device current, so make it before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU (other streams, other threads) race -- serialise them.
+ * Returns IQM_OK, IQM_EINVAL (null pointer, size or parameter out of range) or IQM_ECUDA. */
+#define IQM_SSIM_NOALLOC_MAX_TILES 4096
+int iqm_ssim_noalloc(const uint8_t *d_in, const uint8_t *d_ref, int w, int h, size_t row_bytes,
+                     const iqm_ssim_params *params, float *d_map, double *d_mssim, void *cuda_stream);
+
 /* ---- M-SVD (src/gpu/svd/svd.h:25-28, src/gpu/svd/svd.cpp:39-164) ----------------------- */
 /* `block_map` (nullable, (w/8)*(h/8) floats) receives D/max(D) (SVDResult::imageData). */
 int iqm_msvd(iqm_ctx *ctx, const uint8_t *rgba_in, const uint8_t *rgba_ref, int w, int h,

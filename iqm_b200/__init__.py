@@ -33,7 +33,7 @@ EXPORTS = (
     "iqm_device_name", "iqm_ssim_default_params", "iqm_ssim", "iqm_msvd", "iqm_flip_default_params",
     "iqm_flip_ppd", "iqm_flip", "iqm_fsim", "iqm_ssim_dev", "iqm_msvd_dev", "iqm_flip_dev",
     "iqm_fsim_dev", "iqm_ssim_batch", "iqm_msvd_batch", "iqm_flip_batch", "iqm_fsim_batch",
-    "iqm_last_launch_count", "iqm_fsim_plan_constants",
+    "iqm_last_launch_count", "iqm_fsim_plan_constants", "iqm_ssim_noalloc",
 )
 
 
@@ -99,6 +99,7 @@ def load_library(path=LIB_PATH):
     L.iqm_fsim_batch.argtypes = [vp, PP, ip, ip, ip, dp]
     L.iqm_last_launch_count.argtypes = [vp]
     L.iqm_fsim_plan_constants.argtypes = [vp, ip, ip, ip, dp, dp, dp]
+    L.iqm_ssim_noalloc.argtypes = [vp, vp, ip, ip, ctypes.c_size_t, ctypes.POINTER(SSIMParams), vp, vp, vp]
     _lib = L
     return L
 

@@ -25,6 +25,7 @@
 //     (deterministic, no second launch).
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "iqm_internal.cuh"
 
@@ -467,4 +468,104 @@ extern "C" __attribute__((visibility("default"))) int iqm_ssim(iqm_ctx *ctx, con
                                            cudaMemcpyDeviceToHost, ctx->stream));
         IQM_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
     });
+}
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free SSIM.  Some callers cannot let a library allocate device memory: a host
+// application that reserves the whole GPU for its own allocator, or a plugin whose host accounts
+// for every byte it hands out.  iqm_ssim_noalloc serves them: the caller passes device inputs and
+// outputs, and the kernel's scratch (pair descriptor, completion counter, per-tile partial sums)
+// lives in the fixed array below, which every GPU that loads this library holds until exit.
+namespace {
+
+struct NoallocScratch {
+    SsimPairDev desc;                                 // the pair of the current call
+    unsigned counter;                                 // CTAs finished; must be 0 at launch
+    double partials[IQM_SSIM_NOALLOC_MAX_TILES];      // one per tile
+};
+
+static __device__ __align__(256) unsigned char g_ssim_noalloc_scratch[sizeof(NoallocScratch)];
+
+// Host-side copies of the array's device address, one per device, filled on the first call made
+// with that device current.  In host code the symbol itself is only a stand-in, not an address.
+constexpr int NOALLOC_MAX_DEVICES = 64;
+void *g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+std::mutex g_noalloc_mu;
+
+// Writes the descriptor and clears the counter (the array keeps the previous call's contents).
+__global__ void ssim_noalloc_setup_kernel(NoallocScratch *s, SsimPairDev d) {
+    s->desc = d;
+    s->counter = 0u;
+}
+
+}  // namespace
+
+extern "C" __attribute__((visibility("default"))) int iqm_ssim_noalloc(
+    const uint8_t *d_in, const uint8_t *d_ref, int w, int h, size_t row_bytes, const iqm_ssim_params *params,
+    float *d_map, double *d_mssim, void *cuda_stream) {
+    if (!d_in || !d_ref || !d_mssim) return IQM_EINVAL;
+    const iqm_ssim_params p = resolve(params);
+    try {
+        check_params(p);
+    } catch (const iqm::Error &e) {
+        return e.code;
+    }
+    const int R = (p.kernel_size - 1) / 2;
+    if (w < 2 * R || h < 2 * R || w > 65536 || h > 65536 || row_bytes < size_t(w) * 4) return IQM_EINVAL;
+    const int tiles_x = int(iqm::ceil_div(w, TW));
+    const long tiles = long(tiles_x) * long(iqm::ceil_div(h, strip_rows(R)));
+    if (tiles > IQM_SSIM_NOALLOC_MAX_TILES) return IQM_EINVAL;
+
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return IQM_ECUDA;
+    void *addr = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void *a = nullptr;
+            if (cudaGetSymbolAddress(&a, g_ssim_noalloc_scratch) != cudaSuccess || !a) {
+                cudaGetLastError();
+                return IQM_ECUDA;
+            }
+            g_noalloc_addr[dev] = a;
+        }
+        addr = g_noalloc_addr[dev];
+    }
+    auto *s = static_cast<NoallocScratch *>(addr);
+    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+
+    SsimPairDev d{};
+    d.a = d_in;
+    d.b = d_ref;
+    d.map = d_map;
+    d.pitch = (long long)row_bytes;
+    d.w = w;
+    d.h = h;
+    d.tiles_x = tiles_x;
+    d.tile_base = 0;
+    d.ntiles = int(tiles);
+    d.vec_ok = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_ref) | uintptr_t(row_bytes)) &
+                15u) == 0;
+    ssim_noalloc_setup_kernel<<<1, 1, 0, st>>>(s, d);
+
+    SsimArgs a{};
+    a.pairs = &s->desc;
+    a.npairs = 1;
+    a.partials = s->partials;
+    a.counters = &s->counter;
+    a.scores = d_mssim;
+    for (int k = 0; k < 15; k++) a.g[k] = 0.f;
+    for (int k = -R; k <= R; k++) a.g[k + R] = float(std::exp(-double(k * k) / (2.0 * double(p.sigma) * p.sigma)));
+    a.c1 = p.k1 * p.k1;
+    a.c2 = p.k2 * p.k2;
+    switch (R) {
+        case 1: launch_ssim<1>(a, int(tiles), st); break;
+        case 2: launch_ssim<2>(a, int(tiles), st); break;
+        case 3: launch_ssim<3>(a, int(tiles), st); break;
+        case 4: launch_ssim<4>(a, int(tiles), st); break;
+        case 5: launch_ssim<5>(a, int(tiles), st); break;
+        case 6: launch_ssim<6>(a, int(tiles), st); break;
+        default: launch_ssim<7>(a, int(tiles), st); break;
+    }
+    return cudaGetLastError() == cudaSuccess ? IQM_OK : IQM_ECUDA;
 }
