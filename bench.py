@@ -15,9 +15,7 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 
 import numpy as np
@@ -85,50 +83,54 @@ def metric_implemented(metric, device=0):
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+    """SM clock and throttle reasons sampled through NVML every few ms during the timed region."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
-    def __init__(self, device):
+    def __init__(self, device, period=0.005):
         self.device = device
-        self.proc = None
-        self.path = None
+        self.period = period
+        self.samples = []
+        self.max_mhz = None
+        self._stop = None
+        self._thread = None
+        self.error = None
 
     def start(self):
+        import threading
         try:
-            fd, self.path = tempfile.mkstemp(suffix=".csv")
-            os.close(fd)
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # no NVML: report it instead of a number
+            self.error = "nvml unavailable: %s" % e
+            return
+        self._stop = threading.Event()
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    mhz = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((mhz, rs))
+                except Exception:
+                    pass
+                self._stop.wait(self.period)
+
+        self._thread = threading.Thread(target=run, daemon=True)
+        self._thread.start()
 
     def stop(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        rows = []
-        for line in open(self.path):
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
-        os.unlink(self.path)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        load = [s for s in sm if mx and s > 0.3 * max(mx)] or sm
-        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        if self._thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.error or "not sampled"]}
+        self._stop.set()
+        self._thread.join()
+        mhz = [m for m, _ in self.samples]
+        reasons = sorted({name for _, r in self.samples for name, bit in self.REASONS.items() if r & bit})
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(mhz)}
 
 
 def cpu_baseline(metric, pairs, seconds, one_pair_only=False):
@@ -137,7 +139,7 @@ def cpu_baseline(metric, pairs, seconds, one_pair_only=False):
     from oracle import Oracle
     o = Oracle("f32")
     fn = {"ssim": lambda a, b: o.ssim(a, b), "fsim": lambda a, b: o.fsim(a, b),
-          "flip": lambda a, b: o.flip(a, b, ppd=67.0), "msvd": lambda a, b: o.msvd(a, b)}[metric]
+          "flip": lambda a, b: o.flip(a, b, ppd=o.flip_ppd(3840.0, 0.7, 0.7)), "msvd": lambda a, b: o.msvd(a, b)}[metric]
     done = 0
     t0 = time.perf_counter()
     while True:
@@ -211,6 +213,7 @@ def main():
     rt.set_stream(stream.cuda_stream)
     obj = {"fsim": iqm_b200.FSIM, "ssim": iqm_b200.SSIM, "flip": iqm_b200.FLIP, "msvd": iqm_b200.SVD}[metric](rt)
     nscore = WORKLOADS[metric][2]
+    flip_args = iqm_b200.FLIPArguments(3840.0, 0.7, 0.7)  # 67.02 pixels per degree
 
     # device-resident batch: B distinct buffers (replicas of the distinct synthetic pairs)
     img_bytes = H1080 * W1080 * 4
@@ -226,7 +229,10 @@ def main():
     dev_pairs = [(base + (2 * i) * img_bytes, base + (2 * i + 1) * img_bytes, W1080, H1080, W1080 * 4) for i in range(B)]
 
     def step():
-        obj.compute_dev(dev_pairs, d_scores.data_ptr())
+        if metric == "flip":
+            obj.compute_dev(dev_pairs, d_scores.data_ptr(), flip_args)
+        else:
+            obj.compute_dev(dev_pairs, d_scores.data_ptr())
 
     for _ in range(max(3, args.warmup)):
         step()
@@ -288,7 +294,7 @@ def main():
         elif metric == "msvd":
             rt.check(L.iqm_msvd_batch(rt.h, arr, B, outp))
         elif metric == "flip":
-            p = iqm_b200.FLIPArguments().c()
+            p = flip_args.c()
             rt.check(L.iqm_flip_batch(rt.h, arr, B, ctypes.byref(p), outp))
         else:
             rt.check(L.iqm_fsim_batch(rt.h, arr, B, obj.precision, obj.energy_mode, outp))

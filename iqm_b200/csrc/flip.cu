@@ -1,0 +1,524 @@
+// FLIP (LDR) on sm_100a.
+//
+// Reference path (cadik/IQM, src/gpu/flip/flip.cpp:121-172, src/gpu/flip/flip_color_pipeline.cpp):
+// nine full-image Vulkan dispatches -- sRGB -> YCxCz, feature-filter creation and (racy, in-place)
+// normalisation, horizontal and vertical feature passes, horizontal and vertical CSF passes with
+// the colour pipeline, colour error, and the combine with a viridis lookup.  The per-pixel value
+// pow(dEc, 1 - dEf) is never read back or pooled (FLIPResult::mean_flip is never set); the score
+// here is its mean.
+//
+// Two kernels:
+//   flip_hpass_kernel  one CTA per 256-pixel row segment of both images: RGBA8 -> linear RGB by a
+//                      256-entry table (the sRGB curve of srgb_to_ycxcz.glsl:22-28 on 8-bit inputs),
+//                      -> XYZ -> YCxCz in shared memory, then the horizontal feature taps (g, edge,
+//                      point on (Y+16)/116, feature_filter_horizontal.glsl) and the horizontal CSF
+//                      taps (spatial_prefilter_horizontal.glsl), clamp-to-edge; 4 pixels per thread;
+//                      12 planes out;
+//   flip_vpass_kernel  32x32-pixel output tiles: the 12 planes (+ halo rows, clamp-to-edge) staged in
+//                      shared memory, vertical feature and CSF taps register-blocked 8 rows per
+//                      thread, then YCxCz -> XYZ -> linear RGB (clamped) -> L*a*b* -> Hunt
+//                      (spatial_prefilter.glsl:74-99), HyAB colour error (spatial_detection.glsl),
+//                      feature error (feature_detection.glsl:48-53), combine
+//                      (combine_error_maps.glsl:28) and FP64 pooling; the last CTA of a pair writes
+//                      the mean.
+// Filter taps depend only on pixels-per-degree: computed on the host in double, normalised once.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "iqm_internal.cuh"
+
+#define GLSL_PI 3.141592653589
+
+namespace {
+
+constexpr int MAXR = 32;          // largest supported filter radius (ppd up to ~235)
+constexpr int MAXT = 2 * MAXR + 1;
+constexpr int HSEG = 256;         // pixels per row segment (hpass)
+constexpr int HT = 64;            // hpass threads (4 pixels each)
+constexpr int VT_COLS = 32, VT_ROWS = 32, VT_RPT = 8;  // vpass tile and rows per thread
+constexpr int VT = VT_COLS * (VT_ROWS / VT_RPT);        // 128 threads
+constexpr int NPLANE = 12;        // per pair: [img][dx, ddx, value, Y, Cx, Cz]
+
+struct FlipTaps {
+    int rf;               // feature radius: taps j in [-rf, rf] use index j + rf
+    int rc;               // CSF radius
+    float feat[3][MAXT];  // g, edge, point (normalised as feature_filter_normalize.glsl)
+    float csf[3][MAXT];   // luma, red-green, blue-yellow weights, each normalised to sum 1
+    float lin[256];       // sRGB byte -> linear
+    float rgb2xyz[9], xyz2rgb[9], white[3];
+    float cmax;           // HyAB(Hunt(green), Hunt(blue))^0.7
+};
+
+struct FlipPairDev {
+    const uint8_t *a;
+    const uint8_t *b;
+    float *map;
+    long long pitch;
+    int w, h;
+    int tiles_x, ntiles, tile_base;
+    int vec_ok;
+    long long plane_off;  // offset (floats) of this pair's 12 planes
+    long long seg_base;   // first hpass segment index of this pair
+};
+
+struct FlipArgs {
+    const FlipPairDev *pairs;
+    int npairs;
+    float *planes;
+    double *partials;
+    unsigned *counters;
+    double *scores;
+    long long total_segs;
+};
+
+__device__ __forceinline__ int find_seg(const FlipPairDev *p, int n, long long s) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (p[mid].seg_base <= s) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+__device__ __forceinline__ int find_tile(const FlipPairDev *p, int n, int t) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (p[mid].tile_base <= t) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __grid_constant__ FlipTaps T) {
+    __shared__ float lin[256];
+    __shared__ float ycc[2][3][HSEG + 2 * MAXR];
+    const long long seg = blockIdx.x;
+    const int pi = find_seg(args.pairs, args.npairs, seg);
+    const FlipPairDev P = args.pairs[pi];
+    const int segs_x = (P.w + HSEG - 1) / HSEG;
+    const long long local = seg - P.seg_base;
+    const int y = int(local / segs_x);
+    const int x0 = int(local % segs_x) * HSEG;
+    const int R = max(T.rf, T.rc);
+    for (int i = threadIdx.x; i < 256; i += HT) lin[i] = T.lin[i];
+    __syncthreads();
+    // stage YCxCz of columns x0-R .. x0+HSEG+R-1 (clamped to the image), both images
+    const int ncols = HSEG + 2 * R;
+    for (int q = threadIdx.x; q < 2 * ncols; q += HT) {
+        const int img = q / ncols, c = q - img * ncols;
+        const int x = min(max(x0 - R + c, 0), P.w - 1);
+        const uint32_t px = __ldg(reinterpret_cast<const uint32_t *>((img ? P.b : P.a) + (long long)y * P.pitch) + x);
+        const float r = lin[px & 0xffu], g = lin[(px >> 8) & 0xffu], b = lin[(px >> 16) & 0xffu];
+        float X = T.rgb2xyz[0] * r + T.rgb2xyz[1] * g + T.rgb2xyz[2] * b;
+        float Y = T.rgb2xyz[3] * r + T.rgb2xyz[4] * g + T.rgb2xyz[5] * b;
+        float Z = T.rgb2xyz[6] * r + T.rgb2xyz[7] * g + T.rgb2xyz[8] * b;
+        X /= T.white[0];
+        Y /= T.white[1];
+        Z /= T.white[2];
+        ycc[img][0][c] = 116.0f * Y - 16.0f;
+        ycc[img][1][c] = 500.0f * (X - Y);
+        ycc[img][2][c] = 200.0f * (Y - Z);
+    }
+    __syncthreads();
+    const int n = P.w * P.h;
+    float *planes = args.planes + P.plane_off;
+    const int xl = 4 * threadIdx.x;  // first of this thread's 4 segment columns
+#pragma unroll 1
+    for (int img = 0; img < 2; img++) {
+        float fa[4][3] = {}, ca[4][3] = {};
+        // output column x = x0 + xl + i reads staged column (x - j) + R - x0 = xl + i - j + R
+        for (int j = -R; j <= R; j++) {
+            const bool uf = j >= -T.rf && j <= T.rf, uc = j >= -T.rc && j <= T.rc;
+            const float wg = uf ? T.feat[0][j + T.rf] : 0.f, we = uf ? T.feat[1][j + T.rf] : 0.f,
+                        wp = uf ? T.feat[2][j + T.rf] : 0.f;
+            const float w0 = uc ? T.csf[0][j + T.rc] : 0.f, w1 = uc ? T.csf[1][j + T.rc] : 0.f,
+                        w2 = uc ? T.csf[2][j + T.rc] : 0.f;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int c = xl + i - j + R;
+                const float Yv = ycc[img][0][c];
+                const float v = (Yv + 16.0f) / 116.0f;
+                fa[i][0] = fmaf(we, v, fa[i][0]);  // dx   (edge)
+                fa[i][1] = fmaf(wp, v, fa[i][1]);  // ddx  (point)
+                fa[i][2] = fmaf(wg, v, fa[i][2]);  // value (gauss)
+                ca[i][0] = fmaf(w0, Yv, ca[i][0]);
+                ca[i][1] = fmaf(w1, ycc[img][1][c], ca[i][1]);
+                ca[i][2] = fmaf(w2, ycc[img][2][c], ca[i][2]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int x = x0 + xl + i;
+            if (x >= P.w) continue;
+            const long long p = (long long)y * P.w + x;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                planes[(long long)(img * 6 + c) * n + p] = fa[i][c];
+                planes[(long long)(img * 6 + 3 + c) * n + p] = ca[i][c];
+            }
+        }
+    }
+}
+
+// L*a*b* of normalised XYZ (shaders/flip/spatial_prefilter.glsl:86-96)
+__device__ __forceinline__ void xyzn_to_lab(float x, float y, float z, float lab[3]) {
+    const float delta = 6.0f / 29.0f, limit = 0.008856f;
+    const float k = 1.0f / (3.0f * delta * delta), o = 4.0f / 29.0f;
+    const float cx = x > limit ? powf(x, 1.0f / 3.0f) : x * k + o;
+    const float cy = y > limit ? powf(y, 1.0f / 3.0f) : y * k + o;
+    const float cz = z > limit ? powf(z, 1.0f / 3.0f) : z * k + o;
+    lab[0] = 116.0f * cy - 16.0f;
+    lab[1] = 500.0f * (cx - cy);
+    lab[2] = 200.0f * (cy - cz);
+}
+
+// filtered YCxCz -> Hunt-adjusted L*a*b* (shaders/flip/spatial_prefilter.glsl:74-99)
+__device__ __forceinline__ void ycxcz_to_hunt_lab(const FlipTaps &T, float Y, float Cx, float Cz, float lab[3]) {
+    const float yy = (Y + 16.0f) / 116.0f, cx = Cx / 500.0f, cz = Cz / 200.0f;
+    const float X = (yy + cx) * T.white[0], Yw = yy * T.white[1], Z = (yy - cz) * T.white[2];
+    float rgb[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const float v = T.xyz2rgb[3 * i] * X + T.xyz2rgb[3 * i + 1] * Yw + T.xyz2rgb[3 * i + 2] * Z;
+        rgb[i] = fminf(fmaxf(v, 0.0f), 1.0f);
+    }
+    float xyz[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+        xyz[i] = (T.rgb2xyz[3 * i] * rgb[0] + T.rgb2xyz[3 * i + 1] * rgb[1] + T.rgb2xyz[3 * i + 2] * rgb[2]) / T.white[i];
+    xyzn_to_lab(xyz[0], xyz[1], xyz[2], lab);
+    lab[1] *= 0.01f * lab[0];
+    lab[2] *= 0.01f * lab[0];
+}
+
+__global__ void __launch_bounds__(VT) flip_vpass_kernel(FlipArgs args, const __grid_constant__ FlipTaps T) {
+    extern __shared__ float vs[];  // [NPLANE][rows][VT_COLS]
+    __shared__ double red[VT / 32];
+    __shared__ int is_last;
+    const int gt = blockIdx.x;
+    const int pi = find_tile(args.pairs, args.npairs, gt);
+    const FlipPairDev P = args.pairs[pi];
+    const int local = gt - P.tile_base;
+    const int x0 = (local % P.tiles_x) * VT_COLS, y0 = (local / P.tiles_x) * VT_ROWS;
+    const int R = max(T.rf, T.rc);
+    const int rows = VT_ROWS + 2 * R;
+    const int n = P.w * P.h;
+    const float *planes = args.planes + P.plane_off;
+    // stage rows y0-R .. y0+VT_ROWS+R-1 (clamped), columns x0 .. x0+31 (clamped)
+    for (int q = threadIdx.x; q < NPLANE * rows * VT_COLS; q += VT) {
+        const int c = q % VT_COLS, r = (q / VT_COLS) % rows, pl = q / (VT_COLS * rows);
+        const int y = min(max(y0 - R + r, 0), P.h - 1), x = min(x0 + c, P.w - 1);
+        vs[(pl * rows + r) * VT_COLS + c] = planes[(long long)pl * n + (long long)y * P.w + x];
+    }
+    __syncthreads();
+    const int c = threadIdx.x % VT_COLS, rg = threadIdx.x / VT_COLS;
+    const int r0 = rg * VT_RPT;  // first output row of this thread within the tile
+    // accumulators per output row: per image d(2), dd(2), csf(3)
+    float acc[VT_RPT][2][7];
+#pragma unroll
+    for (int i = 0; i < VT_RPT; i++)
+#pragma unroll
+        for (int m = 0; m < 2; m++)
+#pragma unroll
+            for (int q = 0; q < 7; q++) acc[i][m][q] = 0.f;
+    // staged row s holds image row y0 - R + s; output row y = y0 + r0 + i reads rows y - k,
+    // k in [-r, r], i.e. s = r0 + i - k + R.
+    for (int s = r0; s <= r0 + VT_RPT - 1 + 2 * R; s++) {
+        float v[2][6];
+#pragma unroll
+        for (int m = 0; m < 2; m++)
+#pragma unroll
+            for (int q = 0; q < 6; q++) v[m][q] = vs[((m * 6 + q) * rows + s) * VT_COLS + c];
+#pragma unroll
+        for (int i = 0; i < VT_RPT; i++) {
+            const int k = r0 + i - s + R;
+            if (k >= -T.rf && k <= T.rf) {
+                const float g = T.feat[0][k + T.rf], e = T.feat[1][k + T.rf], p = T.feat[2][k + T.rf];
+#pragma unroll
+                for (int m = 0; m < 2; m++) {
+                    acc[i][m][0] = fmaf(v[m][0], g, acc[i][m][0]);  // dx * g
+                    acc[i][m][1] = fmaf(v[m][2], e, acc[i][m][1]);  // value * edge
+                    acc[i][m][2] = fmaf(v[m][1], g, acc[i][m][2]);  // ddx * g
+                    acc[i][m][3] = fmaf(v[m][2], p, acc[i][m][3]);  // value * point
+                }
+            }
+            if (k >= -T.rc && k <= T.rc) {
+                const float w0 = T.csf[0][k + T.rc], w1 = T.csf[1][k + T.rc], w2 = T.csf[2][k + T.rc];
+#pragma unroll
+                for (int m = 0; m < 2; m++) {
+                    acc[i][m][4] = fmaf(v[m][3], w0, acc[i][m][4]);
+                    acc[i][m][5] = fmaf(v[m][4], w1, acc[i][m][5]);
+                    acc[i][m][6] = fmaf(v[m][5], w2, acc[i][m][6]);
+                }
+            }
+        }
+    }
+    double dsum = 0.0;
+    const int x = x0 + c;
+#pragma unroll
+    for (int i = 0; i < VT_RPT; i++) {
+        const int y = y0 + r0 + i;
+        if (x >= P.w || y >= P.h) continue;
+        float lab[2][3], dl[2], ddl[2];
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+            dl[m] = sqrtf(acc[i][m][0] * acc[i][m][0] + acc[i][m][1] * acc[i][m][1]);
+            ddl[m] = sqrtf(acc[i][m][2] * acc[i][m][2] + acc[i][m][3] * acc[i][m][3]);
+            ycxcz_to_hunt_lab(T, acc[i][m][4], acc[i][m][5], acc[i][m][6], lab[m]);
+        }
+        // feature error (feature_detection.glsl:48-53)
+        const float ed = fabsf(dl[0] - dl[1]), pd = fabsf(ddl[0] - ddl[1]);
+        const float def = sqrtf(rsqrtf(2.0f) * fmaxf(ed, pd));
+        // colour error (spatial_detection.glsl:67-82)
+        const float d0 = lab[0][0] - lab[1][0], d1 = lab[0][1] - lab[1][1], d2 = lab[0][2] - lab[1][2];
+        const float hy = fabsf(d0) + sqrtf(d1 * d1 + d2 * d2);
+        const float de = powf(hy, 0.7f);
+        const float pcc = 0.4f * T.cmax;
+        const float dec = de < pcc ? (0.95f / pcc) * de : 0.95f + ((de - pcc) / (T.cmax - pcc)) * (1.0f - 0.95f);
+        const float val = powf(dec, 1.0f - def);
+        if (P.map) P.map[(long long)y * P.w + x] = val;
+        dsum += double(val);
+    }
+    for (int d = 16; d > 0; d >>= 1) dsum += __shfl_down_sync(0xffffffffu, dsum, d);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < VT / 32; i++) t += red[i];
+        args.partials[gt] = t;
+        __threadfence();
+        const unsigned prev = atomicAdd(&args.counters[pi], 1u);
+        is_last = prev == unsigned(P.ntiles - 1);
+    }
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    double t = 0.0;
+    for (int i = threadIdx.x; i < P.ntiles; i += VT) t += __ldcg(&args.partials[P.tile_base + i]);
+    for (int d = 16; d > 0; d >>= 1) t += __shfl_down_sync(0xffffffffu, t, d);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < VT / 32; i++) s += red[i];
+        args.scores[pi] = s / double(n);
+        args.counters[pi] = 0u;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// host side
+
+double ppd_of(const iqm_flip_params &p) {  // src/gpu/flip/flip.cpp:125 (float operands)
+    const float f = p.monitor_distance * (p.monitor_resolution_x / p.monitor_width);
+    return double(f) * (M_PI / 180.0);
+}
+
+void make_taps(double ppd, FlipTaps &T) {
+    // feature taps: shaders/flip/feature_filter.glsl:26-37 with the kernel size of flip.cpp:126,
+    // then feature_filter_normalize.glsl:27-46 (positive and negative parts normalised separately)
+    const float ppdf = float(ppd);
+    const int K = 2 * int(std::ceil(3 * 0.5 * 0.082 * ppd)) + 1;
+    const double sd = 0.5 * 0.082 * double(ppdf);
+    const int radius = int(std::ceil(3.0f * float(0.5f * 0.082f * ppdf)));
+    IQM_REQUIRE(K / 2 <= MAXR, "pixels per degree too large for the FLIP filters");
+    T.rf = K / 2;
+    std::vector<double> t[3];
+    for (int c = 0; c < 3; c++) t[c].assign(K, 0.0);
+    double pos[3] = {0, 0, 0}, neg[3] = {0, 0, 0};
+    for (int x = 0; x < K; x++) {
+        const double xc = double(x - radius);
+        const double g = std::exp(-(xc * xc) / (2.0 * sd * sd));
+        t[0][x] = g;
+        t[1][x] = -xc * g;
+        t[2][x] = (xc * xc / (sd * sd) - 1.0) * g;
+        for (int c = 0; c < 3; c++) (t[c][x] > 0 ? pos[c] : neg[c]) += std::fabs(t[c][x]);
+    }
+    for (int c = 0; c < 3; c++)
+        for (int x = 0; x < MAXT; x++)
+            T.feat[c][x] = x < K ? float(t[c][x] > 0 ? t[c][x] / pos[c] : t[c][x] / neg[c]) : 0.f;
+    // CSF taps: shaders/flip/spatial_prefilter_horizontal.glsl:20-61
+    const double pi = GLSL_PI;
+    const int rc = int(std::ceil(3.0f * std::sqrt(0.04f / (2.0f * float(pi) * float(pi))) * ppdf));
+    IQM_REQUIRE(rc <= MAXR, "pixels per degree too large for the FLIP filters");
+    T.rc = rc;
+    const double par[3][4] = {{1.0, 0.0047, 0, 0.00001}, {1.0, 0.0053, 0, 0.00001}, {34.1, 0.04, 13.5, 0.025}};
+    const double dx = 1.0 / double(ppdf);
+    for (int ch = 0; ch < 3; ch++) {
+        std::vector<double> w(2 * rc + 1);
+        double tot = 0;
+        for (int j = -rc; j <= rc; j++) {
+            const double d = (j * dx) * (j * dx);
+            const double* q = par[ch];
+            w[j + rc] = q[0] * std::sqrt(pi / q[1]) * std::exp(-pi * pi * d / q[1]) +
+                        q[2] * std::sqrt(pi / q[3]) * std::exp(-pi * pi * d / q[3]);
+            tot += w[j + rc];
+        }
+        for (int j = 0; j < MAXT; j++) T.csf[ch][j] = j < 2 * rc + 1 ? float(w[j] / tot) : 0.f;
+    }
+    // sRGB -> linear for every byte value (srgb_to_ycxcz.glsl:22-28)
+    for (int i = 0; i < 256; i++) {
+        const float c = float(i) / 255.0f;
+        T.lin[i] = c > 0.04045f ? std::pow((c + 0.055f) / 1.055f, 2.4f) : c / 12.92f;
+    }
+    // RGB_TO_XYZ (srgb_to_ycxcz.glsl:16-20), XYZ_TO_RGB (spatial_prefilter.glsl:20-24): GLSL mat3
+    // is column-major and `v * M` dots v with each column, so row i below is column i there.
+    const double m[9] = {10135552.0 / 24577794, 8788810.0 / 24577794, 4435075.0 / 24577794,
+                         2613072.0 / 12288897, 8788810.0 / 12288897, 887015.0 / 12288897,
+                         1425312.0 / 73733382, 8788810.0 / 73733382, 70074185.0 / 73733382};
+    const double mi[9] = {3.241003275, -1.537398934, -0.498615861, -0.969224334, 1.875930071,
+                          0.041554224, 0.055639423, -0.204011202, 1.057148933};
+    for (int i = 0; i < 9; i++) {
+        T.rgb2xyz[i] = float(m[i]);
+        T.xyz2rgb[i] = float(mi[i]);
+    }
+    for (int i = 0; i < 3; i++) T.white[i] = T.rgb2xyz[3 * i] + T.rgb2xyz[3 * i + 1] + T.rgb2xyz[3 * i + 2];
+    // cmax = HyAB(Hunt(green), Hunt(blue))^0.7 (spatial_detection.glsl:73-81), host double
+    auto lab_of = [&](double r, double g, double b, double lab[3]) {
+        double xyz[3];
+        for (int i = 0; i < 3; i++) xyz[i] = (m[3 * i] * r + m[3 * i + 1] * g + m[3 * i + 2] * b) / double(T.white[i]);
+        const double delta = 6.0 / 29.0, lim = 0.008856;
+        double c[3];
+        for (int i = 0; i < 3; i++) c[i] = xyz[i] > lim ? std::cbrt(xyz[i]) : xyz[i] / (3 * delta * delta) + 4.0 / 29.0;
+        lab[0] = 116 * c[1] - 16;
+        lab[1] = 500 * (c[0] - c[1]) * 0.01 * lab[0];
+        lab[2] = 200 * (c[1] - c[2]) * 0.01 * lab[0];
+    };
+    double lg[3], lb[3];
+    lab_of(0, 1, 0, lg);
+    lab_of(0, 0, 1, lb);
+    const double hy = std::fabs(lg[0] - lb[0]) + std::sqrt((lg[1] - lb[1]) * (lg[1] - lb[1]) + (lg[2] - lb[2]) * (lg[2] - lb[2]));
+    T.cmax = float(std::pow(hy, 0.7));
+}
+
+iqm_flip_params resolve(const iqm_flip_params *p) {
+    iqm_flip_params d;
+    iqm_flip_default_params(&d);
+    return p ? *p : d;
+}
+
+void check_params(const iqm_flip_params &p) {
+    IQM_REQUIRE(std::isfinite(p.monitor_resolution_x) && std::isfinite(p.monitor_distance) &&
+                    std::isfinite(p.monitor_width) && p.monitor_resolution_x > 0 && p.monitor_distance > 0 &&
+                    p.monitor_width > 0,
+                "FLIP monitor parameters must be positive");
+}
+
+void flip_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_flip_params &params,
+                  const std::vector<float *> &maps, double *d_scores) {
+    FlipTaps T{};
+    make_taps(ppd_of(params), T);
+    const int n = int(pairs.size());
+    std::vector<FlipPairDev> hd(n);
+    long long segs = 0, plane_floats = 0;
+    int tiles = 0;
+    for (int i = 0; i < n; i++) {
+        const iqm_pair &q = pairs[i];
+        FlipPairDev &d = hd[i];
+        d.a = q.input;
+        d.b = q.ref;
+        d.map = maps.empty() ? nullptr : maps[i];
+        d.pitch = (long long)q.row_bytes;
+        d.w = q.w;
+        d.h = q.h;
+        d.tiles_x = int(iqm::ceil_div(q.w, VT_COLS));
+        d.ntiles = d.tiles_x * int(iqm::ceil_div(q.h, VT_ROWS));
+        d.tile_base = tiles;
+        d.vec_ok = 0;
+        d.plane_off = plane_floats;
+        d.seg_base = segs;
+        tiles += d.ntiles;
+        segs += (long long)iqm::ceil_div(q.w, HSEG) * q.h;
+        plane_floats += (long long)NPLANE * q.w * q.h;
+    }
+    IQM_REQUIRE(segs < (1LL << 31) && tiles < (1 << 30), "batch too large");
+    auto *d_desc = static_cast<FlipPairDev *>(iqm::upload_bytes(ctx, ctx->desc, hd.data(), sizeof(FlipPairDev) * n));
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t pb = al(sizeof(float) * size_t(plane_floats)), qb = al(sizeof(double) * tiles),
+                 cb = al(sizeof(unsigned) * n);
+    auto *base = static_cast<uint8_t *>(ctx->scratch.get(pb + qb + cb, ctx->stream));
+    FlipArgs a{};
+    a.pairs = d_desc;
+    a.npairs = n;
+    a.planes = reinterpret_cast<float *>(base);
+    a.partials = reinterpret_cast<double *>(base + pb);
+    a.counters = reinterpret_cast<unsigned *>(base + pb + qb);
+    a.scores = d_scores;
+    a.total_segs = segs;
+    IQM_CHECK_CUDA(cudaMemsetAsync(a.counters, 0, sizeof(unsigned) * n, ctx->stream));
+    flip_hpass_kernel<<<unsigned(segs), HT, 0, ctx->stream>>>(a, T);
+    iqm::check_launch(ctx, "flip_hpass_kernel");
+    const int R = std::max(T.rf, T.rc);
+    const size_t smem = sizeof(float) * NPLANE * (VT_ROWS + 2 * R) * VT_COLS;
+    if (smem > 48 * 1024)
+        IQM_CHECK_CUDA(cudaFuncSetAttribute((const void *)flip_vpass_kernel,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    flip_vpass_kernel<<<tiles, VT, smem, ctx->stream>>>(a, T);
+    iqm::check_launch(ctx, "flip_vpass_kernel");
+}
+
+}  // namespace
+
+#define IQM_API extern "C" __attribute__((visibility("default")))
+
+IQM_API void iqm_flip_default_params(iqm_flip_params *p) {
+    if (!p) return;
+    // src/gpu/flip/flip.h:21-25
+    p->monitor_resolution_x = 2560.f;
+    p->monitor_distance = 0.7f;
+    p->monitor_width = 0.6f;
+}
+
+IQM_API double iqm_flip_ppd(const iqm_flip_params *p) { return ppd_of(resolve(p)); }
+
+IQM_API int iqm_flip_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_flip_params *params,
+                         double *d_scores) {
+    return iqm::guarded(ctx, [&] {
+        const iqm_flip_params p = resolve(params);
+        check_params(p);
+        iqm::check_pairs(pairs, n, 1, 1);
+        IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
+        flip_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), p, {}, d_scores);
+    });
+}
+
+IQM_API int iqm_flip_batch(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_flip_params *params,
+                           double *scores) {
+    return iqm::guarded(ctx, [&] {
+        const iqm_flip_params p = resolve(params);
+        check_params(p);
+        iqm::check_pairs(pairs, n, 1, 1);
+        IQM_REQUIRE(scores != nullptr, "scores is NULL");
+        auto dev = iqm::upload_pairs(ctx, pairs, n);
+        auto *d_scores = static_cast<double *>(ctx->scores.get(sizeof(double) * n, ctx->stream));
+        flip_enqueue(ctx, dev, p, {}, d_scores);
+        IQM_CHECK_CUDA(cudaMemcpyAsync(scores, d_scores, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        IQM_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+IQM_API int iqm_flip(iqm_ctx *ctx, const uint8_t *rgba_in, const uint8_t *rgba_ref, int w, int h, size_t row_bytes,
+                     const iqm_flip_params *params, float *err_map, double *mean_flip) {
+    return iqm::guarded(ctx, [&] {
+        const iqm_flip_params p = resolve(params);
+        check_params(p);
+        IQM_REQUIRE(mean_flip != nullptr, "mean_flip is NULL");
+        iqm_pair hp{rgba_in, rgba_ref, w, h, row_bytes};
+        iqm::check_pairs(&hp, 1, 1, 1);
+        auto dev = iqm::upload_pairs(ctx, &hp, 1);
+        auto *d_score = static_cast<double *>(ctx->scores.get(sizeof(double), ctx->stream));
+        std::vector<float *> maps;
+        float *d_map = nullptr;
+        if (err_map) {
+            d_map = static_cast<float *>(ctx->maps.get(sizeof(float) * size_t(w) * h, ctx->stream));
+            maps.push_back(d_map);
+        }
+        flip_enqueue(ctx, dev, p, maps, d_score);
+        IQM_CHECK_CUDA(cudaMemcpyAsync(mean_flip, d_score, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        if (err_map)
+            IQM_CHECK_CUDA(cudaMemcpyAsync(err_map, d_map, sizeof(float) * size_t(w) * h, cudaMemcpyDeviceToHost,
+                                           ctx->stream));
+        IQM_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}

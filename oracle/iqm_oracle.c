@@ -573,9 +573,11 @@ int oracle_fsim(const uint8_t *in, const uint8_t *ref, int w, int h, long row_by
 /* FLIP (LDR)                                                                                   */
 /* ========================================================================================== */
 
-/* src/gpu/flip/flip.cpp:125 */
+/* src/gpu/flip/flip.cpp:125 -- FLIPArguments holds floats (src/gpu/flip/flip.h:21-25), so the first
+ * two operations are float arithmetic; the pi/180 factor is double. */
 double oracle_flip_ppd(double res_x, double distance, double width) {
-    return distance * (res_x / width) * (M_PI / 180.0);
+    float f = (float)distance * ((float)res_x / (float)width);
+    return (double)f * (M_PI / 180.0);
 }
 
 /* GLSL mat3(...) is column-major and `v * M` dots v with each column:
