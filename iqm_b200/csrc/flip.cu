@@ -22,6 +22,9 @@
 //                      (combine_error_maps.glsl:28) and FP64 pooling; the last CTA of a pair writes
 //                      the mean.
 // Filter taps depend only on pixels-per-degree: computed on the host in double, normalised once.
+// Every multiply-add in the per-image arithmetic is an explicit fmaf, so both images of a pair
+// round identically and FLIP(a, a) is exactly 0 (left to the compiler, a*a + b*b may be fused in a
+// different operand order for each image).
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -91,7 +94,7 @@ __device__ __forceinline__ int find_tile(const FlipPairDev *p, int n, int t) {
 
 __global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __grid_constant__ FlipTaps T) {
     __shared__ float lin[256];
-    __shared__ float ycc[2][3][HSEG + 2 * MAXR];
+    __shared__ float ycc[2][4][HSEG + 2 * MAXR];  // Y, Cx, Cz and (Y + 16) / 116
     const long long seg = blockIdx.x;
     const int pi = find_seg(args.pairs, args.npairs, seg);
     const FlipPairDev P = args.pairs[pi];
@@ -109,15 +112,16 @@ __global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __g
         const int x = min(max(x0 - R + c, 0), P.w - 1);
         const uint32_t px = __ldg(reinterpret_cast<const uint32_t *>((img ? P.b : P.a) + (long long)y * P.pitch) + x);
         const float r = lin[px & 0xffu], g = lin[(px >> 8) & 0xffu], b = lin[(px >> 16) & 0xffu];
-        float X = T.rgb2xyz[0] * r + T.rgb2xyz[1] * g + T.rgb2xyz[2] * b;
-        float Y = T.rgb2xyz[3] * r + T.rgb2xyz[4] * g + T.rgb2xyz[5] * b;
-        float Z = T.rgb2xyz[6] * r + T.rgb2xyz[7] * g + T.rgb2xyz[8] * b;
+        float X = fmaf(T.rgb2xyz[0], r, fmaf(T.rgb2xyz[1], g, T.rgb2xyz[2] * b));
+        float Y = fmaf(T.rgb2xyz[3], r, fmaf(T.rgb2xyz[4], g, T.rgb2xyz[5] * b));
+        float Z = fmaf(T.rgb2xyz[6], r, fmaf(T.rgb2xyz[7], g, T.rgb2xyz[8] * b));
         X /= T.white[0];
         Y /= T.white[1];
         Z /= T.white[2];
-        ycc[img][0][c] = 116.0f * Y - 16.0f;
+        ycc[img][0][c] = fmaf(116.0f, Y, -16.0f);
         ycc[img][1][c] = 500.0f * (X - Y);
         ycc[img][2][c] = 200.0f * (Y - Z);
+        ycc[img][3][c] = (ycc[img][0][c] + 16.0f) / 116.0f;
     }
     __syncthreads();
     const int n = P.w * P.h;
@@ -137,7 +141,7 @@ __global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __g
             for (int i = 0; i < 4; i++) {
                 const int c = xl + i - j + R;
                 const float Yv = ycc[img][0][c];
-                const float v = (Yv + 16.0f) / 116.0f;
+                const float v = ycc[img][3][c];
                 fa[i][0] = fmaf(we, v, fa[i][0]);  // dx   (edge)
                 fa[i][1] = fmaf(wp, v, fa[i][1]);  // ddx  (point)
                 fa[i][2] = fmaf(wg, v, fa[i][2]);  // value (gauss)
@@ -164,10 +168,10 @@ __global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __g
 __device__ __forceinline__ void xyzn_to_lab(float x, float y, float z, float lab[3]) {
     const float delta = 6.0f / 29.0f, limit = 0.008856f;
     const float k = 1.0f / (3.0f * delta * delta), o = 4.0f / 29.0f;
-    const float cx = x > limit ? powf(x, 1.0f / 3.0f) : x * k + o;
-    const float cy = y > limit ? powf(y, 1.0f / 3.0f) : y * k + o;
-    const float cz = z > limit ? powf(z, 1.0f / 3.0f) : z * k + o;
-    lab[0] = 116.0f * cy - 16.0f;
+    const float cx = x > limit ? powf(x, 1.0f / 3.0f) : fmaf(x, k, o);
+    const float cy = y > limit ? powf(y, 1.0f / 3.0f) : fmaf(y, k, o);
+    const float cz = z > limit ? powf(z, 1.0f / 3.0f) : fmaf(z, k, o);
+    lab[0] = fmaf(116.0f, cy, -16.0f);
     lab[1] = 500.0f * (cx - cy);
     lab[2] = 200.0f * (cy - cz);
 }
@@ -179,13 +183,14 @@ __device__ __forceinline__ void ycxcz_to_hunt_lab(const FlipTaps &T, float Y, fl
     float rgb[3];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-        const float v = T.xyz2rgb[3 * i] * X + T.xyz2rgb[3 * i + 1] * Yw + T.xyz2rgb[3 * i + 2] * Z;
+        const float v = fmaf(T.xyz2rgb[3 * i], X, fmaf(T.xyz2rgb[3 * i + 1], Yw, T.xyz2rgb[3 * i + 2] * Z));
         rgb[i] = fminf(fmaxf(v, 0.0f), 1.0f);
     }
     float xyz[3];
 #pragma unroll
     for (int i = 0; i < 3; i++)
-        xyz[i] = (T.rgb2xyz[3 * i] * rgb[0] + T.rgb2xyz[3 * i + 1] * rgb[1] + T.rgb2xyz[3 * i + 2] * rgb[2]) / T.white[i];
+        xyz[i] = fmaf(T.rgb2xyz[3 * i], rgb[0], fmaf(T.rgb2xyz[3 * i + 1], rgb[1], T.rgb2xyz[3 * i + 2] * rgb[2])) /
+                 T.white[i];
     xyzn_to_lab(xyz[0], xyz[1], xyz[2], lab);
     lab[1] *= 0.01f * lab[0];
     lab[2] *= 0.01f * lab[0];
@@ -262,8 +267,8 @@ __global__ void __launch_bounds__(VT) flip_vpass_kernel(FlipArgs args, const __g
         float lab[2][3], dl[2], ddl[2];
 #pragma unroll
         for (int m = 0; m < 2; m++) {
-            dl[m] = sqrtf(acc[i][m][0] * acc[i][m][0] + acc[i][m][1] * acc[i][m][1]);
-            ddl[m] = sqrtf(acc[i][m][2] * acc[i][m][2] + acc[i][m][3] * acc[i][m][3]);
+            dl[m] = sqrtf(fmaf(acc[i][m][0], acc[i][m][0], acc[i][m][1] * acc[i][m][1]));
+            ddl[m] = sqrtf(fmaf(acc[i][m][2], acc[i][m][2], acc[i][m][3] * acc[i][m][3]));
             ycxcz_to_hunt_lab(T, acc[i][m][4], acc[i][m][5], acc[i][m][6], lab[m]);
         }
         // feature error (feature_detection.glsl:48-53)
@@ -271,7 +276,7 @@ __global__ void __launch_bounds__(VT) flip_vpass_kernel(FlipArgs args, const __g
         const float def = sqrtf(rsqrtf(2.0f) * fmaxf(ed, pd));
         // colour error (spatial_detection.glsl:67-82)
         const float d0 = lab[0][0] - lab[1][0], d1 = lab[0][1] - lab[1][1], d2 = lab[0][2] - lab[1][2];
-        const float hy = fabsf(d0) + sqrtf(d1 * d1 + d2 * d2);
+        const float hy = fabsf(d0) + sqrtf(fmaf(d1, d1, d2 * d2));
         const float de = powf(hy, 0.7f);
         const float pcc = 0.4f * T.cmax;
         const float dec = de < pcc ? (0.95f / pcc) * de : 0.95f + ((de - pcc) / (T.cmax - pcc)) * (1.0f - 0.95f);
