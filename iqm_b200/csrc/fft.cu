@@ -93,7 +93,13 @@ const FftLen &fft_len(iqm_ctx *ctx, int n) {
     if (factor(n, r)) {
         L.bluestein = 0;
         L.nst = int(r.size());
-        for (int i = 0; i < L.nst; i++) L.radix[i] = r[i];
+        int st = 1;
+        for (int i = 0; i < L.nst; i++) {
+            L.radix[i] = r[i];
+            L.stride[i] = st;
+            L.inv_stride[i] = 1.0f / float(st);
+            st *= r[i];
+        }
     } else {
         L.bluestein = 1;
         L.nst = 0;
@@ -102,7 +108,13 @@ const FftLen &fft_len(iqm_ctx *ctx, int n) {
         L.m = m;
         factor(m, r);
         L.mst = int(r.size());
-        for (int i = 0; i < L.mst; i++) L.mradix[i] = r[i];
+        int st = 1;
+        for (int i = 0; i < L.mst; i++) {
+            L.mradix[i] = r[i];
+            L.mstride[i] = st;
+            L.minv_stride[i] = 1.0f / float(st);
+            st *= r[i];
+        }
         table(mtw, m);
         chirp.resize(n);
         std::vector<std::complex<double>> c(n);

@@ -26,12 +26,16 @@ struct FftLen {
     int n;
     int nst;
     int radix[FFT_MAX_STAGES];
+    int stride[FFT_MAX_STAGES];    // L: product of the earlier radices
+    float inv_stride[FFT_MAX_STAGES];
     const float2 *tw;         // n entries, exp(-2 pi i t / n)
     // Bluestein data (bluestein != 0): x -> c * IFFT_m( FFT_m(c * x) * B ), c = chirp
     int bluestein;
     int m;
     int mst;
     int mradix[FFT_MAX_STAGES];
+    int mstride[FFT_MAX_STAGES];
+    float minv_stride[FFT_MAX_STAGES];
     const float2 *mtw;        // m entries, exp(-2 pi i t / m)
     const float2 *chirp;      // n entries, exp(-pi i t^2 / n)
     const float2 *bfwd;       // m entries, FFT_m(conj chirp, wrapped) / m      (sign -1)
@@ -231,6 +235,106 @@ __device__ inline float2 *fft_run(float2 *a, float2 *b, const FftLen &P, float s
         y[t * stride + j] = cmul(y[t * stride + j], c);
     }
     __syncthreads();
+    return y;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Warp-level engine: one transform per warp, stages separated by __syncwarp only, so the warps of
+// a CTA progress independently.  j / L is computed as floor((j + 0.5) / L) in float: for j < 2^22
+// the rounding error (about (j/L) 2^-23) stays below the 0.5/L distance to the next integer.
+
+template <int P>
+__device__ __forceinline__ void warp_stage(const float2 *in, float2 *out, int n, int L, float invL,
+                                           const float2 *tw, float s) {
+    const int q = n / P;
+    const int twstep = n / (L * P);
+    for (int j = threadIdx.x & 31; j < q; j += 32) {
+        const int jl = __float2int_rz((float(j) + 0.5f) * invL);
+        const int k = j - jl * L;
+        float2 v[P];
+#pragma unroll
+        for (int r = 0; r < P; r++) v[r] = in[j + r * q];
+        if (k != 0) {
+#pragma unroll
+            for (int r = 1; r < P; r++) v[r] = cmul(v[r], tw_at(tw, r * k * twstep, s));
+        }
+        dft_small<P>(v, s);
+        const int base = jl * L * P + k;
+#pragma unroll
+        for (int r = 0; r < P; r++) out[base + r * L] = v[r];
+    }
+}
+
+__device__ __forceinline__ void warp_stage_generic(const float2 *in, float2 *out, int n, int L, float invL, int p,
+                                                   const float2 *tw, float s) {
+    const int q = n / p;
+    const int twstep = n / (L * p);
+    for (int j = threadIdx.x & 31; j < q; j += 32) {
+        const int jl = __float2int_rz((float(j) + 0.5f) * invL);
+        const int k = j - jl * L;
+        const int base = jl * L * p + k;
+        for (int qq = 0; qq < p; qq++) {
+            float2 acc = make_float2(0.f, 0.f);
+            for (int r = 0; r < p; r++) {
+                float2 x = in[j + r * q];
+                if (k != 0 && r != 0) x = cmul(x, tw_at(tw, r * k * twstep, s));
+                const int e = (r * qq) % p;
+                acc = e ? cadd(acc, cmul(x, tw_at(tw, e * q, s))) : cadd(acc, x);
+            }
+            out[base + qq * L] = acc;
+        }
+    }
+}
+
+__device__ inline float2 *warp_stockham(float2 *a, float2 *b, int n, int nst, const int *radix, const int *stride,
+                                        const float *inv_stride, const float2 *tw, float s) {
+    float2 *in = a, *out = b;
+    for (int st = 0; st < nst; st++) {
+        const int p = radix[st], L = stride[st];
+        const float invL = inv_stride[st];
+        __syncwarp();
+        switch (p) {
+            case 2: warp_stage<2>(in, out, n, L, invL, tw, s); break;
+            case 3: warp_stage<3>(in, out, n, L, invL, tw, s); break;
+            case 4: warp_stage<4>(in, out, n, L, invL, tw, s); break;
+            case 5: warp_stage<5>(in, out, n, L, invL, tw, s); break;
+            case 8: warp_stage<8>(in, out, n, L, invL, tw, s); break;
+            default: warp_stage_generic(in, out, n, L, invL, p, tw, s); break;
+        }
+        float2 *t = in;
+        in = out;
+        out = t;
+    }
+    __syncwarp();
+    return in;
+}
+
+// One transform of length P.n held in a[0..n) by the calling warp (b: scratch; both of
+// fft_work_len(P) entries).  Returns the buffer with the unscaled result.
+__device__ inline float2 *fft_warp(float2 *a, float2 *b, const FftLen &P, float s) {
+    if (!P.bluestein) return warp_stockham(a, b, P.n, P.nst, P.radix, P.stride, P.inv_stride, P.tw, s);
+    const int n = P.n, m = P.m, lane = threadIdx.x & 31;
+    __syncwarp();
+    for (int j = lane; j < m; j += 32) {
+        if (j < n) {
+            float2 c = __ldg(P.chirp + j);
+            if (s > 0) c = conjf2(c);
+            a[j] = cmul(a[j], c);
+        } else {
+            a[j] = make_float2(0.f, 0.f);
+        }
+    }
+    float2 *r = warp_stockham(a, b, m, P.mst, P.mradix, P.mstride, P.minv_stride, P.mtw, -1.f);
+    const float2 *B = s < 0 ? P.bfwd : P.binv;
+    for (int j = lane; j < m; j += 32) r[j] = cmul(r[j], __ldg(B + j));
+    float2 *o = (r == a) ? b : a;
+    float2 *y = warp_stockham(r, o, m, P.mst, P.mradix, P.mstride, P.minv_stride, P.mtw, 1.f);
+    for (int j = lane; j < n; j += 32) {
+        float2 c = __ldg(P.chirp + j);
+        if (s > 0) c = conjf2(c);
+        y[j] = cmul(y[j], c);
+    }
+    __syncwarp();
     return y;
 }
 

@@ -22,9 +22,8 @@
 //                      (combine_error_maps.glsl:28) and FP64 pooling; the last CTA of a pair writes
 //                      the mean.
 // Filter taps depend only on pixels-per-degree: computed on the host in double, normalised once.
-// Every multiply-add in the per-image arithmetic is an explicit fmaf, so both images of a pair
-// round identically and FLIP(a, a) is exactly 0 (left to the compiler, a*a + b*b may be fused in a
-// different operand order for each image).
+// Both images go through the same compiled code (the per-pixel colour math is one non-inlined
+// function, the row pass one loop), so identical images give exactly 0.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -196,6 +195,15 @@ __device__ __forceinline__ void ycxcz_to_hunt_lab(const FlipTaps &T, float Y, fl
     lab[2] *= 0.01f * lab[0];
 }
 
+// Everything one image contributes to a pixel, from its filtered sums: gradient and second-derivative
+// magnitudes and the Hunt-adjusted L*a*b* colour.  Not inlined: both images run the one compiled
+// copy, so identical inputs round identically and FLIP(a, a) is exactly 0.
+__device__ __noinline__ void per_image(const FlipTaps &T, const float *acc, float lab[3], float &dl, float &ddl) {
+    dl = sqrtf(fmaf(acc[0], acc[0], acc[1] * acc[1]));
+    ddl = sqrtf(fmaf(acc[2], acc[2], acc[3] * acc[3]));
+    ycxcz_to_hunt_lab(T, acc[4], acc[5], acc[6], lab);
+}
+
 __global__ void __launch_bounds__(VT) flip_vpass_kernel(FlipArgs args, const __grid_constant__ FlipTaps T) {
     extern __shared__ float vs[];  // [NPLANE][rows][VT_COLS]
     __shared__ double red[VT / 32];
@@ -265,12 +273,8 @@ __global__ void __launch_bounds__(VT) flip_vpass_kernel(FlipArgs args, const __g
         const int y = y0 + r0 + i;
         if (x >= P.w || y >= P.h) continue;
         float lab[2][3], dl[2], ddl[2];
-#pragma unroll
-        for (int m = 0; m < 2; m++) {
-            dl[m] = sqrtf(fmaf(acc[i][m][0], acc[i][m][0], acc[i][m][1] * acc[i][m][1]));
-            ddl[m] = sqrtf(fmaf(acc[i][m][2], acc[i][m][2], acc[i][m][3] * acc[i][m][3]));
-            ycxcz_to_hunt_lab(T, acc[i][m][4], acc[i][m][5], acc[i][m][6], lab[m]);
-        }
+        per_image(T, acc[i][0], lab[0], dl[0], ddl[0]);
+        per_image(T, acc[i][1], lab[1], dl[1], ddl[1]);
         // feature error (feature_detection.glsl:48-53)
         const float ed = fabsf(dl[0] - dl[1]), pd = fabsf(ddl[0] - ddl[1]);
         const float def = sqrtf(rsqrtf(2.0f) * fmaxf(ed, pd));

@@ -20,7 +20,10 @@
 //                           three pooled sums in FP64; the last CTA of a pair writes FSIM, FSIMc
 // The 16 filters and the size-only constants (EM_n, EstSumAn2, EstSumAiAj; fsim_filter_noise.glsl,
 // fsim_mult_filters.glsl) are built once per W'xH' with the same kernels and cached on the context.
-// Pairs are processed in chunks whose intermediates fit the 126 MB L2.
+// Schedule per group: ingest and the forward transform for all pairs at once; the two inverse passes
+// in chunks of pairs whose 32 intermediate planes fit the 126 MB L2; noise and final kernels for
+// all pairs at once.  Every transform runs on one warp (fft.cuh warp engine), CTAs hold 1-8 of
+// them, so stages synchronise with __syncwarp only.
 #include <algorithm>
 #include <cmath>
 #include <map>
@@ -65,10 +68,11 @@ struct FsimPairDev {
 struct FsimGroup {
     const FsimPairDev *pairs;
     int G;          // pairs in this launch
+    int pair0;      // group index of the first pair of this launch (inverse-pass chunks)
     int w2, h2, n;
     float *yiq;     // G x 2 x 3 x n   (I, Q, Y)
     float2 *spec;   // G x 2 x n
-    float2 *T;      // G x 2 x 16 x n  (after the column pass of the inverse transform)
+    float2 *T;      // chunk x 2 x 16 x n  (after the column pass of the inverse transform)
     float *amp;     // G x 8 x n       (img*4 + o)
     float *energy;  // G x 8 x n
     float *eo0;     // G x 8 x n       |EO(s=0, o)|^2
@@ -77,7 +81,7 @@ struct FsimGroup {
     unsigned *counters;
     int tiles;
     double *scores;    // 2 per pair: fsim, fsimc
-    const float *filters;
+    const float *filters;  // 16 planes, column-major: filters[z][x * h2 + y]
     const double *consts;
     int energy_mode;
 };
@@ -120,7 +124,7 @@ __global__ void fsim_filters_kernel(float *filters, int w2, int h2) {
         const float dtheta = fabsf(atan2f(ds, dc));
         const float a = expf(-(dtheta * dtheta) / (2.0f * (theta_sigma * theta_sigma)));
 #pragma unroll
-        for (int s = 0; s < 4; s++) filters[(o * 4 + s) * n + p] = lg[s] * a;
+        for (int s = 0; s < 4; s++) filters[(o * 4 + s) * n + x * h2 + y] = lg[s] * a;
     }
 }
 
@@ -147,6 +151,7 @@ __global__ void fsim_em_kernel(const float *filters, int n, double *consts) {
 // ---------------------------------------------------------------------------------------------
 // ingest -- shaders/fsim/fsim_downsample.glsl:21-55: RGB x 255 -> (I, Q, Y), F x F box starting
 // at (x F - F/2, y F - F/2), out-of-image samples contribute 0, divided by F^2 always.
+template <int FF>  // FF = downscale factor when known at compile time, 0 = read it from the pair
 __global__ void __launch_bounds__(FT) fsim_ingest_kernel(FsimGroup g) {
     __shared__ float u8f[256];  // (b / 255) * 255 in float, as the unorm load followed by * 255.0
     for (int i = threadIdx.x; i < 256; i += FT) u8f[i] = __fdiv_rn(float(i), 255.0f) * 255.0f;
@@ -156,16 +161,20 @@ __global__ void __launch_bounds__(FT) fsim_ingest_kernel(FsimGroup g) {
     if (p >= g.n) return;
     const FsimPairDev P = g.pairs[pi];
     const int x = p % g.w2, y = p / g.w2;
-    const int F = P.F;
+    const int F = FF ? FF : P.F;
     const int xs = x * F - F / 2, ys = y * F - F / 2;
     const float scaler = float(F * F);
 #pragma unroll
     for (int img = 0; img < 2; img++) {
         const uint8_t *base = img ? P.b : P.a;
         float sI = 0.f, sQ = 0.f, sY = 0.f;
-        for (int j = xs; j < xs + F; j++) {
+#pragma unroll
+        for (int jj = 0; jj < F; jj++) {  // x outer, y inner, as fsim_downsample.glsl:46-52
+            const int j = xs + jj;
             if (j < 0 || j >= P.w) continue;
-            for (int k = ys; k < ys + F; k++) {
+#pragma unroll
+            for (int kk = 0; kk < F; kk++) {
+                const int k = ys + kk;
                 if (k < 0 || k >= P.h) continue;
                 const uint32_t px = __ldg(reinterpret_cast<const uint32_t *>(base + (long long)k * P.pitch) + j);
                 const float r = u8f[px & 0xffu], gg = u8f[(px >> 8) & 0xffu], b = u8f[(px >> 16) & 0xffu];
@@ -182,152 +191,171 @@ __global__ void __launch_bounds__(FT) fsim_ingest_kernel(FsimGroup g) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// forward transform (src/gpu/fsim/fsim.cpp:270-368: luma as complex (Y, 0), sign -1, unscaled)
-__global__ void __launch_bounds__(FT) fsim_fwd_rows_kernel(FsimGroup g, FftLen L, int rows, int wl) {
+// forward transform (src/gpu/fsim/fsim.cpp:270-368: luma as complex (Y, 0), sign -1, unscaled).
+// One warp per row; rows per CTA = warps per CTA.
+__global__ void __launch_bounds__(FT, 1) fsim_fwd_rows_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl) {
     extern __shared__ float2 sm[];
-    float2 *a = sm, *b = sm + rows * wl;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int plane = blockIdx.y;  // pair*2 + img
-    const int y0 = blockIdx.x * rows;
-    const int nr = min(rows, g.h2 - y0);
-    const float *Y = g.yiq + (size_t(plane) * 3 + 2) * g.n;
-    for (int idx = threadIdx.x; idx < nr * g.w2; idx += FT) {
-        const int r = idx / g.w2, x = idx - r * g.w2;
-        a[r * wl + x] = make_float2(Y[(y0 + r) * g.w2 + x], 0.f);
-    }
-    const float2 *res = iqm::fft_run(a, b, L, -1.f, nr, wl);
-    float2 *S = g.spec + size_t(plane) * g.n;
-    for (int idx = threadIdx.x; idx < nr * g.w2; idx += FT) {
-        const int r = idx / g.w2, x = idx - r * g.w2;
-        S[(y0 + r) * g.w2 + x] = res[r * wl + x];
-    }
+    const int y = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (y >= g.h2) return;  // warp-uniform; no block-wide barrier follows
+    float2 *a = sm + size_t(warp) * 2 * wl, *b = a + wl;
+    const float *Y = g.yiq + (size_t(plane) * 3 + 2) * g.n + size_t(y) * g.w2;
+    for (int x = lane; x < g.w2; x += 32) a[x] = make_float2(Y[x], 0.f);
+    const float2 *res = iqm::fft_warp(a, b, L, -1.f);
+    float2 *S = g.spec + size_t(plane) * g.n + size_t(y) * g.w2;
+    for (int x = lane; x < g.w2; x += 32) S[x] = res[x];
 }
 
-__global__ void __launch_bounds__(FT) fsim_fwd_cols_kernel(FsimGroup g, FftLen L, int cols, int wl) {
+// Column passes: a CTA of nw (power of two) warps owns nw adjacent columns; the column slab is
+// loaded and stored cooperatively (nw*8-byte row segments) and each warp transforms one column.
+__device__ __forceinline__ int slab_parity(float2 *res, float2 *a) { return res == a ? 0 : 1; }
+
+__global__ void __launch_bounds__(FT, 1) fsim_fwd_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int lw) {
     extern __shared__ float2 sm[];
-    float2 *a = sm, *b = sm + cols * wl;
+    __shared__ int parity;
+    const int nw = 1 << lw, warp = threadIdx.x >> 5;
     const int plane = blockIdx.y;
-    const int x0 = blockIdx.x * cols;
-    const int nc = min(cols, g.w2 - x0);
+    const int x0 = blockIdx.x * nw;
+    const int nc = min(nw, g.w2 - x0);
     float2 *S = g.spec + size_t(plane) * g.n;
-    for (int idx = threadIdx.x; idx < nc * g.h2; idx += FT) {
-        const int y = idx / nc, c = idx - y * nc;
-        a[c * wl + y] = S[y * g.w2 + x0 + c];
+    for (int idx = threadIdx.x; idx < nw * g.h2; idx += blockDim.x) {
+        const int c = idx & (nw - 1), y = idx >> lw;
+        if (c < nc) sm[size_t(c) * 2 * wl + y] = S[size_t(y) * g.w2 + x0 + c];
     }
-    const float2 *res = iqm::fft_run(a, b, L, -1.f, nc, wl);
-    for (int idx = threadIdx.x; idx < nc * g.h2; idx += FT) {
-        const int y = idx / nc, c = idx - y * nc;
-        S[y * g.w2 + x0 + c] = res[c * wl + y];
+    __syncthreads();
+    if (warp < nc) {
+        float2 *a = sm + size_t(warp) * 2 * wl;
+        float2 *res = iqm::fft_warp(a, a + wl, L, -1.f);
+        if (warp == 0 && (threadIdx.x & 31) == 0) parity = slab_parity(res, a);
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nw * g.h2; idx += blockDim.x) {
+        const int c = idx & (nw - 1), y = idx >> lw;
+        if (c < nc) S[size_t(y) * g.w2 + x0 + c] = sm[size_t(c) * 2 * wl + parity * wl + y];
     }
 }
 
 // ---------------------------------------------------------------------------------------------
-// inverse transform, pass 1 (along y) of the 16 filtered spectra of one orientation:
+// inverse transform, pass 1 (along y) of the 4 filtered spectra of orientation o:
 // spectrum x H[o*4+s] (fsim_filter_combinations.glsl:53-56), sign +1.  consts_mode uses a
 // spectrum of ones, i.e. transforms the filters themselves (block 0 of the reference's buffer).
-__global__ void __launch_bounds__(FT) fsim_inv_cols_kernel(FsimGroup g, FftLen L, int cols, int wl, int consts_mode) {
+__global__ void __launch_bounds__(FT, 1) fsim_inv_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int lw, int consts_mode) {
     extern __shared__ float2 sm[];
-    float2 *S = sm;                 // cols x h2 spectrum slice
-    float2 *a = sm + cols * g.h2;   // cols x wl
-    float2 *b = a + cols * wl;
+    __shared__ int parity;
+    const int nw = 1 << lw, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int o = blockIdx.y;
-    const int plane = blockIdx.z;  // pair*2 + img (0 in consts mode)
-    const int x0 = blockIdx.x * cols;
-    const int nc = min(cols, g.w2 - x0);
-    const float2 *src = g.spec + size_t(plane) * g.n;
-    for (int idx = threadIdx.x; idx < nc * g.h2; idx += FT) {
-        const int y = idx / nc, c = idx - y * nc;
-        S[c * g.h2 + y] = consts_mode ? make_float2(1.f, 0.f) : src[y * g.w2 + x0 + c];
+    const int plane = blockIdx.z;  // chunk-local pair*2 + img
+    const int x0 = blockIdx.x * nw;
+    const int nc = min(nw, g.w2 - x0);
+    const int h2 = g.h2;
+    float2 *Sl = sm;                          // nw columns x h2 (column-major)
+    float2 *work = sm + size_t(nw) * h2;      // per warp: a, b of wl each
+    const float2 *src = g.spec + size_t(g.pair0 * 2 + plane) * g.n;
+    for (int idx = threadIdx.x; idx < nw * h2; idx += blockDim.x) {
+        const int c = idx & (nw - 1), y = idx >> lw;
+        if (c < nc) Sl[size_t(c) * h2 + y] = consts_mode ? make_float2(1.f, 0.f) : src[size_t(y) * g.w2 + x0 + c];
     }
     __syncthreads();
     for (int s = 0; s < 4; s++) {
         const int z = o * 4 + s;
-        const float *H = g.filters + size_t(z) * g.n;
-        for (int idx = threadIdx.x; idx < nc * g.h2; idx += FT) {
-            const int y = idx / nc, c = idx - y * nc;
-            const float h = __ldg(H + y * g.w2 + x0 + c);
-            const float2 v = S[c * g.h2 + y];
-            a[c * wl + y] = make_float2(h * v.x, h * v.y);
+        if (warp < nc) {
+            float2 *a = work + size_t(warp) * 2 * wl;
+            const float *H = g.filters + size_t(z) * g.n + size_t(x0 + warp) * h2;
+            const float2 *col = Sl + size_t(warp) * h2;
+            for (int y = lane; y < h2; y += 32) {
+                const float hv = __ldg(H + y);
+                const float2 v = col[y];
+                a[y] = make_float2(hv * v.x, hv * v.y);
+            }
+            float2 *res = iqm::fft_warp(a, a + wl, L, 1.f);
+            if (warp == 0 && lane == 0) parity = slab_parity(res, a);
         }
-        const float2 *res = iqm::fft_run(a, b, L, 1.f, nc, wl);
+        __syncthreads();
         float2 *dst = g.T + (size_t(plane) * 16 + z) * g.n;
-        for (int idx = threadIdx.x; idx < nc * g.h2; idx += FT) {
-            const int y = idx / nc, c = idx - y * nc;
-            dst[y * g.w2 + x0 + c] = res[c * wl + y];
+        for (int idx = threadIdx.x; idx < nw * h2; idx += blockDim.x) {
+            const int c = idx & (nw - 1), y = idx >> lw;
+            if (c < nc) dst[size_t(y) * g.w2 + x0 + c] = work[size_t(c) * 2 * wl + parity * wl + y];
         }
         __syncthreads();
     }
 }
 
-// inverse transform, pass 2 (along x) of the 4 scales of orientation o for one row, scaled 1/N,
-// then per pixel (shaders/fsim/fsim_sum_filter_responses.glsl:43-80):
-//   sumAn = sum_s |EO_s|;  (MeanE, MeanO) = (sum E, sum O) / (|(sum E, sum O)| + 1e-4)
-//   Energy = sum_s E MeanE + O MeanO - |E MeanO - O MeanE|
-// and |EO_0|^2 for the noise median (shaders/fsim/fsim_pack_for_median.glsl:39-43).
-// consts_mode instead accumulates, per row, sum_s Re_s^2 N and sum_{i<j} Re_i Re_j N
+// Per-pixel response sums of one orientation from its 4 scales (scaled by 1/N here), as
+// shaders/fsim/fsim_sum_filter_responses.glsl:43-80 and fsim_pack_for_median.glsl:39-43.
+__device__ __forceinline__ void response_sums(const float2 v[4], float invN, float &sA, float &en, float &e0) {
+    float re[4], im[4];
+    float sE = 0.f, sO = 0.f;
+    sA = 0.f;
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+        re[s] = v[s].x * invN;
+        im[s] = v[s].y * invN;
+        sA += sqrtf(re[s] * re[s] + im[s] * im[s]);
+        sE += re[s];
+        sO += im[s];
+    }
+    const float xe = sqrtf(sE * sE + sO * sO) + 0.0001f;
+    const float mE = sE / xe, mO = sO / xe;
+    en = 0.f;
+#pragma unroll
+    for (int s = 0; s < 4; s++) en += re[s] * mE + im[s] * mO - fabsf(re[s] * mO - im[s] * mE);
+    e0 = re[0] * re[0] + im[0] * im[0];
+}
+
+// inverse transform, pass 2 (along x): warp (r, s) of a CTA transforms row y0 + r, scale s.
+// consts_mode (rr = 1) instead accumulates, per row, sum_s Re_s^2 N and sum_{i<j} Re_i Re_j N
 // (shaders/fsim/fsim_mult_filters.glsl:37-58) over p < ceil(N/2) and over all p.
-__global__ void __launch_bounds__(FT) fsim_inv_rows_kernel(FsimGroup g, FftLen L, int wl, int seq,
-                                                           int consts_mode, double *rowsums) {
+__global__ void __launch_bounds__(FT, 1) fsim_inv_rows_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int rr, int consts_mode,
+                                                           double *rowsums) {
     extern __shared__ float2 sm[];
-    const int y = blockIdx.x, o = blockIdx.y, plane = blockIdx.z;
+    __shared__ int parity;
+    __shared__ double red[4][FT / 32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = warp >> 2, s = warp & 3;
+    const int o = blockIdx.y, plane = blockIdx.z;  // plane: chunk-local pair*2 + img
     const int w2 = g.w2;
-    const float2 *src = g.T + (size_t(plane) * 16 + o * 4) * g.n + size_t(y) * w2;
-    float2 *keep;  // 4 x w2 results
-    if (!seq) {
-        float2 *a = sm, *b = sm + 4 * wl;
-        for (int idx = threadIdx.x; idx < 4 * w2; idx += FT) {
-            const int s = idx / w2, x = idx - s * w2;
-            a[s * wl + x] = src[size_t(s) * g.n + x];
-        }
-        float2 *res = iqm::fft_run(a, b, L, 1.f, 4, wl);
-        // compact to stride w2 is unnecessary: index with stride wl below
-        keep = res;
-    } else {
-        keep = sm;                      // 4 x w2
-        float2 *a = sm + 4 * w2, *b = a + wl;
-        for (int s = 0; s < 4; s++) {
-            for (int x = threadIdx.x; x < w2; x += FT) a[x] = src[size_t(s) * g.n + x];
-            const float2 *res = iqm::fft_run(a, b, L, 1.f, 1, wl);
-            for (int x = threadIdx.x; x < w2; x += FT) keep[s * w2 + x] = res[x];
-            __syncthreads();
+    const int y0 = blockIdx.x * rr;
+    {
+        const int y = y0 + r;
+        if (r < rr && y < g.h2) {
+            float2 *a = sm + size_t(warp) * 2 * wl;
+            const float2 *src = g.T + (size_t(plane) * 16 + o * 4 + s) * g.n + size_t(y) * w2;
+            for (int x = lane; x < w2; x += 32) a[x] = src[x];
+            float2 *res = iqm::fft_warp(a, a + wl, L, 1.f);
+            if (warp == 0 && lane == 0) parity = slab_parity(res, a);
         }
     }
-    const int ks = seq ? w2 : wl;
+    __syncthreads();
     const float invN = 1.0f / float(g.n);
     if (!consts_mode) {
-        const size_t off = (size_t(plane) * 4 + o) * g.n + size_t(y) * w2;
-        for (int x = threadIdx.x; x < w2; x += FT) {
-            float re[4], im[4];
-            float sA = 0.f, sE = 0.f, sO = 0.f;
+        const int gp = g.pair0 * 2 + plane;
+        for (int idx = threadIdx.x; idx < rr * w2; idx += blockDim.x) {
+            const int rl = idx / w2, x = idx - rl * w2;
+            const int y = y0 + rl;
+            if (y >= g.h2) continue;
+            float2 v[4];
 #pragma unroll
-            for (int s = 0; s < 4; s++) {
-                const float2 v = keep[s * ks + x];
-                re[s] = v.x * invN;
-                im[s] = v.y * invN;
-                sA += sqrtf(re[s] * re[s] + im[s] * im[s]);
-                sE += re[s];
-                sO += im[s];
-            }
-            const float xe = sqrtf(sE * sE + sO * sO) + 0.0001f;
-            const float mE = sE / xe, mO = sO / xe;
-            float en = 0.f;
-#pragma unroll
-            for (int s = 0; s < 4; s++) en += re[s] * mE + im[s] * mO - fabsf(re[s] * mO - im[s] * mE);
-            g.amp[off + x] = sA;
-            g.energy[off + x] = en;
-            g.eo0[off + x] = re[0] * re[0] + im[0] * im[0];
+            for (int q = 0; q < 4; q++) v[q] = sm[size_t(rl * 4 + q) * 2 * wl + parity * wl + x];
+            float sA, en, e0;
+            response_sums(v, invN, sA, en, e0);
+            const size_t off = (size_t(gp) * 4 + o) * g.n + size_t(y) * w2 + x;
+            g.amp[off] = sA;
+            g.energy[off] = en;
+            g.eo0[off] = e0;
         }
     } else {
-        __shared__ double red[4][FT / 32];
+        const int y = y0;  // rr == 1
         const long lim = (long(g.n) + 1) / 2;
         const float fn = float(g.n);
         double acc[4] = {0.0, 0.0, 0.0, 0.0};  // an2 (ref), aiaj (ref), an2 (full), aiaj (full)
-        for (int x = threadIdx.x; x < w2; x += FT) {
+        for (int x = threadIdx.x; x < w2; x += blockDim.x) {
             float re[4];
 #pragma unroll
-            for (int s = 0; s < 4; s++) re[s] = keep[s * ks + x].x * invN;
+            for (int q = 0; q < 4; q++) re[q] = sm[size_t(q) * 2 * wl + parity * wl + x].x * invN;
             float q2 = 0.f, qx = 0.f;
 #pragma unroll
-            for (int s = 0; s < 4; s++) q2 += (re[s] * re[s]) * fn;
+            for (int q = 0; q < 4; q++) q2 += (re[q] * re[q]) * fn;
 #pragma unroll
             for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -340,18 +368,87 @@ __global__ void __launch_bounds__(FT) fsim_inv_rows_kernel(FsimGroup g, FftLen L
             acc[2] += q2;
             acc[3] += qx;
         }
+        const int nw = blockDim.x >> 5;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             double v = acc[q];
             for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
-            if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = v;
+            if (lane == 0) red[q][warp] = v;
         }
         __syncthreads();
         if (threadIdx.x < 4) {
             double t = 0.0;
-            for (int i = 0; i < FT / 32; i++) t += red[threadIdx.x][i];
+            for (int i = 0; i < nw; i++) t += red[threadIdx.x][i];
             rowsums[(size_t(o) * g.h2 + y) * 4 + threadIdx.x] = t;
         }
+    }
+}
+
+// Sequential form of pass 2 for rows too long for four warp buffers (Bluestein lengths): the whole
+// CTA transforms one scale at a time with the block-level engine.
+__global__ void __launch_bounds__(FT, 1) fsim_inv_rows_seq_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int consts_mode,
+                                                               double *rowsums) {
+    extern __shared__ float2 sm[];
+    __shared__ double red[4][FT / 32];
+    const int y = blockIdx.x, o = blockIdx.y, plane = blockIdx.z;
+    const int w2 = g.w2;
+    const float2 *src = g.T + (size_t(plane) * 16 + o * 4) * g.n + size_t(y) * w2;
+    float2 *keep = sm;  // 4 x w2
+    float2 *a = sm + 4 * w2, *b = a + wl;
+    for (int s = 0; s < 4; s++) {
+        for (int x = threadIdx.x; x < w2; x += FT) a[x] = src[size_t(s) * g.n + x];
+        const float2 *res = iqm::fft_run(a, b, L, 1.f, 1, wl);
+        for (int x = threadIdx.x; x < w2; x += FT) keep[s * w2 + x] = res[x];
+        __syncthreads();
+    }
+    const float invN = 1.0f / float(g.n);
+    if (!consts_mode) {
+        const size_t off = (size_t(g.pair0 * 2 + plane) * 4 + o) * g.n + size_t(y) * w2;
+        for (int x = threadIdx.x; x < w2; x += FT) {
+            float2 v[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) v[q] = keep[q * w2 + x];
+            float sA, en, e0;
+            response_sums(v, invN, sA, en, e0);
+            g.amp[off + x] = sA;
+            g.energy[off + x] = en;
+            g.eo0[off + x] = e0;
+        }
+        return;
+    }
+    const long lim = (long(g.n) + 1) / 2;
+    const float fn = float(g.n);
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int x = threadIdx.x; x < w2; x += FT) {
+        float re[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) re[q] = keep[q * w2 + x].x * invN;
+        float q2 = 0.f, qx = 0.f;
+#pragma unroll
+        for (int q = 0; q < 4; q++) q2 += (re[q] * re[q]) * fn;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = i + 1; j < 4; j++) qx += re[i] * re[j] * fn;
+        const long p = long(y) * w2 + x;
+        if (p < lim) {
+            acc[0] += q2;
+            acc[1] += qx;
+        }
+        acc[2] += q2;
+        acc[3] += qx;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        double v = acc[q];
+        for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
+        if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double t = 0.0;
+        for (int i = 0; i < FT / 32; i++) t += red[threadIdx.x][i];
+        rowsums[(size_t(o) * g.h2 + y) * 4 + threadIdx.x] = t;
     }
 }
 
@@ -477,17 +574,27 @@ __global__ void __launch_bounds__(FT) fsim_final_kernel(FsimGroup g) {
     __syncthreads();
     if (!is_last) return;
     __threadfence();
-    if (threadIdx.x < 3) {
-        double t = 0.0;
+    {
+        double t[3] = {0.0, 0.0, 0.0};
         const double *pp = g.partials + size_t(pi) * g.tiles * 3;
-        for (int i = 0; i < g.tiles; i++) t += __ldcg(pp + size_t(i) * 3 + threadIdx.x);
-        red[threadIdx.x][0] = t;
+        for (int i = threadIdx.x; i < g.tiles; i += FT)
+#pragma unroll
+            for (int q = 0; q < 3; q++) t[q] += __ldcg(pp + size_t(i) * 3 + q);
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            for (int d = 16; d > 0; d >>= 1) t[q] += __shfl_down_sync(0xffffffffu, t[q], d);
+            if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = t[q];
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
+        double tot[3] = {0.0, 0.0, 0.0};
+        for (int i = 0; i < FT / 32; i++)
+            for (int q = 0; q < 3; q++) tot[q] += red[q][i];
         const int out = g.pairs[pi].out;
-        g.scores[2 * out] = red[1][0] / red[0][0];
-        g.scores[2 * out + 1] = red[2][0] / red[0][0];
+        g.scores[2 * out] = tot[1] / tot[0];
+        g.scores[2 * out + 1] = tot[2] / tot[0];
         g.counters[pi] = 0u;
     }
 }
@@ -512,36 +619,76 @@ void set_smem(const void *fn, size_t bytes) {
         IQM_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
 }
 
+// Launch shapes of the transform kernels for one plane size.
 struct Shapes {
-    int rows_fwd, cols_fwd, cols_inv, seq_rows;
-    size_t sm_rows_fwd, sm_cols_fwd, sm_cols_inv, sm_rows_inv;
+    int wl_row, wl_col;   // work lengths (n, or Bluestein m)
+    int lw_rows;          // log2 warps (rows) per CTA, forward rows
+    int lw_fcols;         // log2 warps (columns) per CTA, forward columns
+    int lw_icols;         // log2 warps (columns) per CTA, inverse columns
+    int rr;               // rows per CTA in the inverse row pass (0: sequential kernel)
+    size_t sm_rows, sm_fcols, sm_icols, sm_irows;
 };
+
+int lw_fit(size_t per_warp, size_t fixed_per_warp = 0) {
+    int lw = 3;  // up to 8 warps
+    while (lw > 0 && (size_t(1) << lw) * (per_warp + fixed_per_warp) > 160 * 1024) lw--;
+    return lw;
+}
 
 Shapes shapes_for(const iqm::FsimPlan &P) {
     Shapes s{};
-    const int wlr = iqm::fft_work_len(P.row), wlc = iqm::fft_work_len(P.col);
     const size_t f2 = sizeof(float2);
-    auto round8 = [](int c) { return c >= 8 ? c & ~7 : c; };  // whole 64-byte row segments
-    s.rows_fwd = std::max(1, std::min(8, int((64 * 1024) / (2 * wlr * f2))));
-    s.sm_rows_fwd = 2 * size_t(s.rows_fwd) * wlr * f2;
-    s.cols_fwd = round8(std::max(1, std::min(16, int((64 * 1024) / (2 * wlc * f2)))));
-    s.sm_cols_fwd = 2 * size_t(s.cols_fwd) * wlc * f2;
-    s.cols_inv = round8(std::max(1, std::min(16, int((96 * 1024) / ((P.h2 + 2 * wlc) * f2)))));
-    s.sm_cols_inv = size_t(s.cols_inv) * (P.h2 + 2 * wlc) * f2;
-    const size_t batch4 = 2 * 4 * size_t(wlr) * f2;
-    s.seq_rows = batch4 > 160 * 1024 ? 1 : 0;
-    s.sm_rows_inv = s.seq_rows ? (4 * size_t(P.w2) + 2 * wlr) * f2 : batch4;
-    IQM_REQUIRE(s.sm_rows_fwd <= SMEM_CAP && s.sm_cols_fwd <= SMEM_CAP && s.sm_cols_inv <= SMEM_CAP &&
-                    s.sm_rows_inv <= SMEM_CAP,
+    s.wl_row = iqm::fft_work_len(P.row);
+    s.wl_col = iqm::fft_work_len(P.col);
+    s.lw_rows = lw_fit(2 * size_t(s.wl_row) * f2);
+    s.sm_rows = (size_t(1) << s.lw_rows) * 2 * s.wl_row * f2;
+    s.lw_fcols = lw_fit(2 * size_t(s.wl_col) * f2);
+    s.sm_fcols = (size_t(1) << s.lw_fcols) * 2 * s.wl_col * f2;
+    s.lw_icols = lw_fit((2 * size_t(s.wl_col) + P.h2) * f2);
+    s.sm_icols = (size_t(1) << s.lw_icols) * (2 * size_t(s.wl_col) + P.h2) * f2;
+    const size_t per_row = 4 * 2 * size_t(s.wl_row) * f2;
+    if (2 * per_row <= 120 * 1024) {
+        s.rr = 2;
+    } else if (per_row <= SMEM_CAP) {
+        s.rr = 1;
+    } else {
+        s.rr = 0;
+    }
+    s.sm_irows = s.rr ? s.rr * per_row : (4 * size_t(P.w2) + 2 * s.wl_row) * f2;
+    IQM_REQUIRE(s.sm_rows <= SMEM_CAP && s.sm_fcols <= SMEM_CAP && s.sm_icols <= SMEM_CAP && s.sm_irows <= SMEM_CAP,
                 "FSIM plane too large for the shared-memory FFT");
     return s;
 }
 
 void configure_kernels(const Shapes &s) {
-    set_smem((const void *)fsim_fwd_rows_kernel, s.sm_rows_fwd);
-    set_smem((const void *)fsim_fwd_cols_kernel, s.sm_cols_fwd);
-    set_smem((const void *)fsim_inv_cols_kernel, s.sm_cols_inv);
-    set_smem((const void *)fsim_inv_rows_kernel, s.sm_rows_inv);
+    set_smem((const void *)fsim_fwd_rows_kernel, s.sm_rows);
+    set_smem((const void *)fsim_fwd_cols_kernel, s.sm_fcols);
+    set_smem((const void *)fsim_inv_cols_kernel, s.sm_icols);
+    if (s.rr) {
+        set_smem((const void *)fsim_inv_rows_kernel, s.sm_irows);
+    } else {
+        set_smem((const void *)fsim_inv_rows_seq_kernel, s.sm_irows);
+    }
+}
+
+void launch_inv_rows(const FsimGroup &g, const iqm::FsimPlan &P, const Shapes &s, int planes, int consts_mode,
+                     double *rowsums, cudaStream_t st) {
+    if (s.rr && !(consts_mode && s.rr != 1)) {
+        fsim_inv_rows_kernel<<<dim3(iqm::ceil_div(P.h2, s.rr), 4, planes), 128 * s.rr, s.sm_irows, st>>>(
+            g, P.row, s.wl_row, s.rr, consts_mode, rowsums);
+    } else if (s.rr) {  // consts mode runs one row per CTA
+        fsim_inv_rows_kernel<<<dim3(P.h2, 4, planes), 128, s.sm_irows / s.rr, st>>>(g, P.row, s.wl_row, 1, 1, rowsums);
+    } else {
+        fsim_inv_rows_seq_kernel<<<dim3(P.h2, 4, planes), FT, s.sm_irows, st>>>(g, P.row, s.wl_row, consts_mode,
+                                                                                 rowsums);
+    }
+}
+
+void launch_inv_cols(const FsimGroup &g, const iqm::FsimPlan &P, const Shapes &s, int planes, int consts_mode,
+                     cudaStream_t st) {
+    const int nw = 1 << s.lw_icols;
+    fsim_inv_cols_kernel<<<dim3(iqm::ceil_div(P.w2, nw), 4, planes), 32 * nw, s.sm_icols, st>>>(
+        g, P.col, s.wl_col, s.lw_icols, consts_mode);
 }
 
 iqm::FsimPlan *get_plan(iqm_ctx *ctx, int w2, int h2) {
@@ -578,11 +725,9 @@ iqm::FsimPlan *get_plan(iqm_ctx *ctx, int w2, int h2) {
         g.T = static_cast<float2 *>(tmp);
         g.filters = P->filters;
         double *rowsums = reinterpret_cast<double *>(static_cast<uint8_t *>(tmp) + tbytes);
-        const int wlr = iqm::fft_work_len(P->row), wlc = iqm::fft_work_len(P->col);
-        fsim_inv_cols_kernel<<<dim3(iqm::ceil_div(w2, s.cols_inv), 4, 1), FT, s.sm_cols_inv, st>>>(g, P->col, s.cols_inv,
-                                                                                                  wlc, 1);
+        launch_inv_cols(g, *P, s, 1, 1, st);
         IQM_CHECK_CUDA(cudaGetLastError());
-        fsim_inv_rows_kernel<<<dim3(h2, 4, 1), FT, s.sm_rows_inv, st>>>(g, P->row, wlr, s.seq_rows, 1, rowsums);
+        launch_inv_rows(g, *P, s, 1, 1, rowsums, st);
         IQM_CHECK_CUDA(cudaGetLastError());
         fsim_consts_reduce_kernel<<<1, 32, 0, st>>>(rowsums, h2, P->consts);
         IQM_CHECK_CUDA(cudaGetLastError());
@@ -611,19 +756,31 @@ struct Layout {
     size_t yiq, spec, T, planes, thr, partials, counters, total;
 };
 
-Layout layout_for(int G, int n, int tiles) {
+// G pairs of the group; chunk pairs' worth of inverse-pass intermediates.
+Layout layout_for(int G, int chunk, int n, int tiles) {
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     Layout L{};
     size_t off = 0;
     L.yiq = off; off += al(sizeof(float) * size_t(G) * 6 * n);
     L.spec = off; off += al(sizeof(float2) * size_t(G) * 2 * n);
-    L.T = off; off += al(sizeof(float2) * size_t(G) * 32 * n);
+    L.T = off; off += al(sizeof(float2) * size_t(chunk) * 32 * n);
     L.planes = off; off += al(sizeof(float) * size_t(G) * 24 * n);
     L.thr = off; off += al(sizeof(float) * size_t(G) * 8);
     L.partials = off; off += al(sizeof(double) * size_t(G) * tiles * 3);
     L.counters = off; off += al(sizeof(unsigned) * size_t(G));
     L.total = off;
     return L;
+}
+
+void launch_ingest(const FsimGroup &g, int F_uniform, int tiles, cudaStream_t st) {
+    const dim3 grid(tiles, g.G);
+    switch (F_uniform) {
+        case 1: fsim_ingest_kernel<1><<<grid, FT, 0, st>>>(g); break;
+        case 2: fsim_ingest_kernel<2><<<grid, FT, 0, st>>>(g); break;
+        case 4: fsim_ingest_kernel<4><<<grid, FT, 0, st>>>(g); break;
+        case 8: fsim_ingest_kernel<8><<<grid, FT, 0, st>>>(g); break;
+        default: fsim_ingest_kernel<0><<<grid, FT, 0, st>>>(g); break;
+    }
 }
 
 // Enqueue FSIM for device-resident pairs; scores[2*i], scores[2*i+1] = FSIM, FSIMc of pair i.
@@ -641,72 +798,81 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
         groups[{w2, h2}].push_back(i);
         hd[i] = FsimPairDev{q.input, q.ref, (long long)q.row_bytes, q.w, q.h, F, i};
     }
-    // descriptors ordered group by group
     std::vector<FsimPairDev> ordered;
     ordered.reserve(n_pairs);
     for (auto &kv : groups)
         for (int i : kv.second) ordered.push_back(hd[i]);
     auto *d_desc = static_cast<FsimPairDev *>(
         iqm::upload_bytes(ctx, ctx->desc, ordered.data(), sizeof(FsimPairDev) * n_pairs));
+    // scratch for the largest group layout
+    size_t need = 0;
+    for (auto &kv : groups) {
+        const int n = kv.first.first * kv.first.second;
+        const int G = int(kv.second.size());
+        const int chunk = std::max(1, std::min(G, int((80ull << 20) / (sizeof(float2) * 32 * size_t(n)))));
+        need = std::max(need, layout_for(G, chunk, n, int(iqm::ceil_div(n, FT))).total);
+    }
+    auto *base = static_cast<uint8_t *>(ctx->scratch.get(need, ctx->stream));
+    cudaStream_t st = ctx->stream;
     size_t first = 0;
     for (auto &kv : groups) {
         const int w2 = kv.first.first, h2 = kv.first.second;
-        const int Gtot = int(kv.second.size());
+        const int G = int(kv.second.size());
         iqm::FsimPlan *P = get_plan(ctx, w2, h2);
         const Shapes s = shapes_for(*P);
         configure_kernels(s);
         const int n = P->n;
         const int tiles = int(iqm::ceil_div(n, FT));
-        // chunk so that one chunk's intermediates (~400 bytes per plane pixel) stay in L2
-        const size_t per_pair = layout_for(1, n, tiles).total;
-        const int chunk = std::max(1, std::min(Gtot, int((96ull << 20) / per_pair)));
-        const Layout Lc = layout_for(chunk, n, tiles);
-        auto *base = static_cast<uint8_t *>(ctx->scratch.get(Lc.total, ctx->stream));
-        const int wlr = iqm::fft_work_len(P->row), wlc = iqm::fft_work_len(P->col);
-        for (int c0 = 0; c0 < Gtot; c0 += chunk) {
-            const int G = std::min(chunk, Gtot - c0);
-            FsimGroup g{};
-            g.pairs = d_desc + first + c0;
-            g.G = G;
-            g.w2 = w2;
-            g.h2 = h2;
-            g.n = n;
-            g.yiq = reinterpret_cast<float *>(base + Lc.yiq);
-            g.spec = reinterpret_cast<float2 *>(base + Lc.spec);
-            g.T = reinterpret_cast<float2 *>(base + Lc.T);
-            g.amp = reinterpret_cast<float *>(base + Lc.planes);
-            g.energy = g.amp + size_t(G) * 8 * n;
-            g.eo0 = g.energy + size_t(G) * 8 * n;
-            g.thr = reinterpret_cast<float *>(base + Lc.thr);
-            g.partials = reinterpret_cast<double *>(base + Lc.partials);
-            g.counters = reinterpret_cast<unsigned *>(base + Lc.counters);
-            g.tiles = tiles;
-            g.scores = d_scores;
-            g.filters = P->filters;
-            g.consts = P->consts;
-            g.energy_mode = energy_mode;
-            cudaStream_t st = ctx->stream;
-            IQM_CHECK_CUDA(cudaMemsetAsync(g.counters, 0, sizeof(unsigned) * G, st));
-            fsim_ingest_kernel<<<dim3(tiles, G), FT, 0, st>>>(g);
-            iqm::check_launch(ctx, "fsim_ingest_kernel");
-            fsim_fwd_rows_kernel<<<dim3(iqm::ceil_div(h2, s.rows_fwd), 2 * G), FT, s.sm_rows_fwd, st>>>(
-                g, P->row, s.rows_fwd, wlr);
-            iqm::check_launch(ctx, "fsim_fwd_rows_kernel");
-            fsim_fwd_cols_kernel<<<dim3(iqm::ceil_div(w2, s.cols_fwd), 2 * G), FT, s.sm_cols_fwd, st>>>(
-                g, P->col, s.cols_fwd, wlc);
-            iqm::check_launch(ctx, "fsim_fwd_cols_kernel");
-            fsim_inv_cols_kernel<<<dim3(iqm::ceil_div(w2, s.cols_inv), 4, 2 * G), FT, s.sm_cols_inv, st>>>(
-                g, P->col, s.cols_inv, wlc, 0);
+        // inverse-pass chunk: the 32 intermediate planes of `chunk` pairs stay within ~80 MB of L2
+        const int chunk = std::max(1, std::min(G, int((80ull << 20) / (sizeof(float2) * 32 * size_t(n)))));
+        const Layout Lc = layout_for(G, chunk, n, tiles);
+        FsimGroup g{};
+        g.pairs = d_desc + first;
+        g.G = G;
+        g.pair0 = 0;
+        g.w2 = w2;
+        g.h2 = h2;
+        g.n = n;
+        g.yiq = reinterpret_cast<float *>(base + Lc.yiq);
+        g.spec = reinterpret_cast<float2 *>(base + Lc.spec);
+        g.T = reinterpret_cast<float2 *>(base + Lc.T);
+        g.amp = reinterpret_cast<float *>(base + Lc.planes);
+        g.energy = g.amp + size_t(G) * 8 * n;
+        g.eo0 = g.energy + size_t(G) * 8 * n;
+        g.thr = reinterpret_cast<float *>(base + Lc.thr);
+        g.partials = reinterpret_cast<double *>(base + Lc.partials);
+        g.counters = reinterpret_cast<unsigned *>(base + Lc.counters);
+        g.tiles = tiles;
+        g.scores = d_scores;
+        g.filters = P->filters;
+        g.consts = P->consts;
+        g.energy_mode = energy_mode;
+        int F_uniform = hd[kv.second[0]].F;
+        for (int i : kv.second)
+            if (hd[i].F != F_uniform) F_uniform = 0;
+        IQM_CHECK_CUDA(cudaMemsetAsync(g.counters, 0, sizeof(unsigned) * G, st));
+        launch_ingest(g, F_uniform, tiles, st);
+        iqm::check_launch(ctx, "fsim_ingest_kernel");
+        fsim_fwd_rows_kernel<<<dim3(iqm::ceil_div(h2, 1 << s.lw_rows), 2 * G), 32 << s.lw_rows, s.sm_rows, st>>>(
+            g, P->row, s.wl_row);
+        iqm::check_launch(ctx, "fsim_fwd_rows_kernel");
+        fsim_fwd_cols_kernel<<<dim3(iqm::ceil_div(w2, 1 << s.lw_fcols), 2 * G), 32 << s.lw_fcols, s.sm_fcols, st>>>(
+            g, P->col, s.wl_col, s.lw_fcols);
+        iqm::check_launch(ctx, "fsim_fwd_cols_kernel");
+        for (int c0 = 0; c0 < G; c0 += chunk) {
+            FsimGroup gc = g;
+            gc.pair0 = c0;
+            const int cg = std::min(chunk, G - c0);
+            launch_inv_cols(gc, *P, s, 2 * cg, 0, st);
             iqm::check_launch(ctx, "fsim_inv_cols_kernel");
-            fsim_inv_rows_kernel<<<dim3(h2, 4, 2 * G), FT, s.sm_rows_inv, st>>>(g, P->row, wlr, s.seq_rows, 0,
-                                                                                 nullptr);
+            launch_inv_rows(gc, *P, s, 2 * cg, 0, nullptr, st);
             iqm::check_launch(ctx, "fsim_inv_rows_kernel");
-            fsim_noise_kernel<<<dim3(8, G), 1024, 0, st>>>(g);
-            iqm::check_launch(ctx, "fsim_noise_kernel");
-            fsim_final_kernel<<<dim3(tiles, G), FT, 0, st>>>(g);
-            iqm::check_launch(ctx, "fsim_final_kernel");
         }
-        first += Gtot;
+        fsim_noise_kernel<<<dim3(8, G), 1024, 0, st>>>(g);
+        iqm::check_launch(ctx, "fsim_noise_kernel");
+        fsim_final_kernel<<<dim3(tiles, G), FT, 0, st>>>(g);
+        iqm::check_launch(ctx, "fsim_final_kernel");
+        first += G;
     }
 }
 
