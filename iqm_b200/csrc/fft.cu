@@ -1,5 +1,6 @@
 // Host side of the shared-memory FFT engine (fft.cuh): per-length plans with device tables,
 // cached on the context.
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <vector>
@@ -20,30 +21,72 @@ struct FftPlan {
 
 namespace {
 
-// Radix sequence for n (8s, then 4 or 2, then odd primes ascending); false when n has a prime
-// factor above FFT_MAX_GENERIC.
+// Radices the warp engine computes in registers, and the stage count of the best factorisation.
+const int kRegRadix[] = {2, 3, 4, 5, 8};
+
+bool is_reg_radix(int p) {
+    for (int r : kRegRadix)
+        if (r == p) return true;
+    return false;
+}
+
+bool is_prime(int p) {
+    if (p < 2) return false;
+    for (int d = 2; d * d <= p; d++)
+        if (p % d == 0) return false;
+    return true;
+}
+
+// Radix sequence for n with the fewest stages (register radices, plus odd primes up to
+// FFT_MAX_GENERIC as direct butterflies, which count double); odd radices first so the first
+// stage's strided writes avoid shared-memory bank conflicts.  False when n has a prime factor
+// above FFT_MAX_GENERIC.
 bool factor(int n, std::vector<int> &r) {
     r.clear();
-    int m = n;
-    int twos = 0;
-    while (m % 2 == 0) {
-        m /= 2;
-        twos++;
-    }
-    while (twos >= 3) {
-        r.push_back(8);
-        twos -= 3;
-    }
-    if (twos == 2) r.push_back(4);
-    if (twos == 1) r.push_back(2);
-    for (int p = 3; p <= m; p += 2) {
-        while (m % p == 0) {
-            if (p > FFT_MAX_GENERIC) return false;
-            r.push_back(p);
-            m /= p;
+    if (n == 1) return true;
+    // best[m] = (cost, radix) for transforming length m
+    std::vector<int> cost(n + 1, 1 << 20), pick(n + 1, 0);
+    cost[1] = 0;
+    for (int m = 2; m <= n; m++) {
+        if (n % m) continue;
+        for (int p = 2; p <= m && p <= FFT_MAX_GENERIC; p++) {
+            if (m % p) continue;
+            int c;
+            if (is_reg_radix(p)) c = 2;
+            else if (is_prime(p)) c = 5;
+            else continue;
+            if (cost[m / p] + c < cost[m] || (cost[m / p] + c == cost[m] && p > pick[m])) {
+                cost[m] = cost[m / p] + c;
+                pick[m] = p;
+            }
         }
     }
+    if (cost[n] >= (1 << 20)) return false;
+    for (int m = n; m > 1; m /= pick[m]) r.push_back(pick[m]);
+    std::stable_sort(r.begin(), r.end(), [](int x, int y) { return (x & 1) > (y & 1); });
     return true;
+}
+
+// Stage parameters and stage twiddles W_{L p}^{r k} (sign -1) laid out [k][r-1].
+void stage_tables(int n, const std::vector<int> &r, int *radix, int *stride, float *inv_stride, float *inv_q,
+                  int *off, int &len, std::vector<float2> &stw) {
+    int L = 1;
+    len = 0;
+    for (size_t i = 0; i < r.size(); i++) {
+        const int p = r[i];
+        radix[i] = p;
+        stride[i] = L;
+        inv_stride[i] = 1.0f / float(L);
+        inv_q[i] = 1.0f / float(n / p);
+        off[i] = len;
+        for (int k = 0; k < L; k++)
+            for (int q = 1; q < p; q++) {
+                const double a = 2.0 * M_PI * double(q) * double(k) / double(L * p);
+                stw.push_back(make_float2(float(std::cos(a)), float(-std::sin(a))));
+            }
+        len += (p - 1) * L;
+        L *= p;
+    }
 }
 
 // In-place radix-2 FFT in double (host), used only to precompute Bluestein kernels.
@@ -88,18 +131,12 @@ const FftLen &fft_len(iqm_ctx *ctx, int n) {
     FftLen &L = plan->len;
     L.n = n;
     std::vector<int> r;
-    std::vector<float2> tw, mtw, chirp, bf, bi;
+    std::vector<float2> tw, mtw, chirp, bf, bi, stw, mstw;
     table(tw, n);
     if (factor(n, r)) {
         L.bluestein = 0;
         L.nst = int(r.size());
-        int st = 1;
-        for (int i = 0; i < L.nst; i++) {
-            L.radix[i] = r[i];
-            L.stride[i] = st;
-            L.inv_stride[i] = 1.0f / float(st);
-            st *= r[i];
-        }
+        stage_tables(n, r, L.radix, L.stride, L.inv_stride, L.inv_q, L.stw_off, L.stw_len, stw);
     } else {
         L.bluestein = 1;
         L.nst = 0;
@@ -108,13 +145,7 @@ const FftLen &fft_len(iqm_ctx *ctx, int n) {
         L.m = m;
         factor(m, r);
         L.mst = int(r.size());
-        int st = 1;
-        for (int i = 0; i < L.mst; i++) {
-            L.mradix[i] = r[i];
-            L.mstride[i] = st;
-            L.minv_stride[i] = 1.0f / float(st);
-            st *= r[i];
-        }
+        stage_tables(m, r, L.mradix, L.mstride, L.minv_stride, L.minv_q, L.mstw_off, L.mstw_len, mstw);
         table(mtw, m);
         chirp.resize(n);
         std::vector<std::complex<double>> c(n);
@@ -138,7 +169,9 @@ const FftLen &fft_len(iqm_ctx *ctx, int n) {
             for (int k = 0; k < m; k++) dst[k] = make_float2(float(b[k].real() / m), float(b[k].imag() / m));
         }
     }
-    const size_t bytes = sizeof(float2) * (tw.size() + mtw.size() + chirp.size() + bf.size() + bi.size());
+    IQM_REQUIRE(int(r.size()) <= FFT_MAX_STAGES, "FFT length needs too many stages");
+    const size_t bytes =
+        sizeof(float2) * (tw.size() + mtw.size() + chirp.size() + bf.size() + bi.size() + stw.size() + mstw.size());
     if (cudaMalloc(&plan->dev, bytes) != cudaSuccess) {
         cudaGetLastError();
         delete plan;
@@ -157,6 +190,8 @@ const FftLen &fft_len(iqm_ctx *ctx, int n) {
     L.chirp = put(chirp);
     L.bfwd = put(bf);
     L.binv = put(bi);
+    L.stw = put(stw);
+    L.mstw = put(mstw);
     ctx->fft_plans[n] = plan;
     return L;
 }

@@ -28,6 +28,10 @@ struct FftLen {
     int radix[FFT_MAX_STAGES];
     int stride[FFT_MAX_STAGES];    // L: product of the earlier radices
     float inv_stride[FFT_MAX_STAGES];
+    float inv_q[FFT_MAX_STAGES];   // 1 / (n / radix)
+    int stw_off[FFT_MAX_STAGES];   // offset of each stage's twiddles in stw
+    int stw_len;                   // entries of stw: sum over stages of (radix - 1) * stride
+    const float2 *stw;        // stage twiddles W_{L p}^{r k} (sign -1), [k][r-1] per stage
     const float2 *tw;         // n entries, exp(-2 pi i t / n)
     // Bluestein data (bluestein != 0): x -> c * IFFT_m( FFT_m(c * x) * B ), c = chirp
     int bluestein;
@@ -36,6 +40,10 @@ struct FftLen {
     int mradix[FFT_MAX_STAGES];
     int mstride[FFT_MAX_STAGES];
     float minv_stride[FFT_MAX_STAGES];
+    float minv_q[FFT_MAX_STAGES];
+    int mstw_off[FFT_MAX_STAGES];
+    int mstw_len;
+    const float2 *mstw;
     const float2 *mtw;        // m entries, exp(-2 pi i t / m)
     const float2 *chirp;      // n entries, exp(-pi i t^2 / n)
     const float2 *bfwd;       // m entries, FFT_m(conj chirp, wrapped) / m      (sign -1)
@@ -239,67 +247,82 @@ __device__ inline float2 *fft_run(float2 *a, float2 *b, const FftLen &P, float s
 }
 
 // ---------------------------------------------------------------------------------------------
-// Warp-level engine: one transform per warp, stages separated by __syncwarp only, so the warps of
-// a CTA progress independently.  j / L is computed as floor((j + 0.5) / L) in float: for j < 2^22
-// the rounding error (about (j/L) 2^-23) stays below the 0.5/L distance to the next integer.
+// Warp-level engine: a warp transforms nb sequences (stored wl apart) with __syncwarp between
+// stages only, so the warps of a CTA progress independently.  Stage twiddles are read from `stw`
+// (usually a shared-memory copy of FftLen::stw), laid out [k][r-1] so each butterfly reads a
+// contiguous run.  Integer quotients use floor((i + 0.5) * (1/d)) in float, exact for i < 2^22.
 
 template <int P>
-__device__ __forceinline__ void warp_stage(const float2 *in, float2 *out, int n, int L, float invL,
-                                           const float2 *tw, float s) {
+__device__ __forceinline__ void warp_stage(const float2 *in, float2 *out, int n, int L, float invL, float invq,
+                                           const float2 *stw, float s, int nb, int wl) {
     const int q = n / P;
-    const int twstep = n / (L * P);
-    for (int j = threadIdx.x & 31; j < q; j += 32) {
+    for (int idx = threadIdx.x & 31; idx < nb * q; idx += 32) {
+        const int t = nb > 1 ? __float2int_rz((float(idx) + 0.5f) * invq) : 0;
+        const int j = idx - t * q;
+        const float2 *src = in + t * wl;
+        float2 *dst = out + t * wl;
         const int jl = __float2int_rz((float(j) + 0.5f) * invL);
         const int k = j - jl * L;
         float2 v[P];
 #pragma unroll
-        for (int r = 0; r < P; r++) v[r] = in[j + r * q];
+        for (int r = 0; r < P; r++) v[r] = src[j + r * q];
         if (k != 0) {
+            const float2 *w = stw + k * (P - 1) - 1;
 #pragma unroll
-            for (int r = 1; r < P; r++) v[r] = cmul(v[r], tw_at(tw, r * k * twstep, s));
+            for (int r = 1; r < P; r++) v[r] = cmul(v[r], make_float2(w[r].x, -s * w[r].y));
         }
         dft_small<P>(v, s);
         const int base = jl * L * P + k;
 #pragma unroll
-        for (int r = 0; r < P; r++) out[base + r * L] = v[r];
+        for (int r = 0; r < P; r++) dst[base + r * L] = v[r];
     }
 }
 
-__device__ __forceinline__ void warp_stage_generic(const float2 *in, float2 *out, int n, int L, float invL, int p,
-                                                   const float2 *tw, float s) {
+// odd prime radix without a register kernel: direct p-point DFT from the length-n table
+__device__ __forceinline__ void warp_stage_generic(const float2 *in, float2 *out, int n, int L, float invL,
+                                                   float invq, int p, const float2 *stw, const float2 *tw, float s,
+                                                   int nb, int wl) {
     const int q = n / p;
-    const int twstep = n / (L * p);
-    for (int j = threadIdx.x & 31; j < q; j += 32) {
+    for (int idx = threadIdx.x & 31; idx < nb * q; idx += 32) {
+        const int t = nb > 1 ? __float2int_rz((float(idx) + 0.5f) * invq) : 0;
+        const int j = idx - t * q;
+        const float2 *src = in + t * wl;
+        float2 *dst = out + t * wl;
         const int jl = __float2int_rz((float(j) + 0.5f) * invL);
         const int k = j - jl * L;
         const int base = jl * L * p + k;
         for (int qq = 0; qq < p; qq++) {
             float2 acc = make_float2(0.f, 0.f);
             for (int r = 0; r < p; r++) {
-                float2 x = in[j + r * q];
-                if (k != 0 && r != 0) x = cmul(x, tw_at(tw, r * k * twstep, s));
+                float2 x = src[j + r * q];
+                if (k != 0 && r != 0) {
+                    const float2 w = stw[k * (p - 1) + r - 1];
+                    x = cmul(x, make_float2(w.x, -s * w.y));
+                }
                 const int e = (r * qq) % p;
                 acc = e ? cadd(acc, cmul(x, tw_at(tw, e * q, s))) : cadd(acc, x);
             }
-            out[base + qq * L] = acc;
+            dst[base + qq * L] = acc;
         }
     }
 }
 
 __device__ inline float2 *warp_stockham(float2 *a, float2 *b, int n, int nst, const int *radix, const int *stride,
-                                        const float *inv_stride, const float2 *tw, float s) {
+                                        const float *inv_stride, const float *inv_q, const int *stw_off,
+                                        const float2 *stw, const float2 *tw, float s, int nb, int wl) {
     float2 *in = a, *out = b;
     for (int st = 0; st < nst; st++) {
         const int p = radix[st], L = stride[st];
-        const float invL = inv_stride[st];
+        const float invL = inv_stride[st], iq = inv_q[st];
+        const float2 *w = stw + stw_off[st];
         __syncwarp();
         switch (p) {
-            case 2: warp_stage<2>(in, out, n, L, invL, tw, s); break;
-            case 3: warp_stage<3>(in, out, n, L, invL, tw, s); break;
-            case 4: warp_stage<4>(in, out, n, L, invL, tw, s); break;
-            case 5: warp_stage<5>(in, out, n, L, invL, tw, s); break;
-            case 8: warp_stage<8>(in, out, n, L, invL, tw, s); break;
-            default: warp_stage_generic(in, out, n, L, invL, p, tw, s); break;
+            case 2: warp_stage<2>(in, out, n, L, invL, iq, w, s, nb, wl); break;
+            case 3: warp_stage<3>(in, out, n, L, invL, iq, w, s, nb, wl); break;
+            case 4: warp_stage<4>(in, out, n, L, invL, iq, w, s, nb, wl); break;
+            case 5: warp_stage<5>(in, out, n, L, invL, iq, w, s, nb, wl); break;
+            case 8: warp_stage<8>(in, out, n, L, invL, iq, w, s, nb, wl); break;
+            default: warp_stage_generic(in, out, n, L, invL, iq, p, w, tw, s, nb, wl); break;
         }
         float2 *t = in;
         in = out;
@@ -309,31 +332,49 @@ __device__ inline float2 *warp_stockham(float2 *a, float2 *b, int n, int nst, co
     return in;
 }
 
-// One transform of length P.n held in a[0..n) by the calling warp (b: scratch; both of
-// fft_work_len(P) entries).  Returns the buffer with the unscaled result.
-__device__ inline float2 *fft_warp(float2 *a, float2 *b, const FftLen &P, float s) {
-    if (!P.bluestein) return warp_stockham(a, b, P.n, P.nst, P.radix, P.stride, P.inv_stride, P.tw, s);
+// Copies the stage twiddles of P into shared memory (all threads of the block; call before a
+// __syncthreads).  Returns the entries copied.
+__device__ inline void stage_twiddles_to_shared(const FftLen &P, float2 *dst) {
+    const float2 *src = P.bluestein ? P.mstw : P.stw;
+    const int len = P.bluestein ? P.mstw_len : P.stw_len;
+    for (int i = threadIdx.x; i < len; i += blockDim.x) dst[i] = __ldg(src + i);
+}
+__host__ __device__ inline int stage_twiddle_len(const FftLen &P) { return P.bluestein ? P.mstw_len : P.stw_len; }
+
+// nb transforms of length P.n held at a + t*wl (t < nb) by the calling warp (b: scratch of the same
+// shape; wl >= fft_work_len(P)).  `stw` is the stage-twiddle table (shared copy or P.stw / P.mstw).
+// Returns the buffer with the unscaled results.
+__device__ inline float2 *fft_warp(float2 *a, float2 *b, const FftLen &P, const float2 *stw, float s, int nb, int wl) {
+    if (!P.bluestein)
+        return warp_stockham(a, b, P.n, P.nst, P.radix, P.stride, P.inv_stride, P.inv_q, P.stw_off, stw, P.tw, s, nb,
+                             wl);
     const int n = P.n, m = P.m, lane = threadIdx.x & 31;
     __syncwarp();
-    for (int j = lane; j < m; j += 32) {
-        if (j < n) {
+    for (int t = 0; t < nb; t++)
+        for (int j = lane; j < m; j += 32) {
+            float2 *x = a + t * wl;
+            if (j < n) {
+                float2 c = __ldg(P.chirp + j);
+                if (s > 0) c = conjf2(c);
+                x[j] = cmul(x[j], c);
+            } else {
+                x[j] = make_float2(0.f, 0.f);
+            }
+        }
+    float2 *r = warp_stockham(a, b, m, P.mst, P.mradix, P.mstride, P.minv_stride, P.minv_q, P.mstw_off, stw, P.mtw,
+                              -1.f, nb, wl);
+    const float2 *B = s < 0 ? P.bfwd : P.binv;
+    for (int t = 0; t < nb; t++)
+        for (int j = lane; j < m; j += 32) r[t * wl + j] = cmul(r[t * wl + j], __ldg(B + j));
+    float2 *o = (r == a) ? b : a;
+    float2 *y = warp_stockham(r, o, m, P.mst, P.mradix, P.mstride, P.minv_stride, P.minv_q, P.mstw_off, stw, P.mtw,
+                              1.f, nb, wl);
+    for (int t = 0; t < nb; t++)
+        for (int j = lane; j < n; j += 32) {
             float2 c = __ldg(P.chirp + j);
             if (s > 0) c = conjf2(c);
-            a[j] = cmul(a[j], c);
-        } else {
-            a[j] = make_float2(0.f, 0.f);
+            y[t * wl + j] = cmul(y[t * wl + j], c);
         }
-    }
-    float2 *r = warp_stockham(a, b, m, P.mst, P.mradix, P.mstride, P.minv_stride, P.mtw, -1.f);
-    const float2 *B = s < 0 ? P.bfwd : P.binv;
-    for (int j = lane; j < m; j += 32) r[j] = cmul(r[j], __ldg(B + j));
-    float2 *o = (r == a) ? b : a;
-    float2 *y = warp_stockham(r, o, m, P.mst, P.mradix, P.mstride, P.minv_stride, P.mtw, 1.f);
-    for (int j = lane; j < n; j += 32) {
-        float2 c = __ldg(P.chirp + j);
-        if (s > 0) c = conjf2(c);
-        y[j] = cmul(y[j], c);
-    }
     __syncwarp();
     return y;
 }

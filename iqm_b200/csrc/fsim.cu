@@ -191,48 +191,67 @@ __global__ void __launch_bounds__(FT) fsim_ingest_kernel(FsimGroup g) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// forward transform (src/gpu/fsim/fsim.cpp:270-368: luma as complex (Y, 0), sign -1, unscaled).
-// One warp per row; rows per CTA = warps per CTA.
+// Transform kernels.  Shared memory of every transform CTA starts with the stage twiddles of its
+// length (FftLen::stw), followed by per-warp work buffers: a warp transforms NB sequences at once
+// (buffer a: NB x wl, buffer b: NB x wl), which keeps the lanes busy on stages with few butterflies.
+constexpr int NB = 1;
+
+__device__ __forceinline__ float2 *warp_area(float2 *base, int warp, int wl) { return base + size_t(warp) * 2 * NB * wl; }
+
+// forward transform (src/gpu/fsim/fsim.cpp:270-368: luma as complex (Y, 0), sign -1, unscaled),
+// NB rows per warp.
 __global__ void __launch_bounds__(FT, 1) fsim_fwd_rows_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl) {
     extern __shared__ float2 sm[];
+    const int tl = iqm::stage_twiddle_len(L);
+    iqm::stage_twiddles_to_shared(L, sm);
+    __syncthreads();
+    float2 *work = sm + ((tl + 1) & ~1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int plane = blockIdx.y;  // pair*2 + img
-    const int y = blockIdx.x * (blockDim.x >> 5) + warp;
-    if (y >= g.h2) return;  // warp-uniform; no block-wide barrier follows
-    float2 *a = sm + size_t(warp) * 2 * wl, *b = a + wl;
-    const float *Y = g.yiq + (size_t(plane) * 3 + 2) * g.n + size_t(y) * g.w2;
-    for (int x = lane; x < g.w2; x += 32) a[x] = make_float2(Y[x], 0.f);
-    const float2 *res = iqm::fft_warp(a, b, L, -1.f);
-    float2 *S = g.spec + size_t(plane) * g.n + size_t(y) * g.w2;
-    for (int x = lane; x < g.w2; x += 32) S[x] = res[x];
+    const int y0 = (blockIdx.x * (blockDim.x >> 5) + warp) * NB;
+    if (y0 >= g.h2) return;  // warp-uniform; no block-wide barrier follows
+    const int nb = min(NB, g.h2 - y0);
+    float2 *a = warp_area(work, warp, wl), *b = a + NB * wl;
+    const float *Y = g.yiq + (size_t(plane) * 3 + 2) * g.n + size_t(y0) * g.w2;
+    for (int t = 0; t < nb; t++)
+        for (int x = lane; x < g.w2; x += 32) a[t * wl + x] = make_float2(Y[size_t(t) * g.w2 + x], 0.f);
+    const float2 *res = iqm::fft_warp(a, b, L, sm, -1.f, NB == 1 ? 1 : nb, wl);
+    float2 *S = g.spec + size_t(plane) * g.n + size_t(y0) * g.w2;
+    for (int t = 0; t < nb; t++)
+        for (int x = lane; x < g.w2; x += 32) S[size_t(t) * g.w2 + x] = res[t * wl + x];
 }
 
-// Column passes: a CTA of nw (power of two) warps owns nw adjacent columns; the column slab is
-// loaded and stored cooperatively (nw*8-byte row segments) and each warp transforms one column.
+// Column passes: a CTA of nw warps owns NB*nw adjacent columns (nw power of two); the column slab
+// is loaded and stored cooperatively and each warp transforms NB of its columns.
 __device__ __forceinline__ int slab_parity(float2 *res, float2 *a) { return res == a ? 0 : 1; }
 
 __global__ void __launch_bounds__(FT, 1) fsim_fwd_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int lw) {
     extern __shared__ float2 sm[];
     __shared__ int parity;
-    const int nw = 1 << lw, warp = threadIdx.x >> 5;
+    const int tl = iqm::stage_twiddle_len(L);
+    iqm::stage_twiddles_to_shared(L, sm);
+    float2 *work = sm + ((tl + 1) & ~1);
+    const int nw = 1 << lw, cols = NB * nw, warp = threadIdx.x >> 5;
     const int plane = blockIdx.y;
-    const int x0 = blockIdx.x * nw;
-    const int nc = min(nw, g.w2 - x0);
+    const int x0 = blockIdx.x * cols;
+    const int nc = min(cols, g.w2 - x0);
     float2 *S = g.spec + size_t(plane) * g.n;
-    for (int idx = threadIdx.x; idx < nw * g.h2; idx += blockDim.x) {
-        const int c = idx & (nw - 1), y = idx >> lw;
-        if (c < nc) sm[size_t(c) * 2 * wl + y] = S[size_t(y) * g.w2 + x0 + c];
+    // column c lives in warp c / NB, slot c % NB
+    for (int idx = threadIdx.x; idx < cols * g.h2; idx += blockDim.x) {
+        const int c = idx % cols, y = idx / cols;
+        if (c < nc) warp_area(work, c / NB, wl)[(c % NB) * wl + y] = S[size_t(y) * g.w2 + x0 + c];
     }
     __syncthreads();
-    if (warp < nc) {
-        float2 *a = sm + size_t(warp) * 2 * wl;
-        float2 *res = iqm::fft_warp(a, a + wl, L, -1.f);
+    const int nbw = min(NB, nc - warp * NB);
+    if (nbw > 0) {
+        float2 *a = warp_area(work, warp, wl);
+        float2 *res = iqm::fft_warp(a, a + NB * wl, L, sm, -1.f, NB == 1 ? 1 : nbw, wl);
         if (warp == 0 && (threadIdx.x & 31) == 0) parity = slab_parity(res, a);
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < nw * g.h2; idx += blockDim.x) {
-        const int c = idx & (nw - 1), y = idx >> lw;
-        if (c < nc) S[size_t(y) * g.w2 + x0 + c] = sm[size_t(c) * 2 * wl + parity * wl + y];
+    for (int idx = threadIdx.x; idx < cols * g.h2; idx += blockDim.x) {
+        const int c = idx % cols, y = idx / cols;
+        if (c < nc) S[size_t(y) * g.w2 + x0 + c] = warp_area(work, c / NB, wl)[parity * NB * wl + (c % NB) * wl + y];
     }
 }
 
@@ -243,39 +262,45 @@ __global__ void __launch_bounds__(FT, 1) fsim_fwd_cols_kernel(FsimGroup g, const
 __global__ void __launch_bounds__(FT, 1) fsim_inv_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int lw, int consts_mode) {
     extern __shared__ float2 sm[];
     __shared__ int parity;
-    const int nw = 1 << lw, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tl = iqm::stage_twiddle_len(L);
+    iqm::stage_twiddles_to_shared(L, sm);
+    const int nw = 1 << lw, cols = NB * nw, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int o = blockIdx.y;
     const int plane = blockIdx.z;  // chunk-local pair*2 + img
-    const int x0 = blockIdx.x * nw;
-    const int nc = min(nw, g.w2 - x0);
+    const int x0 = blockIdx.x * cols;
+    const int nc = min(cols, g.w2 - x0);
     const int h2 = g.h2;
-    float2 *Sl = sm;                          // nw columns x h2 (column-major)
-    float2 *work = sm + size_t(nw) * h2;      // per warp: a, b of wl each
+    float2 *Sl = sm + ((tl + 1) & ~1);     // cols x h2 spectrum slab (column-major)
+    float2 *work = Sl + size_t(cols) * h2;  // per warp: a, b of NB x wl each
     const float2 *src = g.spec + size_t(g.pair0 * 2 + plane) * g.n;
-    for (int idx = threadIdx.x; idx < nw * h2; idx += blockDim.x) {
-        const int c = idx & (nw - 1), y = idx >> lw;
+    for (int idx = threadIdx.x; idx < cols * h2; idx += blockDim.x) {
+        const int c = idx % cols, y = idx / cols;
         if (c < nc) Sl[size_t(c) * h2 + y] = consts_mode ? make_float2(1.f, 0.f) : src[size_t(y) * g.w2 + x0 + c];
     }
     __syncthreads();
+    const int nbw = min(NB, nc - warp * NB);
     for (int s = 0; s < 4; s++) {
         const int z = o * 4 + s;
-        if (warp < nc) {
-            float2 *a = work + size_t(warp) * 2 * wl;
-            const float *H = g.filters + size_t(z) * g.n + size_t(x0 + warp) * h2;
-            const float2 *col = Sl + size_t(warp) * h2;
-            for (int y = lane; y < h2; y += 32) {
-                const float hv = __ldg(H + y);
-                const float2 v = col[y];
-                a[y] = make_float2(hv * v.x, hv * v.y);
+        if (nbw > 0) {
+            float2 *a = warp_area(work, warp, wl);
+            for (int t = 0; t < nbw; t++) {
+                const int c = warp * NB + t;
+                const float *H = g.filters + size_t(z) * g.n + size_t(x0 + c) * h2;
+                const float2 *col = Sl + size_t(c) * h2;
+                for (int y = lane; y < h2; y += 32) {
+                    const float hv = __ldg(H + y);
+                    const float2 v = col[y];
+                    a[t * wl + y] = make_float2(hv * v.x, hv * v.y);
+                }
             }
-            float2 *res = iqm::fft_warp(a, a + wl, L, 1.f);
+            float2 *res = iqm::fft_warp(a, a + NB * wl, L, sm, 1.f, NB == 1 ? 1 : nbw, wl);
             if (warp == 0 && lane == 0) parity = slab_parity(res, a);
         }
         __syncthreads();
         float2 *dst = g.T + (size_t(plane) * 16 + z) * g.n;
-        for (int idx = threadIdx.x; idx < nw * h2; idx += blockDim.x) {
-            const int c = idx & (nw - 1), y = idx >> lw;
-            if (c < nc) dst[size_t(y) * g.w2 + x0 + c] = work[size_t(c) * 2 * wl + parity * wl + y];
+        for (int idx = threadIdx.x; idx < cols * h2; idx += blockDim.x) {
+            const int c = idx % cols, y = idx / cols;
+            if (c < nc) dst[size_t(y) * g.w2 + x0 + c] = warp_area(work, c / NB, wl)[parity * NB * wl + (c % NB) * wl + y];
         }
         __syncthreads();
     }
@@ -303,30 +328,41 @@ __device__ __forceinline__ void response_sums(const float2 v[4], float invN, flo
     e0 = re[0] * re[0] + im[0] * im[0];
 }
 
-// inverse transform, pass 2 (along x): warp (r, s) of a CTA transforms row y0 + r, scale s.
-// consts_mode (rr = 1) instead accumulates, per row, sum_s Re_s^2 N and sum_{i<j} Re_i Re_j N
-// (shaders/fsim/fsim_mult_filters.glsl:37-58) over p < ceil(N/2) and over all p.
+// inverse transform, pass 2 (along x): a CTA handles rr rows with WPR = 4/NB warps per row;
+// warp (r, h) transforms scales h*NB .. h*NB+NB-1 of row y0 + r.  consts_mode (rr = 1) instead accumulates, per row, sum_s Re_s^2 N and
+// sum_{i<j} Re_i Re_j N (shaders/fsim/fsim_mult_filters.glsl:37-58) over p < ceil(N/2) and all p.
 __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int rr, int consts_mode,
-                                                           double *rowsums) {
+                                                              double *rowsums) {
     extern __shared__ float2 sm[];
     __shared__ int parity;
     __shared__ double red[4][FT / 32];
+    const int tl = iqm::stage_twiddle_len(L);
+    iqm::stage_twiddles_to_shared(L, sm);
+    __syncthreads();
+    float2 *work = sm + ((tl + 1) & ~1);
+    constexpr int WPR = 4 / NB;  // warps per row
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r = warp >> 2, s = warp & 3;
+    const int r = warp / WPR, h = warp % WPR;
     const int o = blockIdx.y, plane = blockIdx.z;  // plane: chunk-local pair*2 + img
     const int w2 = g.w2;
     const int y0 = blockIdx.x * rr;
     {
         const int y = y0 + r;
         if (r < rr && y < g.h2) {
-            float2 *a = sm + size_t(warp) * 2 * wl;
-            const float2 *src = g.T + (size_t(plane) * 16 + o * 4 + s) * g.n + size_t(y) * w2;
-            for (int x = lane; x < w2; x += 32) a[x] = src[x];
-            float2 *res = iqm::fft_warp(a, a + wl, L, 1.f);
+            float2 *a = warp_area(work, warp, wl);
+            for (int t = 0; t < NB; t++) {
+                const float2 *src = g.T + (size_t(plane) * 16 + o * 4 + h * NB + t) * g.n + size_t(y) * w2;
+                for (int x = lane; x < w2; x += 32) a[t * wl + x] = src[x];
+            }
+            float2 *res = iqm::fft_warp(a, a + NB * wl, L, sm, 1.f, NB, wl);
             if (warp == 0 && lane == 0) parity = slab_parity(res, a);
         }
     }
     __syncthreads();
+    // scale s of row rl: warp rl*WPR + s/NB, slot s%NB
+    auto at = [&](int rl, int s, int x) -> float2 {
+        return warp_area(work, rl * WPR + s / NB, wl)[parity * NB * wl + (s % NB) * wl + x];
+    };
     const float invN = 1.0f / float(g.n);
     if (!consts_mode) {
         const int gp = g.pair0 * 2 + plane;
@@ -336,7 +372,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_kernel(FsimGroup g, const
             if (y >= g.h2) continue;
             float2 v[4];
 #pragma unroll
-            for (int q = 0; q < 4; q++) v[q] = sm[size_t(rl * 4 + q) * 2 * wl + parity * wl + x];
+            for (int q = 0; q < 4; q++) v[q] = at(rl, q, x);
             float sA, en, e0;
             response_sums(v, invN, sA, en, e0);
             const size_t off = (size_t(gp) * 4 + o) * g.n + size_t(y) * w2 + x;
@@ -352,7 +388,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_kernel(FsimGroup g, const
         for (int x = threadIdx.x; x < w2; x += blockDim.x) {
             float re[4];
 #pragma unroll
-            for (int q = 0; q < 4; q++) re[q] = sm[size_t(q) * 2 * wl + parity * wl + x].x * invN;
+            for (int q = 0; q < 4; q++) re[q] = at(0, q, x).x * invN;
             float q2 = 0.f, qx = 0.f;
 #pragma unroll
             for (int q = 0; q < 4; q++) q2 += (re[q] * re[q]) * fn;
@@ -622,16 +658,16 @@ void set_smem(const void *fn, size_t bytes) {
 // Launch shapes of the transform kernels for one plane size.
 struct Shapes {
     int wl_row, wl_col;   // work lengths (n, or Bluestein m)
-    int lw_rows;          // log2 warps (rows) per CTA, forward rows
-    int lw_fcols;         // log2 warps (columns) per CTA, forward columns
-    int lw_icols;         // log2 warps (columns) per CTA, inverse columns
+    int lw_rows;          // log2 warps per CTA, forward rows (NB rows per warp)
+    int lw_fcols;         // log2 warps per CTA, forward columns (NB columns per warp)
+    int lw_icols;         // log2 warps per CTA, inverse columns
     int rr;               // rows per CTA in the inverse row pass (0: sequential kernel)
     size_t sm_rows, sm_fcols, sm_icols, sm_irows;
 };
 
-int lw_fit(size_t per_warp, size_t fixed_per_warp = 0) {
+int lw_fit(size_t fixed, size_t per_warp) {
     int lw = 3;  // up to 8 warps
-    while (lw > 0 && (size_t(1) << lw) * (per_warp + fixed_per_warp) > 160 * 1024) lw--;
+    while (lw > 0 && fixed + (size_t(1) << lw) * per_warp > 160 * 1024) lw--;
     return lw;
 }
 
@@ -640,21 +676,24 @@ Shapes shapes_for(const iqm::FsimPlan &P) {
     const size_t f2 = sizeof(float2);
     s.wl_row = iqm::fft_work_len(P.row);
     s.wl_col = iqm::fft_work_len(P.col);
-    s.lw_rows = lw_fit(2 * size_t(s.wl_row) * f2);
-    s.sm_rows = (size_t(1) << s.lw_rows) * 2 * s.wl_row * f2;
-    s.lw_fcols = lw_fit(2 * size_t(s.wl_col) * f2);
-    s.sm_fcols = (size_t(1) << s.lw_fcols) * 2 * s.wl_col * f2;
-    s.lw_icols = lw_fit((2 * size_t(s.wl_col) + P.h2) * f2);
-    s.sm_icols = (size_t(1) << s.lw_icols) * (2 * size_t(s.wl_col) + P.h2) * f2;
-    const size_t per_row = 4 * 2 * size_t(s.wl_row) * f2;
-    if (2 * per_row <= 120 * 1024) {
+    const size_t twr = size_t((iqm::stage_twiddle_len(P.row) + 1) & ~1) * f2;
+    const size_t twc = size_t((iqm::stage_twiddle_len(P.col) + 1) & ~1) * f2;
+    const size_t warp_row = 2 * NB * size_t(s.wl_row) * f2, warp_col = 2 * NB * size_t(s.wl_col) * f2;
+    s.lw_rows = lw_fit(twr, warp_row);
+    s.sm_rows = twr + (size_t(1) << s.lw_rows) * warp_row;
+    s.lw_fcols = lw_fit(twc, warp_col);
+    s.sm_fcols = twc + (size_t(1) << s.lw_fcols) * warp_col;
+    s.lw_icols = lw_fit(twc, warp_col + NB * size_t(P.h2) * f2);
+    s.sm_icols = twc + (size_t(1) << s.lw_icols) * (warp_col + NB * size_t(P.h2) * f2);
+    const size_t per_row = (4 / NB) * warp_row;  // 4/NB warps per row (four scales)
+    if (twr + 2 * per_row <= 120 * 1024) {
         s.rr = 2;
-    } else if (per_row <= SMEM_CAP) {
+    } else if (twr + per_row <= SMEM_CAP) {
         s.rr = 1;
     } else {
         s.rr = 0;
     }
-    s.sm_irows = s.rr ? s.rr * per_row : (4 * size_t(P.w2) + 2 * s.wl_row) * f2;
+    s.sm_irows = s.rr ? twr + s.rr * per_row : (4 * size_t(P.w2) + 2 * s.wl_row) * f2;
     IQM_REQUIRE(s.sm_rows <= SMEM_CAP && s.sm_fcols <= SMEM_CAP && s.sm_icols <= SMEM_CAP && s.sm_irows <= SMEM_CAP,
                 "FSIM plane too large for the shared-memory FFT");
     return s;
@@ -674,10 +713,12 @@ void configure_kernels(const Shapes &s) {
 void launch_inv_rows(const FsimGroup &g, const iqm::FsimPlan &P, const Shapes &s, int planes, int consts_mode,
                      double *rowsums, cudaStream_t st) {
     if (s.rr && !(consts_mode && s.rr != 1)) {
-        fsim_inv_rows_kernel<<<dim3(iqm::ceil_div(P.h2, s.rr), 4, planes), 128 * s.rr, s.sm_irows, st>>>(
+        fsim_inv_rows_kernel<<<dim3(iqm::ceil_div(P.h2, s.rr), 4, planes), 32 * (4 / NB) * s.rr, s.sm_irows, st>>>(
             g, P.row, s.wl_row, s.rr, consts_mode, rowsums);
     } else if (s.rr) {  // consts mode runs one row per CTA
-        fsim_inv_rows_kernel<<<dim3(P.h2, 4, planes), 128, s.sm_irows / s.rr, st>>>(g, P.row, s.wl_row, 1, 1, rowsums);
+        const size_t twr = size_t((iqm::stage_twiddle_len(P.row) + 1) & ~1) * sizeof(float2);
+        fsim_inv_rows_kernel<<<dim3(P.h2, 4, planes), 32 * (4 / NB), twr + (s.sm_irows - twr) / s.rr, st>>>(
+            g, P.row, s.wl_row, 1, 1, rowsums);
     } else {
         fsim_inv_rows_seq_kernel<<<dim3(P.h2, 4, planes), FT, s.sm_irows, st>>>(g, P.row, s.wl_row, consts_mode,
                                                                                  rowsums);
@@ -687,7 +728,7 @@ void launch_inv_rows(const FsimGroup &g, const iqm::FsimPlan &P, const Shapes &s
 void launch_inv_cols(const FsimGroup &g, const iqm::FsimPlan &P, const Shapes &s, int planes, int consts_mode,
                      cudaStream_t st) {
     const int nw = 1 << s.lw_icols;
-    fsim_inv_cols_kernel<<<dim3(iqm::ceil_div(P.w2, nw), 4, planes), 32 * nw, s.sm_icols, st>>>(
+    fsim_inv_cols_kernel<<<dim3(iqm::ceil_div(P.w2, NB * nw), 4, planes), 32 * nw, s.sm_icols, st>>>(
         g, P.col, s.wl_col, s.lw_icols, consts_mode);
 }
 
@@ -853,10 +894,10 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
         IQM_CHECK_CUDA(cudaMemsetAsync(g.counters, 0, sizeof(unsigned) * G, st));
         launch_ingest(g, F_uniform, tiles, st);
         iqm::check_launch(ctx, "fsim_ingest_kernel");
-        fsim_fwd_rows_kernel<<<dim3(iqm::ceil_div(h2, 1 << s.lw_rows), 2 * G), 32 << s.lw_rows, s.sm_rows, st>>>(
+        fsim_fwd_rows_kernel<<<dim3(iqm::ceil_div(h2, NB << s.lw_rows), 2 * G), 32 << s.lw_rows, s.sm_rows, st>>>(
             g, P->row, s.wl_row);
         iqm::check_launch(ctx, "fsim_fwd_rows_kernel");
-        fsim_fwd_cols_kernel<<<dim3(iqm::ceil_div(w2, 1 << s.lw_fcols), 2 * G), 32 << s.lw_fcols, s.sm_fcols, st>>>(
+        fsim_fwd_cols_kernel<<<dim3(iqm::ceil_div(w2, NB << s.lw_fcols), 2 * G), 32 << s.lw_fcols, s.sm_fcols, st>>>(
             g, P->col, s.wl_col, s.lw_fcols);
         iqm::check_launch(ctx, "fsim_fwd_cols_kernel");
         for (int c0 = 0; c0 < G; c0 += chunk) {
