@@ -91,6 +91,9 @@ __device__ __forceinline__ int find_tile(const FlipPairDev *p, int n, int t) {
     return lo;
 }
 
+// RF, RC > 0: filter radii fixed at compile time (tap loops unrolled, weights as constant-bank
+// operands); 0: read from T.
+template <int RF, int RC>
 __global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __grid_constant__ FlipTaps T) {
     __shared__ float lin[256];
     __shared__ float ycc[2][4][HSEG + 2 * MAXR];  // Y, Cx, Cz and (Y + 16) / 116
@@ -101,7 +104,8 @@ __global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __g
     const long long local = seg - P.seg_base;
     const int y = int(local / segs_x);
     const int x0 = int(local % segs_x) * HSEG;
-    const int R = max(T.rf, T.rc);
+    const int rf = RF ? RF : T.rf, rc = RC ? RC : T.rc;
+    const int R = max(rf, rc);
     for (int i = threadIdx.x; i < 256; i += HT) lin[i] = T.lin[i];
     __syncthreads();
     // stage YCxCz of columns x0-R .. x0+HSEG+R-1 (clamped to the image), both images
@@ -130,12 +134,13 @@ __global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __g
     for (int img = 0; img < 2; img++) {
         float fa[4][3] = {}, ca[4][3] = {};
         // output column x = x0 + xl + i reads staged column (x - j) + R - x0 = xl + i - j + R
+#pragma unroll
         for (int j = -R; j <= R; j++) {
-            const bool uf = j >= -T.rf && j <= T.rf, uc = j >= -T.rc && j <= T.rc;
-            const float wg = uf ? T.feat[0][j + T.rf] : 0.f, we = uf ? T.feat[1][j + T.rf] : 0.f,
-                        wp = uf ? T.feat[2][j + T.rf] : 0.f;
-            const float w0 = uc ? T.csf[0][j + T.rc] : 0.f, w1 = uc ? T.csf[1][j + T.rc] : 0.f,
-                        w2 = uc ? T.csf[2][j + T.rc] : 0.f;
+            const bool uf = j >= -rf && j <= rf, uc = j >= -rc && j <= rc;
+            const float wg = uf ? T.feat[0][j + rf] : 0.f, we = uf ? T.feat[1][j + rf] : 0.f,
+                        wp = uf ? T.feat[2][j + rf] : 0.f;
+            const float w0 = uc ? T.csf[0][j + rc] : 0.f, w1 = uc ? T.csf[1][j + rc] : 0.f,
+                        w2 = uc ? T.csf[2][j + rc] : 0.f;
 #pragma unroll
             for (int i = 0; i < 4; i++) {
                 const int c = xl + i - j + R;
@@ -195,15 +200,28 @@ __device__ __forceinline__ void ycxcz_to_hunt_lab(const FlipTaps &T, float Y, fl
     lab[2] *= 0.01f * lab[0];
 }
 
-// Everything one image contributes to a pixel, from its filtered sums: gradient and second-derivative
-// magnitudes and the Hunt-adjusted L*a*b* colour.  Not inlined: both images run the one compiled
-// copy, so identical inputs round identically and FLIP(a, a) is exactly 0.
-__device__ __noinline__ void per_image(const FlipTaps &T, const float *acc, float lab[3], float &dl, float &ddl) {
-    dl = sqrtf(fmaf(acc[0], acc[0], acc[1] * acc[1]));
-    ddl = sqrtf(fmaf(acc[2], acc[2], acc[3] * acc[3]));
-    ycxcz_to_hunt_lab(T, acc[4], acc[5], acc[6], lab);
+// Everything one image contributes to a pixel, from its seven filtered sums: gradient and
+// second-derivative magnitudes and the Hunt-adjusted L*a*b* colour.  Not inlined: both images run
+// the one compiled copy, so identical inputs round identically and FLIP(a, a) is exactly 0.
+// Arguments and result travel by value (registers).
+struct ImgTerms {
+    float L, a, b, dl, ddl;
+};
+
+__device__ __noinline__ ImgTerms per_image(const FlipTaps &T, float d0, float d1, float dd0, float dd1, float cY,
+                                           float cCx, float cCz) {
+    ImgTerms o;
+    o.dl = sqrtf(fmaf(d0, d0, d1 * d1));
+    o.ddl = sqrtf(fmaf(dd0, dd0, dd1 * dd1));
+    float lab[3];
+    ycxcz_to_hunt_lab(T, cY, cCx, cCz, lab);
+    o.L = lab[0];
+    o.a = lab[1];
+    o.b = lab[2];
+    return o;
 }
 
+template <int RF, int RC>
 __global__ void __launch_bounds__(VT) flip_vpass_kernel(FlipArgs args, const __grid_constant__ FlipTaps T) {
     extern __shared__ float vs[];  // [NPLANE][rows][VT_COLS]
     __shared__ double red[VT / 32];
@@ -213,7 +231,8 @@ __global__ void __launch_bounds__(VT) flip_vpass_kernel(FlipArgs args, const __g
     const FlipPairDev P = args.pairs[pi];
     const int local = gt - P.tile_base;
     const int x0 = (local % P.tiles_x) * VT_COLS, y0 = (local / P.tiles_x) * VT_ROWS;
-    const int R = max(T.rf, T.rc);
+    const int rf = RF ? RF : T.rf, rc = RC ? RC : T.rc;
+    const int R = max(rf, rc);
     const int rows = VT_ROWS + 2 * R;
     const int n = P.w * P.h;
     const float *planes = args.planes + P.plane_off;
@@ -234,9 +253,11 @@ __global__ void __launch_bounds__(VT) flip_vpass_kernel(FlipArgs args, const __g
         for (int m = 0; m < 2; m++)
 #pragma unroll
             for (int q = 0; q < 7; q++) acc[i][m][q] = 0.f;
-    // staged row s holds image row y0 - R + s; output row y = y0 + r0 + i reads rows y - k,
-    // k in [-r, r], i.e. s = r0 + i - k + R.
-    for (int s = r0; s <= r0 + VT_RPT - 1 + 2 * R; s++) {
+    // staged row s = r0 + d holds image row y0 - R + s; output row y = y0 + r0 + i reads rows
+    // y - k, k in [-r, r], i.e. d = i - k + R.
+#pragma unroll
+    for (int d = 0; d <= VT_RPT - 1 + 2 * R; d++) {
+        const int s = r0 + d;
         float v[2][6];
 #pragma unroll
         for (int m = 0; m < 2; m++)
@@ -244,9 +265,9 @@ __global__ void __launch_bounds__(VT) flip_vpass_kernel(FlipArgs args, const __g
             for (int q = 0; q < 6; q++) v[m][q] = vs[((m * 6 + q) * rows + s) * VT_COLS + c];
 #pragma unroll
         for (int i = 0; i < VT_RPT; i++) {
-            const int k = r0 + i - s + R;
-            if (k >= -T.rf && k <= T.rf) {
-                const float g = T.feat[0][k + T.rf], e = T.feat[1][k + T.rf], p = T.feat[2][k + T.rf];
+            const int k = i - d + R;
+            if (k >= -rf && k <= rf) {
+                const float g = T.feat[0][k + rf], e = T.feat[1][k + rf], p = T.feat[2][k + rf];
 #pragma unroll
                 for (int m = 0; m < 2; m++) {
                     acc[i][m][0] = fmaf(v[m][0], g, acc[i][m][0]);  // dx * g
@@ -255,8 +276,8 @@ __global__ void __launch_bounds__(VT) flip_vpass_kernel(FlipArgs args, const __g
                     acc[i][m][3] = fmaf(v[m][2], p, acc[i][m][3]);  // value * point
                 }
             }
-            if (k >= -T.rc && k <= T.rc) {
-                const float w0 = T.csf[0][k + T.rc], w1 = T.csf[1][k + T.rc], w2 = T.csf[2][k + T.rc];
+            if (k >= -rc && k <= rc) {
+                const float w0 = T.csf[0][k + rc], w1 = T.csf[1][k + rc], w2 = T.csf[2][k + rc];
 #pragma unroll
                 for (int m = 0; m < 2; m++) {
                     acc[i][m][4] = fmaf(v[m][3], w0, acc[i][m][4]);
@@ -273,8 +294,16 @@ __global__ void __launch_bounds__(VT) flip_vpass_kernel(FlipArgs args, const __g
         const int y = y0 + r0 + i;
         if (x >= P.w || y >= P.h) continue;
         float lab[2][3], dl[2], ddl[2];
-        per_image(T, acc[i][0], lab[0], dl[0], ddl[0]);
-        per_image(T, acc[i][1], lab[1], dl[1], ddl[1]);
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+            const ImgTerms t = per_image(T, acc[i][m][0], acc[i][m][1], acc[i][m][2], acc[i][m][3], acc[i][m][4],
+                                         acc[i][m][5], acc[i][m][6]);
+            lab[m][0] = t.L;
+            lab[m][1] = t.a;
+            lab[m][2] = t.b;
+            dl[m] = t.dl;
+            ddl[m] = t.ddl;
+        }
         // feature error (feature_detection.glsl:48-53)
         const float ed = fabsf(dl[0] - dl[1]), pd = fabsf(ddl[0] - ddl[1]);
         const float def = sqrtf(rsqrtf(2.0f) * fmaxf(ed, pd));
@@ -456,14 +485,23 @@ void flip_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_fl
     a.scores = d_scores;
     a.total_segs = segs;
     IQM_CHECK_CUDA(cudaMemsetAsync(a.counters, 0, sizeof(unsigned) * n, ctx->stream));
-    flip_hpass_kernel<<<unsigned(segs), HT, 0, ctx->stream>>>(a, T);
-    iqm::check_launch(ctx, "flip_hpass_kernel");
     const int R = std::max(T.rf, T.rc);
     const size_t smem = sizeof(float) * NPLANE * (VT_ROWS + 2 * R) * VT_COLS;
-    if (smem > 48 * 1024)
-        IQM_CHECK_CUDA(cudaFuncSetAttribute((const void *)flip_vpass_kernel,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    flip_vpass_kernel<<<tiles, VT, smem, ctx->stream>>>(a, T);
+    auto run = [&](auto hk, auto vk) {
+        hk<<<unsigned(segs), HT, 0, ctx->stream>>>(a, T);
+        iqm::check_launch(ctx, "flip_hpass_kernel");
+        if (smem > 48 * 1024)
+            IQM_CHECK_CUDA(cudaFuncSetAttribute((const void *)vk, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        vk<<<tiles, VT, smem, ctx->stream>>>(a, T);
+    };
+    // the two viewing set-ups in common use get kernels with their radii built in
+    if (T.rf == 7 && T.rc == 8) {
+        run(flip_hpass_kernel<7, 8>, flip_vpass_kernel<7, 8>);        // default monitor, 52.1 ppd
+    } else if (T.rf == 9 && T.rc == 10) {
+        run(flip_hpass_kernel<9, 10>, flip_vpass_kernel<9, 10>);      // 67 ppd
+    } else {
+        run(flip_hpass_kernel<0, 0>, flip_vpass_kernel<0, 0>);
+    }
     iqm::check_launch(ctx, "flip_vpass_kernel");
 }
 

@@ -10,8 +10,8 @@
 //   msvd_block_kernel  one thread per block slot: 8 rows x 8 RGBA8 pixels of both images straight
 //                      into registers (two 16-byte loads per row and image, coalesced across a
 //                      warp of horizontally adjacent blocks), OpenCV's 15-bit fixed-point grey,
-//                      one-sided Jacobi SVD in registers (FP32 rotations, FP64 column norms and
-//                      inner products driving the convergence test), D in FP32 as the shader does;
+//                      one-sided Jacobi SVD in registers (FP32 rotations and inner products, FP64
+//                      convergence test and final norms), D in FP32 as the shader does;
 //   msvd_pool_kernel   one CTA per pair: exact median by radix select (select.cuh), then the mean
 //                      absolute deviation summed in FP64, and the optional D/max(D) map.
 #include <cfloat>
@@ -82,44 +82,47 @@ __device__ __forceinline__ void load_block(const uint8_t *img, long long pitch, 
 }
 
 // Singular values (descending) of the 8x8 matrix whose columns are c[0..7]; c is destroyed.
-// One-sided Jacobi: each (i, j) column pair is rotated so the columns become orthogonal; the
-// rotation is applied in FP32, the inner product and the squared norms are accumulated in FP64
-// and a pair is skipped once |<ci,cj>| <= eps * |ci| |cj| (compared squared, eps = FLT_EPSILON).
+// One-sided Jacobi: each (i, j) column pair is rotated so the columns become orthogonal.  Inner
+// products, rotations and the squared column norms (recomputed from the rotated columns) are FP32;
+// the rotation test |<ci,cj>|^2 > eps^2 |ci|^2 |cj|^2 is evaluated in FP64 (eps = 4 FLT_EPSILON,
+// above FP32 rounding noise, so sweeps stop: at most 6 on the OpenCV fixture blocks), and the final
+// norms are accumulated in FP64.
 __device__ __forceinline__ void svd8_values(float c[8][8], float s[8]) {
-    double nrm[8];
+    float nrm[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) {
-        double q = 0.0;
+        float q = 0.f;
 #pragma unroll
-        for (int r = 0; r < 8; r++) q = fma(double(c[i][r]), double(c[i][r]), q);
+        for (int r = 0; r < 8; r++) q = fmaf(c[i][r], c[i][r], q);
         nrm[i] = q;
     }
-    const double eps2 = double(FLT_EPSILON) * double(FLT_EPSILON);
+    const double eps2 = 16.0 * double(FLT_EPSILON) * double(FLT_EPSILON);
     for (int sweep = 0; sweep < 60; sweep++) {
         bool changed = false;
 #pragma unroll
         for (int i = 0; i < 7; i++) {
 #pragma unroll
             for (int j = i + 1; j < 8; j++) {
-                double p = 0.0;
+                float p = 0.f;
 #pragma unroll
-                for (int r = 0; r < 8; r++) p = fma(double(c[i][r]), double(c[j][r]), p);
-                if (p * p > eps2 * nrm[i] * nrm[j]) {
-                    // rotation zeroing <ci, cj>: tan(theta) = t, smaller root of t^2 + 2 zeta t - 1 = 0
-                    const float zeta = float((nrm[j] - nrm[i]) / (2.0 * p));
-                    const float t = copysignf(1.0f, zeta) / (fabsf(zeta) + sqrtf(fmaf(zeta, zeta, 1.0f)));
+                for (int r = 0; r < 8; r++) p = fmaf(c[i][r], c[j][r], p);
+                const double pd = double(p);
+                if (pd * pd > eps2 * double(nrm[i]) * double(nrm[j])) {
+                    const float zeta = (nrm[j] - nrm[i]) / (2.0f * p);
+                    const float az = fabsf(zeta);
+                    // tan(theta): smaller root of t^2 + 2 zeta t - 1 = 0 (1/(2 zeta) once zeta^2 overflows)
+                    const float t = copysignf(1.0f, zeta) / (az < 1e18f ? az + sqrtf(fmaf(zeta, zeta, 1.0f)) : 2.0f * az);
                     const float cs = rsqrtf(fmaf(t, t, 1.0f));
                     const float sn = cs * t;
-                    double ni = 0.0, nj = 0.0;
+                    float ni = 0.f, nj = 0.f;
 #pragma unroll
                     for (int r = 0; r < 8; r++) {
                         const float xi = c[i][r], xj = c[j][r];
-                        const float yi = fmaf(cs, xi, -sn * xj);
-                        const float yj = fmaf(sn, xi, cs * xj);
+                        const float yi = fmaf(cs, xi, -sn * xj), yj = fmaf(sn, xi, cs * xj);
                         c[i][r] = yi;
                         c[j][r] = yj;
-                        ni = fma(double(yi), double(yi), ni);
-                        nj = fma(double(yj), double(yj), nj);
+                        ni = fmaf(yi, yi, ni);
+                        nj = fmaf(yj, yj, nj);
                     }
                     nrm[i] = ni;
                     nrm[j] = nj;
@@ -130,7 +133,12 @@ __device__ __forceinline__ void svd8_values(float c[8][8], float s[8]) {
         if (!changed) break;
     }
 #pragma unroll
-    for (int i = 0; i < 8; i++) s[i] = float(sqrt(nrm[i]));
+    for (int i = 0; i < 8; i++) {
+        double q = 0.0;
+#pragma unroll
+        for (int r = 0; r < 8; r++) q = fma(double(c[i][r]), double(c[i][r]), q);
+        s[i] = float(sqrt(q));
+    }
     // descending order (sorting network on 8 registers)
 #define IQM_CSWAP(a, b)                         \
     do {                                        \
