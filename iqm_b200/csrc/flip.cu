@@ -48,7 +48,7 @@ struct FlipTaps {
     float feat[3][MAXT];  // g, edge, point (normalised as feature_filter_normalize.glsl)
     float csf[3][MAXT];   // luma, red-green, blue-yellow weights, each normalised to sum 1
     float lin[256];       // sRGB byte -> linear
-    float rgb2xyz[9], xyz2rgb[9], white[3];
+    float rgb2xyz[9], xyz2rgb[9], white[3], inv_white[3];
     float cmax;           // HyAB(Hunt(green), Hunt(blue))^0.7
 };
 
@@ -118,9 +118,9 @@ __global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __g
         float X = fmaf(T.rgb2xyz[0], r, fmaf(T.rgb2xyz[1], g, T.rgb2xyz[2] * b));
         float Y = fmaf(T.rgb2xyz[3], r, fmaf(T.rgb2xyz[4], g, T.rgb2xyz[5] * b));
         float Z = fmaf(T.rgb2xyz[6], r, fmaf(T.rgb2xyz[7], g, T.rgb2xyz[8] * b));
-        X /= T.white[0];
-        Y /= T.white[1];
-        Z /= T.white[2];
+        X *= T.inv_white[0];
+        Y *= T.inv_white[1];
+        Z *= T.inv_white[2];
         ycc[img][0][c] = fmaf(116.0f, Y, -16.0f);
         ycc[img][1][c] = 500.0f * (X - Y);
         ycc[img][2][c] = 200.0f * (Y - Z);
@@ -133,25 +133,62 @@ __global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __g
 #pragma unroll 1
     for (int img = 0; img < 2; img++) {
         float fa[4][3] = {}, ca[4][3] = {};
-        // output column x = x0 + xl + i reads staged column (x - j) + R - x0 = xl + i - j + R
+        // output column x = x0 + xl + i, tap j, reads staged column xl + i + u with u = R - j
+        if constexpr (RF > 0) {
+            // radii known: slide a 4-wide register window along u (one new value per plane per tap)
+            constexpr int RR = RF > RC ? RF : RC;
+            float win[4][4];
 #pragma unroll
-        for (int j = -R; j <= R; j++) {
-            const bool uf = j >= -rf && j <= rf, uc = j >= -rc && j <= rc;
-            const float wg = uf ? T.feat[0][j + rf] : 0.f, we = uf ? T.feat[1][j + rf] : 0.f,
-                        wp = uf ? T.feat[2][j + rf] : 0.f;
-            const float w0 = uc ? T.csf[0][j + rc] : 0.f, w1 = uc ? T.csf[1][j + rc] : 0.f,
-                        w2 = uc ? T.csf[2][j + rc] : 0.f;
+            for (int q = 0; q < 4; q++)
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
-                const int c = xl + i - j + R;
-                const float Yv = ycc[img][0][c];
-                const float v = ycc[img][3][c];
-                fa[i][0] = fmaf(we, v, fa[i][0]);  // dx   (edge)
-                fa[i][1] = fmaf(wp, v, fa[i][1]);  // ddx  (point)
-                fa[i][2] = fmaf(wg, v, fa[i][2]);  // value (gauss)
-                ca[i][0] = fmaf(w0, Yv, ca[i][0]);
-                ca[i][1] = fmaf(w1, ycc[img][1][c], ca[i][1]);
-                ca[i][2] = fmaf(w2, ycc[img][2][c], ca[i][2]);
+                for (int i = 0; i < 3; i++) win[q][i + 1] = ycc[img][q][xl + i];
+#pragma unroll
+            for (int u = 0; u <= 2 * RR; u++) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+#pragma unroll
+                    for (int i = 0; i < 3; i++) win[q][i] = win[q][i + 1];
+                    win[q][3] = ycc[img][q][xl + u + 3];
+                }
+                const int j = RR - u;
+                if (j >= -RF && j <= RF) {
+                    const float wg = T.feat[0][j + RF], we = T.feat[1][j + RF], wp = T.feat[2][j + RF];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        fa[i][0] = fmaf(we, win[3][i], fa[i][0]);  // dx   (edge)
+                        fa[i][1] = fmaf(wp, win[3][i], fa[i][1]);  // ddx  (point)
+                        fa[i][2] = fmaf(wg, win[3][i], fa[i][2]);  // value (gauss)
+                    }
+                }
+                if (j >= -RC && j <= RC) {
+                    const float w0 = T.csf[0][j + RC], w1 = T.csf[1][j + RC], w2 = T.csf[2][j + RC];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        ca[i][0] = fmaf(w0, win[0][i], ca[i][0]);
+                        ca[i][1] = fmaf(w1, win[1][i], ca[i][1]);
+                        ca[i][2] = fmaf(w2, win[2][i], ca[i][2]);
+                    }
+                }
+            }
+        } else {
+            for (int j = -R; j <= R; j++) {
+                const bool uf = j >= -rf && j <= rf, uc = j >= -rc && j <= rc;
+                const float wg = uf ? T.feat[0][j + rf] : 0.f, we = uf ? T.feat[1][j + rf] : 0.f,
+                            wp = uf ? T.feat[2][j + rf] : 0.f;
+                const float w0 = uc ? T.csf[0][j + rc] : 0.f, w1 = uc ? T.csf[1][j + rc] : 0.f,
+                            w2 = uc ? T.csf[2][j + rc] : 0.f;
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const int c = xl + i - j + R;
+                    const float Yv = ycc[img][0][c];
+                    const float v = ycc[img][3][c];
+                    fa[i][0] = fmaf(we, v, fa[i][0]);  // dx   (edge)
+                    fa[i][1] = fmaf(wp, v, fa[i][1]);  // ddx  (point)
+                    fa[i][2] = fmaf(wg, v, fa[i][2]);  // value (gauss)
+                    ca[i][0] = fmaf(w0, Yv, ca[i][0]);
+                    ca[i][1] = fmaf(w1, ycc[img][1][c], ca[i][1]);
+                    ca[i][2] = fmaf(w2, ycc[img][2][c], ca[i][2]);
+                }
             }
         }
 #pragma unroll
@@ -168,13 +205,20 @@ __global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __g
     }
 }
 
-// L*a*b* of normalised XYZ (shaders/flip/spatial_prefilter.glsl:86-96)
+// x^y for the non-negative bases FLIP raises to powers: exp2(y log2 x) for x > 0 (a few ulp from
+// powf, well inside the score tolerance), powf itself for x = 0 so 0^0 and 0^-y keep their values.
+__device__ __forceinline__ float pow_nonneg(float x, float y) {
+    return x > 0.0f ? exp2f(y * log2f(x)) : powf(x, y);
+}
+
+// L*a*b* of normalised XYZ (shaders/flip/spatial_prefilter.glsl:86-96); the shader's
+// pow(v, 1/3) is a cube root
 __device__ __forceinline__ void xyzn_to_lab(float x, float y, float z, float lab[3]) {
     const float delta = 6.0f / 29.0f, limit = 0.008856f;
     const float k = 1.0f / (3.0f * delta * delta), o = 4.0f / 29.0f;
-    const float cx = x > limit ? powf(x, 1.0f / 3.0f) : fmaf(x, k, o);
-    const float cy = y > limit ? powf(y, 1.0f / 3.0f) : fmaf(y, k, o);
-    const float cz = z > limit ? powf(z, 1.0f / 3.0f) : fmaf(z, k, o);
+    const float cx = x > limit ? cbrtf(x) : fmaf(x, k, o);
+    const float cy = y > limit ? cbrtf(y) : fmaf(y, k, o);
+    const float cz = z > limit ? cbrtf(z) : fmaf(z, k, o);
     lab[0] = fmaf(116.0f, cy, -16.0f);
     lab[1] = 500.0f * (cx - cy);
     lab[2] = 200.0f * (cy - cz);
@@ -182,7 +226,7 @@ __device__ __forceinline__ void xyzn_to_lab(float x, float y, float z, float lab
 
 // filtered YCxCz -> Hunt-adjusted L*a*b* (shaders/flip/spatial_prefilter.glsl:74-99)
 __device__ __forceinline__ void ycxcz_to_hunt_lab(const FlipTaps &T, float Y, float Cx, float Cz, float lab[3]) {
-    const float yy = (Y + 16.0f) / 116.0f, cx = Cx / 500.0f, cz = Cz / 200.0f;
+    const float yy = (Y + 16.0f) * (1.0f / 116.0f), cx = Cx * (1.0f / 500.0f), cz = Cz * (1.0f / 200.0f);
     const float X = (yy + cx) * T.white[0], Yw = yy * T.white[1], Z = (yy - cz) * T.white[2];
     float rgb[3];
 #pragma unroll
@@ -193,8 +237,8 @@ __device__ __forceinline__ void ycxcz_to_hunt_lab(const FlipTaps &T, float Y, fl
     float xyz[3];
 #pragma unroll
     for (int i = 0; i < 3; i++)
-        xyz[i] = fmaf(T.rgb2xyz[3 * i], rgb[0], fmaf(T.rgb2xyz[3 * i + 1], rgb[1], T.rgb2xyz[3 * i + 2] * rgb[2])) /
-                 T.white[i];
+        xyz[i] = fmaf(T.rgb2xyz[3 * i], rgb[0], fmaf(T.rgb2xyz[3 * i + 1], rgb[1], T.rgb2xyz[3 * i + 2] * rgb[2])) *
+                 T.inv_white[i];
     xyzn_to_lab(xyz[0], xyz[1], xyz[2], lab);
     lab[1] *= 0.01f * lab[0];
     lab[2] *= 0.01f * lab[0];
@@ -310,10 +354,10 @@ __global__ void __launch_bounds__(VT) flip_vpass_kernel(FlipArgs args, const __g
         // colour error (spatial_detection.glsl:67-82)
         const float d0 = lab[0][0] - lab[1][0], d1 = lab[0][1] - lab[1][1], d2 = lab[0][2] - lab[1][2];
         const float hy = fabsf(d0) + sqrtf(fmaf(d1, d1, d2 * d2));
-        const float de = powf(hy, 0.7f);
+        const float de = pow_nonneg(hy, 0.7f);
         const float pcc = 0.4f * T.cmax;
         const float dec = de < pcc ? (0.95f / pcc) * de : 0.95f + ((de - pcc) / (T.cmax - pcc)) * (1.0f - 0.95f);
-        const float val = powf(dec, 1.0f - def);
+        const float val = pow_nonneg(dec, 1.0f - def);
         if (P.map) P.map[(long long)y * P.w + x] = val;
         dsum += double(val);
     }
@@ -411,7 +455,10 @@ void make_taps(double ppd, FlipTaps &T) {
         T.rgb2xyz[i] = float(m[i]);
         T.xyz2rgb[i] = float(mi[i]);
     }
-    for (int i = 0; i < 3; i++) T.white[i] = T.rgb2xyz[3 * i] + T.rgb2xyz[3 * i + 1] + T.rgb2xyz[3 * i + 2];
+    for (int i = 0; i < 3; i++) {
+        T.white[i] = T.rgb2xyz[3 * i] + T.rgb2xyz[3 * i + 1] + T.rgb2xyz[3 * i + 2];
+        T.inv_white[i] = 1.0f / T.white[i];
+    }
     // cmax = HyAB(Hunt(green), Hunt(blue))^0.7 (spatial_detection.glsl:73-81), host double
     auto lab_of = [&](double r, double g, double b, double lab[3]) {
         double xyz[3];
