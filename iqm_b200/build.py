@@ -35,6 +35,26 @@ def stale():
     return any(os.path.getmtime(f) > t for f in sources() + headers())
 
 
+HOST_SRC = ["methods.cpp", "args.cpp", "png_io.cpp", "iqm_cuda.cpp", "main.cpp"]
+CLI = os.path.join(HERE, "bin", "IQM")
+CXX = os.environ.get("IQM_CXX", "/usr/bin/g++")
+
+
+def build_cli(force=False, verbose=False):
+    """Builds the IQM command line (iqm_b200/host) against libiqm_cuda.so."""
+    srcs = [os.path.join(HERE, "host", f) for f in HOST_SRC]
+    deps = srcs + glob.glob(os.path.join(HERE, "host", "*.h*")) + [LIB]
+    if not force and os.path.exists(CLI) and all(os.path.getmtime(f) <= os.path.getmtime(CLI) for f in deps):
+        return CLI
+    os.makedirs(os.path.dirname(CLI), exist_ok=True)
+    cmd = [CXX, "-O2", "-std=c++20", "-Wall", "-I", os.path.join(ROOT, "include"), "-o", CLI] + srcs + [
+        "-L", HERE, "-liqm_cuda", "-lz", "-Wl,-rpath,$ORIGIN/.."]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return CLI
+
+
 def build(force=False, verbose=False):
     if not force and not stale():
         return LIB
@@ -48,3 +68,4 @@ def build(force=False, verbose=False):
 
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True)
+    build_cli(force="--force" in sys.argv, verbose=True)

@@ -1,0 +1,23 @@
+// PNG (and binary PNM) input, 8-bit grey PNG output, for the command-line front end.
+// Decoding always yields RGBA8 like the reference's stbi_load(..., 4) (src/main.cpp:37-57):
+// grey -> R=G=B, missing alpha -> 255, 16-bit samples -> their high byte, palettes expanded.
+#ifndef IQM_HOST_PNG_IO_H
+#define IQM_HOST_PNG_IO_H
+
+#include <string>
+#include <vector>
+
+#include "input_image.h"
+
+namespace IQM {
+// Throws std::runtime_error("Failed to load image '<path>', reason: ...") on failure.
+InputImage load_image(const std::string &path);
+// 8-bit single-channel PNG; returns false on failure.
+bool write_grey_png(const std::string &path, int width, int height, const std::vector<unsigned char> &pixels);
+// Decoders exposed for tests: whole file contents in, RGBA8 out.
+InputImage decode_png(const std::vector<unsigned char> &file);
+InputImage decode_pnm(const std::vector<unsigned char> &file);
+std::vector<unsigned char> encode_grey_png(int width, int height, const std::vector<unsigned char> &pixels);
+}  // namespace IQM
+
+#endif

@@ -1,0 +1,114 @@
+"""CPU tests of the C++ command line: argument handling and error behaviour of src/main.cpp and
+src/args.cpp, and the PNG/PNM decoder against PIL (colour types, bit depths, palettes,
+transparency, Adam7 interlacing)."""
+import os
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HOST = os.path.join(ROOT, "iqm_b200", "host")
+
+
+@pytest.fixture(scope="module")
+def cli():
+    from iqm_b200 import build
+    build.build()
+    return build.build_cli()
+
+
+@pytest.fixture(scope="module")
+def png_check(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("native") / "png_check")
+    subprocess.run(["/usr/bin/g++", "-O1", "-std=c++20", "-I", HOST, "-o", exe,
+                    os.path.join(ROOT, "tests", "native", "png_check.cpp"), os.path.join(HOST, "png_io.cpp"), "-lz"],
+                   check=True)
+    return exe
+
+
+def decode(png_check, path):
+    out = subprocess.run([png_check, path], capture_output=True, check=True).stdout
+    w, h = struct.unpack("<II", out[:8])
+    return np.frombuffer(out[8:], np.uint8).reshape(h, w, 4)
+
+
+def pil_rgba(path):
+    from PIL import Image
+    im = Image.open(path)
+    if im.mode in ("I;16", "I;16B", "I"):
+        a = (np.asarray(im).astype(np.uint32) >> 8).astype(np.uint8)
+        rgba = np.stack([a, a, a, np.full_like(a, 255)], -1)
+        return rgba
+    return np.asarray(im.convert("RGBA"))
+
+
+@pytest.mark.parametrize("mode", ["L", "LA", "RGB", "RGBA", "P", "1", "I;16"])
+@pytest.mark.parametrize("interlace", [False, True])
+def test_png_decoder_matches_pil(png_check, tmp_path, mode, interlace):
+    from PIL import Image
+    rng = np.random.default_rng(hash(mode) % 1000)
+    h, w = 37, 53
+    if mode == "I;16":
+        im = Image.fromarray(rng.integers(0, 65536, (h, w), dtype=np.uint16))
+    elif mode == "1":
+        im = Image.fromarray(rng.integers(0, 2, (h, w), dtype=np.uint8) * 255).convert("1")
+    elif mode == "P":
+        im = Image.fromarray(rng.integers(0, 256, (h, w, 3), dtype=np.uint8)).convert("P", palette=Image.ADAPTIVE, colors=50)
+    else:
+        ch = {"L": 1, "LA": 2, "RGB": 3, "RGBA": 4}[mode]
+        arr = rng.integers(0, 256, (h, w, ch), dtype=np.uint8)
+        im = Image.fromarray(arr[..., 0] if ch == 1 else arr, mode=mode)
+    path = str(tmp_path / "t.png")
+    im.save(path, interlace=interlace)
+    assert np.array_equal(decode(png_check, path), pil_rgba(path))
+
+
+def test_pnm_decoder(png_check, tmp_path):
+    from PIL import Image
+    rng = np.random.default_rng(5)
+    arr = rng.integers(0, 256, (20, 30, 3), dtype=np.uint8)
+    path = str(tmp_path / "t.ppm")
+    Image.fromarray(arr).save(path)
+    got = decode(png_check, path)
+    assert np.array_equal(got[..., :3], arr) and np.all(got[..., 3] == 255)
+
+
+def test_grey_png_encoder_round_trip(png_check, tmp_path):
+    from PIL import Image
+    rng = np.random.default_rng(6)
+    px = rng.integers(0, 256, (23, 41), dtype=np.uint8)
+    png = subprocess.run([png_check, "--encode", "41", "23"], input=px.tobytes(), capture_output=True, check=True).stdout
+    path = str(tmp_path / "g.png")
+    open(path, "wb").write(png)
+    assert np.array_equal(np.asarray(Image.open(path)), px)
+
+
+def test_cli_argument_errors(cli):
+    # src/args.cpp:32-34 and :52-60: unknown or missing arguments throw outside main's try block
+    r = subprocess.run([cli, "--method", "SSIM_CPU", "--input", "a", "--ref", "b"], capture_output=True, text=True)
+    assert r.returncode != 0 and "Unknown method" in r.stderr
+    r = subprocess.run([cli, "--input", "a", "--ref", "b"], capture_output=True, text=True)
+    assert r.returncode != 0 and "missing method" in r.stderr
+    r = subprocess.run([cli, "--method", "FSIM", "--ref", "b"], capture_output=True, text=True)
+    assert r.returncode != 0 and "missing input" in r.stderr
+
+
+def test_cli_load_and_size_errors(cli, tmp_path):
+    from PIL import Image
+    r = subprocess.run([cli, "--method", "SSIM", "--input", str(tmp_path / "none.png"), "--ref", "x"],
+                       capture_output=True, text=True)
+    assert r.returncode == 255 and "Failed to load image" in r.stderr
+    a, b = str(tmp_path / "a.png"), str(tmp_path / "b.png")
+    Image.new("RGB", (10, 12)).save(a)
+    Image.new("RGB", (11, 12)).save(b)
+    r = subprocess.run([cli, "--method", "FLIP", "--input", a, "--ref", b], capture_output=True, text=True)
+    assert r.returncode == 255 and "Compared images must have the same size" in r.stderr
+
+
+def test_cli_cw_ssim_is_a_no_op(cli, tmp_path):
+    # src/main.cpp:275-276: CW_SSIM_CPU is accepted and does nothing
+    r = subprocess.run([cli, "--method", "CW_SSIM_CPU", "--input", "a", "--ref", "b", "-v"], capture_output=True,
+                       text=True)
+    assert r.returncode == 0 and r.stdout.strip() == "Selected method: CW-SSIM"
