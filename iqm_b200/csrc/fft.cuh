@@ -380,3 +380,61 @@ __device__ inline float2 *fft_warp(float2 *a, float2 *b, const FftLen &P, const 
 }
 
 }  // namespace iqm
+
+namespace iqm {
+
+// ---------------------------------------------------------------------------------------------
+// Fixed-length warp engine: the radix sequence is a template parameter pack, so every stride,
+// quotient and loop bound is a compile-time constant and the butterflies carry no runtime index
+// arithmetic beyond the lane number.  Same stage rule and twiddle layout as the runtime engine.
+template <int N, int L, int... Rs>
+struct FixedStages;
+
+template <int N, int L>
+struct FixedStages<N, L> {
+    static __device__ __forceinline__ float2 *run(float2 *in, float2 *out, const float2 *, int, float) {
+        __syncwarp();
+        return in;
+    }
+};
+
+template <int N, int L, int P, int... Rs>
+struct FixedStages<N, L, P, Rs...> {
+    static __device__ __forceinline__ float2 *run(float2 *in, float2 *out, const float2 *stw, int stw_off, float s) {
+        constexpr int Q = N / P;
+        __syncwarp();
+        const int lane = threadIdx.x & 31;
+#pragma unroll
+        for (int it = 0; it < (Q + 31) / 32; it++) {
+            const int j = lane + 32 * it;
+            if ((Q % 32 == 0) || j < Q) {
+                const int jl = j / L, k = j - jl * L;
+                float2 v[P];
+#pragma unroll
+                for (int r = 0; r < P; r++) v[r] = in[j + r * Q];
+                if (L > 1 && k != 0) {
+                    const float2 *w = stw + stw_off + k * (P - 1) - 1;
+#pragma unroll
+                    for (int r = 1; r < P; r++) v[r] = cmul(v[r], make_float2(w[r].x, -s * w[r].y));
+                }
+                dft_small<P>(v, s);
+                const int base = jl * L * P + k;
+#pragma unroll
+                for (int r = 0; r < P; r++) out[base + r * L] = v[r];
+            }
+        }
+        return FixedStages<N, L * P, Rs...>::run(out, in, stw, stw_off + (P - 1) * L, s);
+    }
+};
+
+// Plan types: a length and its radix sequence (must match what the host planner picks for N,
+// since the stage-twiddle table is laid out for that sequence).
+template <int N, int... Rs>
+struct FixedPlan {
+    static constexpr int n = N;
+    static __device__ __forceinline__ float2 *run(float2 *a, float2 *b, const float2 *stw, float s) {
+        return FixedStages<N, 1, Rs...>::run(a, b, stw, 0, s);
+    }
+};
+
+}  // namespace iqm

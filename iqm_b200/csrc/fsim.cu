@@ -26,6 +26,7 @@
 // them, so stages synchronise with __syncwarp only.
 #include <algorithm>
 #include <cmath>
+#include <initializer_list>
 #include <map>
 
 #include "fft.cuh"
@@ -194,12 +195,32 @@ __global__ void __launch_bounds__(FT) fsim_ingest_kernel(FsimGroup g) {
 // Transform kernels.  Shared memory of every transform CTA starts with the stage twiddles of its
 // length (FftLen::stw), followed by per-warp work buffers: a warp transforms NB sequences at once
 // (buffer a: NB x wl, buffer b: NB x wl), which keeps the lanes busy on stages with few butterflies.
-constexpr int NB = 1;
+constexpr int NB = 1;  // the transform engines run one sequence per warp
 
 __device__ __forceinline__ float2 *warp_area(float2 *base, int warp, int wl) { return base + size_t(warp) * 2 * NB * wl; }
 
+// Transform engines: the runtime-planned warp engine for any length, or a fixed-length one whose
+// radix sequence is compiled in (the host picks it only when it equals the length's own plan, so
+// the stage twiddle table in shared memory has the layout it expects).
+struct GenericEngine {
+    static __device__ __forceinline__ float2 *run(float2 *a, float2 *b, const FftLen &L, const float2 *stw, float s,
+                                                  int wl) {
+        return iqm::fft_warp(a, b, L, stw, s, 1, wl);
+    }
+};
+template <class FP>
+struct FixedEngine {
+    static __device__ __forceinline__ float2 *run(float2 *a, float2 *b, const FftLen &, const float2 *stw, float s,
+                                                  int) {
+        return FP::run(a, b, stw, s);
+    }
+};
+using Engine270 = FixedEngine<iqm::FixedPlan<270, 5, 3, 3, 3, 2>>;
+using Engine480 = FixedEngine<iqm::FixedPlan<480, 5, 3, 8, 4>>;
+
 // forward transform (src/gpu/fsim/fsim.cpp:270-368: luma as complex (Y, 0), sign -1, unscaled),
 // NB rows per warp.
+template <class Eng>
 __global__ void __launch_bounds__(FT, 1) fsim_fwd_rows_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl) {
     extern __shared__ float2 sm[];
     const int tl = iqm::stage_twiddle_len(L);
@@ -215,7 +236,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_fwd_rows_kernel(FsimGroup g, const
     const float *Y = g.yiq + (size_t(plane) * 3 + 2) * g.n + size_t(y0) * g.w2;
     for (int t = 0; t < nb; t++)
         for (int x = lane; x < g.w2; x += 32) a[t * wl + x] = make_float2(Y[size_t(t) * g.w2 + x], 0.f);
-    const float2 *res = iqm::fft_warp(a, b, L, sm, -1.f, NB == 1 ? 1 : nb, wl);
+    const float2 *res = Eng::run(a, b, L, sm, -1.f, wl);
     float2 *S = g.spec + size_t(plane) * g.n + size_t(y0) * g.w2;
     for (int t = 0; t < nb; t++)
         for (int x = lane; x < g.w2; x += 32) S[size_t(t) * g.w2 + x] = res[t * wl + x];
@@ -225,6 +246,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_fwd_rows_kernel(FsimGroup g, const
 // is loaded and stored cooperatively and each warp transforms NB of its columns.
 __device__ __forceinline__ int slab_parity(float2 *res, float2 *a) { return res == a ? 0 : 1; }
 
+template <class Eng>
 __global__ void __launch_bounds__(FT, 1) fsim_fwd_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int lw) {
     extern __shared__ float2 sm[];
     __shared__ int parity;
@@ -245,7 +267,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_fwd_cols_kernel(FsimGroup g, const
     const int nbw = min(NB, nc - warp * NB);
     if (nbw > 0) {
         float2 *a = warp_area(work, warp, wl);
-        float2 *res = iqm::fft_warp(a, a + NB * wl, L, sm, -1.f, NB == 1 ? 1 : nbw, wl);
+        float2 *res = Eng::run(a, a + NB * wl, L, sm, -1.f, wl);
         if (warp == 0 && (threadIdx.x & 31) == 0) parity = slab_parity(res, a);
     }
     __syncthreads();
@@ -259,6 +281,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_fwd_cols_kernel(FsimGroup g, const
 // inverse transform, pass 1 (along y) of the 4 filtered spectra of orientation o:
 // spectrum x H[o*4+s] (fsim_filter_combinations.glsl:53-56), sign +1.  consts_mode uses a
 // spectrum of ones, i.e. transforms the filters themselves (block 0 of the reference's buffer).
+template <class Eng>
 __global__ void __launch_bounds__(FT, 1) fsim_inv_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int lw, int consts_mode) {
     extern __shared__ float2 sm[];
     __shared__ int parity;
@@ -293,7 +316,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_cols_kernel(FsimGroup g, const
                     a[t * wl + y] = make_float2(hv * v.x, hv * v.y);
                 }
             }
-            float2 *res = iqm::fft_warp(a, a + NB * wl, L, sm, 1.f, NB == 1 ? 1 : nbw, wl);
+            float2 *res = Eng::run(a, a + NB * wl, L, sm, 1.f, wl);
             if (warp == 0 && lane == 0) parity = slab_parity(res, a);
         }
         __syncthreads();
@@ -331,6 +354,7 @@ __device__ __forceinline__ void response_sums(const float2 v[4], float invN, flo
 // inverse transform, pass 2 (along x): a CTA handles rr rows with WPR = 4/NB warps per row;
 // warp (r, h) transforms scales h*NB .. h*NB+NB-1 of row y0 + r.  consts_mode (rr = 1) instead accumulates, per row, sum_s Re_s^2 N and
 // sum_{i<j} Re_i Re_j N (shaders/fsim/fsim_mult_filters.glsl:37-58) over p < ceil(N/2) and all p.
+template <class Eng>
 __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int rr, int consts_mode,
                                                               double *rowsums) {
     extern __shared__ float2 sm[];
@@ -354,7 +378,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_kernel(FsimGroup g, const
                 const float2 *src = g.T + (size_t(plane) * 16 + o * 4 + h * NB + t) * g.n + size_t(y) * w2;
                 for (int x = lane; x < w2; x += 32) a[t * wl + x] = src[x];
             }
-            float2 *res = iqm::fft_warp(a, a + NB * wl, L, sm, 1.f, NB, wl);
+            float2 *res = Eng::run(a, a + NB * wl, L, sm, 1.f, wl);
             if (warp == 0 && lane == 0) parity = slab_parity(res, a);
         }
     }
@@ -662,8 +686,33 @@ struct Shapes {
     int lw_fcols;         // log2 warps per CTA, forward columns (NB columns per warp)
     int lw_icols;         // log2 warps per CTA, inverse columns
     int rr;               // rows per CTA in the inverse row pass (0: sequential kernel)
+    int row_eng, col_eng; // transform engine of the row / column length (engine_id)
     size_t sm_rows, sm_fcols, sm_icols, sm_irows;
 };
+
+// Compiled transform engine serving a length: 1 (270) or 2 (480) when the length's own plan is
+// exactly the compiled radix sequence, else 0 (the runtime-planned engine).
+int engine_id(const iqm::FftLen &L) {
+    auto is = [&](int n, std::initializer_list<int> rs) {
+        if (L.bluestein || L.n != n || L.nst != int(rs.size())) return false;
+        int i = 0;
+        for (int r : rs)
+            if (L.radix[i++] != r) return false;
+        return true;
+    };
+    if (is(270, {5, 3, 3, 3, 2})) return 1;
+    if (is(480, {5, 3, 8, 4})) return 2;
+    return 0;
+}
+
+template <class F>
+void with_engine(int id, F &&f) {
+    switch (id) {
+        case 1: f(Engine270{}); break;
+        case 2: f(Engine480{}); break;
+        default: f(GenericEngine{}); break;
+    }
+}
 
 int lw_fit(size_t fixed, size_t per_warp) {
     int lw = 3;  // up to 8 warps
@@ -676,6 +725,8 @@ Shapes shapes_for(const iqm::FsimPlan &P) {
     const size_t f2 = sizeof(float2);
     s.wl_row = iqm::fft_work_len(P.row);
     s.wl_col = iqm::fft_work_len(P.col);
+    s.row_eng = engine_id(P.row);
+    s.col_eng = engine_id(P.col);
     const size_t twr = size_t((iqm::stage_twiddle_len(P.row) + 1) & ~1) * f2;
     const size_t twc = size_t((iqm::stage_twiddle_len(P.col) + 1) & ~1) * f2;
     const size_t warp_row = 2 * NB * size_t(s.wl_row) * f2, warp_col = 2 * NB * size_t(s.wl_col) * f2;
@@ -700,12 +751,17 @@ Shapes shapes_for(const iqm::FsimPlan &P) {
 }
 
 void configure_kernels(const Shapes &s) {
-    set_smem((const void *)fsim_fwd_rows_kernel, s.sm_rows);
-    set_smem((const void *)fsim_fwd_cols_kernel, s.sm_fcols);
-    set_smem((const void *)fsim_inv_cols_kernel, s.sm_icols);
-    if (s.rr) {
-        set_smem((const void *)fsim_inv_rows_kernel, s.sm_irows);
-    } else {
+    with_engine(s.row_eng, [&](auto e) {
+        using E = decltype(e);
+        set_smem((const void *)fsim_fwd_rows_kernel<E>, s.sm_rows);
+        if (s.rr) set_smem((const void *)fsim_inv_rows_kernel<E>, s.sm_irows);
+    });
+    with_engine(s.col_eng, [&](auto e) {
+        using E = decltype(e);
+        set_smem((const void *)fsim_fwd_cols_kernel<E>, s.sm_fcols);
+        set_smem((const void *)fsim_inv_cols_kernel<E>, s.sm_icols);
+    });
+    if (!s.rr) {
         set_smem((const void *)fsim_inv_rows_seq_kernel, s.sm_irows);
     }
 }
@@ -713,12 +769,17 @@ void configure_kernels(const Shapes &s) {
 void launch_inv_rows(const FsimGroup &g, const iqm::FsimPlan &P, const Shapes &s, int planes, int consts_mode,
                      double *rowsums, cudaStream_t st) {
     if (s.rr && !(consts_mode && s.rr != 1)) {
-        fsim_inv_rows_kernel<<<dim3(iqm::ceil_div(P.h2, s.rr), 4, planes), 32 * (4 / NB) * s.rr, s.sm_irows, st>>>(
-            g, P.row, s.wl_row, s.rr, consts_mode, rowsums);
+        with_engine(s.row_eng, [&](auto e) {
+            fsim_inv_rows_kernel<decltype(e)>
+                <<<dim3(iqm::ceil_div(P.h2, s.rr), 4, planes), 32 * (4 / NB) * s.rr, s.sm_irows, st>>>(
+                    g, P.row, s.wl_row, s.rr, consts_mode, rowsums);
+        });
     } else if (s.rr) {  // consts mode runs one row per CTA
         const size_t twr = size_t((iqm::stage_twiddle_len(P.row) + 1) & ~1) * sizeof(float2);
-        fsim_inv_rows_kernel<<<dim3(P.h2, 4, planes), 32 * (4 / NB), twr + (s.sm_irows - twr) / s.rr, st>>>(
-            g, P.row, s.wl_row, 1, 1, rowsums);
+        with_engine(s.row_eng, [&](auto e) {
+            fsim_inv_rows_kernel<decltype(e)><<<dim3(P.h2, 4, planes), 32 * (4 / NB), twr + (s.sm_irows - twr) / s.rr, st>>>(
+                g, P.row, s.wl_row, 1, 1, rowsums);
+        });
     } else {
         fsim_inv_rows_seq_kernel<<<dim3(P.h2, 4, planes), FT, s.sm_irows, st>>>(g, P.row, s.wl_row, consts_mode,
                                                                                  rowsums);
@@ -728,8 +789,10 @@ void launch_inv_rows(const FsimGroup &g, const iqm::FsimPlan &P, const Shapes &s
 void launch_inv_cols(const FsimGroup &g, const iqm::FsimPlan &P, const Shapes &s, int planes, int consts_mode,
                      cudaStream_t st) {
     const int nw = 1 << s.lw_icols;
-    fsim_inv_cols_kernel<<<dim3(iqm::ceil_div(P.w2, NB * nw), 4, planes), 32 * nw, s.sm_icols, st>>>(
-        g, P.col, s.wl_col, s.lw_icols, consts_mode);
+    with_engine(s.col_eng, [&](auto e) {
+        fsim_inv_cols_kernel<decltype(e)><<<dim3(iqm::ceil_div(P.w2, NB * nw), 4, planes), 32 * nw, s.sm_icols, st>>>(
+            g, P.col, s.wl_col, s.lw_icols, consts_mode);
+    });
 }
 
 iqm::FsimPlan *get_plan(iqm_ctx *ctx, int w2, int h2) {
@@ -894,11 +957,17 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
         IQM_CHECK_CUDA(cudaMemsetAsync(g.counters, 0, sizeof(unsigned) * G, st));
         launch_ingest(g, F_uniform, tiles, st);
         iqm::check_launch(ctx, "fsim_ingest_kernel");
-        fsim_fwd_rows_kernel<<<dim3(iqm::ceil_div(h2, NB << s.lw_rows), 2 * G), 32 << s.lw_rows, s.sm_rows, st>>>(
-            g, P->row, s.wl_row);
+        with_engine(s.row_eng, [&](auto e) {
+            fsim_fwd_rows_kernel<decltype(e)>
+                <<<dim3(iqm::ceil_div(h2, NB << s.lw_rows), 2 * G), 32 << s.lw_rows, s.sm_rows, st>>>(g, P->row,
+                                                                                                    s.wl_row);
+        });
         iqm::check_launch(ctx, "fsim_fwd_rows_kernel");
-        fsim_fwd_cols_kernel<<<dim3(iqm::ceil_div(w2, NB << s.lw_fcols), 2 * G), 32 << s.lw_fcols, s.sm_fcols, st>>>(
-            g, P->col, s.wl_col, s.lw_fcols);
+        with_engine(s.col_eng, [&](auto e) {
+            fsim_fwd_cols_kernel<decltype(e)>
+                <<<dim3(iqm::ceil_div(w2, NB << s.lw_fcols), 2 * G), 32 << s.lw_fcols, s.sm_fcols, st>>>(
+                    g, P->col, s.wl_col, s.lw_fcols);
+        });
         iqm::check_launch(ctx, "fsim_fwd_cols_kernel");
         for (int c0 = 0; c0 < G; c0 += chunk) {
             FsimGroup gc = g;
