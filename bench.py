@@ -32,8 +32,10 @@ WORKLOADS = {
     "flip": ("flip_1080p_rgb_67ppd", "rgb_blockquant_pair", 1),
     "msvd": ("msvd_1080p_rgb", "rgb_blockquant_pair", 1),
 }
-# kernel whose CUDA-event duration the roofline figure uses, per metric
-DOMINANT = {"ssim": "ssim_kernel", "msvd": "msvd_block_kernel", "flip": "flip_kernel", "fsim": "fsim pipeline"}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of each metric's dominant
+# kernel from an ncu capture of this benchmark, with the pairs that launch processed; the summaries
+# under profiles/ give the commands.  Scaled by pairs per launch when the live launch differs.
+TRAFFIC = {}
 
 
 def metric_name(metric):
@@ -259,18 +261,34 @@ def main():
     ms_per_step = ms / args.steps
     value = world * B / (ms_per_step / 1e3)
 
-    # roofline of the dominant kernel: algorithmic bytes (each RGBA8 input read once) / duration
+    # per-kernel device time: the same K steps again with an event after every launch on the
+    # library's stream (kept out of the throughput timing above)
+    rt.set_kernel_timing(True)
+    for _ in range(args.steps):
+        step()
+    ktimes = rt.kernel_times()
+    rt.set_kernel_timing(False)
+    ktotal = sum(t for _, t in ktimes.values()) or 1.0
+    kname, (klaunch, kms) = max(ktimes.items(), key=lambda kv: kv[1][1])
+    kernels = {k: {"launches": n, "avg_us": 1e3 * t / max(1, n), "share": t / ktotal} for k, (n, t) in ktimes.items()}
+
+    # roofline of the dominant kernel: algorithmic bytes (each RGBA8 input read once, 8 B per pixel
+    # pair) of the pairs one launch processes / that kernel's average launch duration
     alg_bytes = B * 2 * img_bytes
-    achieved = alg_bytes / (ms_per_step / 1e3) / 1e9
+    pairs_per_launch = B * args.steps / max(1, klaunch)
+    alg_launch = pairs_per_launch * 2 * img_bytes
+    avg_s = kms / max(1, klaunch) / 1e3
+    achieved = alg_launch / avg_s / 1e9
+    traffic = None
+    if metric in TRAFFIC and TRAFFIC[metric]["kernel"] == kname:
+        t = TRAFFIC[metric]
+        traffic = t["bytes_per_launch"] * pairs_per_launch / t["pairs_per_launch"]
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-            "frac": achieved / hbm_peak, "traffic": None, "kernel": DOMINANT[metric],
-            "peak_source": peak_note, "alg_bytes_per_launch": alg_bytes}
-    tr = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tr):
-        try:
-            roof["traffic"] = json.load(open(tr)).get(metric)
-        except Exception:
-            pass
+            "frac": achieved / hbm_peak, "traffic": traffic, "kernel": kname,
+            "peak_source": peak_note, "alg_bytes_per_launch": alg_launch, "pairs_per_launch": pairs_per_launch,
+            "avg_launch_us": avg_s * 1e6, "kernel_share": ktimes[kname][1] / ktotal,
+            "pipeline_frac": alg_bytes / (ms_per_step / 1e3) / 1e9 / hbm_peak,
+            "timing": "CUDA events on the library stream around every launch, second pass of the K steps"}
 
     # end to end: host API with pinned host images and host scores
     e2e = None
@@ -328,7 +346,7 @@ def main():
         "config": {"workload": WORKLOADS[metric][0], "pairs_per_step": B, "width": W1080, "height": H1080,
                    "precision": "fp32", "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (%.0f MB per step), no flush" % (alg_bytes / 1e6)},
-        "roofline": roof, "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "clocks": clk,
+        "roofline": roof, "kernels": kernels, "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(metric, host_pairs, args.cpu_seconds)

@@ -158,6 +158,17 @@ int iqm_fsim_batch(iqm_ctx *ctx, const iqm_pair *pairs, int n, iqm_precision pre
  * benchmark's launch accounting). */
 int iqm_last_launch_count(const iqm_ctx *ctx);
 
+/* Per-kernel device timing, the device-side counterpart of the reference's Timestamps
+ * (src/timestamps.h:11-40, printed by `-v`).  With enable != 0 the context records a CUDA event on
+ * its stream after every kernel launch and after every copy or memset it enqueues, and charges each
+ * kernel the interval since the event before it; enabling or disabling clears the totals.  The
+ * events add a little work between launches, so time throughput with timing off. */
+int iqm_set_kernel_timing(iqm_ctx *ctx, int enable);
+
+/* Waits for the context stream and writes one line per kernel name, "name launches total_ms\n",
+ * into buf (NUL-terminated); IQM_EINVAL if cap is too small. */
+int iqm_kernel_times(iqm_ctx *ctx, char *buf, size_t cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,7 +33,8 @@ EXPORTS = (
     "iqm_device_name", "iqm_ssim_default_params", "iqm_ssim", "iqm_msvd", "iqm_flip_default_params",
     "iqm_flip_ppd", "iqm_flip", "iqm_fsim", "iqm_ssim_dev", "iqm_msvd_dev", "iqm_flip_dev",
     "iqm_fsim_dev", "iqm_ssim_batch", "iqm_msvd_batch", "iqm_flip_batch", "iqm_fsim_batch",
-    "iqm_last_launch_count", "iqm_fsim_plan_constants", "iqm_ssim_noalloc",
+    "iqm_last_launch_count", "iqm_fsim_plan_constants", "iqm_ssim_noalloc", "iqm_set_kernel_timing",
+    "iqm_kernel_times",
 )
 
 
@@ -100,6 +101,8 @@ def load_library(path=LIB_PATH):
     L.iqm_last_launch_count.argtypes = [vp]
     L.iqm_fsim_plan_constants.argtypes = [vp, ip, ip, ip, dp, dp, dp]
     L.iqm_ssim_noalloc.argtypes = [vp, vp, ip, ip, ctypes.c_size_t, ctypes.POINTER(SSIMParams), vp, vp, vp]
+    L.iqm_set_kernel_timing.argtypes = [vp, ip]
+    L.iqm_kernel_times.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
     _lib = L
     return L
 
@@ -144,6 +147,20 @@ class Runtime:
 
     def last_launch_count(self):
         return self.L.iqm_last_launch_count(self.h)
+
+    def set_kernel_timing(self, enable):
+        """Per-kernel device timing on this context's stream (clears the totals)."""
+        self.check(self.L.iqm_set_kernel_timing(self.h, 1 if enable else 0))
+
+    def kernel_times(self):
+        """{kernel name: (launches, total ms)} since timing was enabled; waits for the stream."""
+        buf = ctypes.create_string_buffer(1 << 16)
+        self.check(self.L.iqm_kernel_times(self.h, buf, len(buf)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, n, ms = line.rsplit(" ", 2)
+            out[name] = (int(n), float(ms))
+        return out
 
     def close(self):
         if getattr(self, "h", None):

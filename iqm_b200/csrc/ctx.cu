@@ -11,6 +11,10 @@ namespace {
 thread_local std::string g_create_error;
 }
 
+namespace iqm {
+static void timing_release(iqm_ctx *ctx);
+}
+
 extern "C" __attribute__((visibility("default"))) int iqm_create(int device, iqm_ctx **out) {
     if (!out) return IQM_EINVAL;
     *out = nullptr;
@@ -61,6 +65,7 @@ extern "C" __attribute__((visibility("default"))) int iqm_destroy(iqm_ctx *ctx) 
     ctx->scores.release();
     ctx->pinned.release();
     ctx->ring.release();
+    iqm::timing_release(ctx);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return IQM_OK;
@@ -120,6 +125,7 @@ void *upload_bytes(iqm_ctx *ctx, DevBuf &dst, const void *src, size_t bytes) {
     void *d = dst.get(bytes, ctx->stream);
     IQM_CHECK_CUDA(cudaMemcpyAsync(d, r.host[slot], bytes, cudaMemcpyHostToDevice, ctx->stream));
     IQM_CHECK_CUDA(cudaEventRecord(r.ev[slot], ctx->stream));
+    timing_mark(ctx, nullptr);
     return d;
 }
 
@@ -149,7 +155,79 @@ std::vector<iqm_pair> upload_pairs(iqm_ctx *ctx, const iqm_pair *pairs, int n) {
         dev[i].input = din;
         dev[i].ref = dref;
     }
+    timing_mark(ctx, nullptr);
     return dev;
 }
 
+// Charges every kernel mark the interval since the mark before it, then recycles the events.
+// Waits for the context stream.
+static void timing_collect(iqm_ctx *ctx) {
+    if (ctx->marks.empty()) return;
+    IQM_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (size_t i = 1; i < ctx->marks.size(); i++) {
+        if (!ctx->marks[i].first) continue;
+        float ms = 0.f;
+        IQM_CHECK_CUDA(cudaEventElapsedTime(&ms, ctx->marks[i - 1].second, ctx->marks[i].second));
+        auto &acc = ctx->kernel_ms[ctx->marks[i].first];
+        acc.first++;
+        acc.second += ms;
+    }
+    // the last mark starts the next interval
+    auto last = ctx->marks.back();
+    for (size_t i = 0; i + 1 < ctx->marks.size(); i++) ctx->event_pool.push_back(ctx->marks[i].second);
+    ctx->marks.clear();
+    ctx->marks.push_back({nullptr, last.second});
+}
+
+static void timing_release(iqm_ctx *ctx) {
+    for (auto &m : ctx->marks) cudaEventDestroy(m.second);
+    for (auto e : ctx->event_pool) cudaEventDestroy(e);
+    ctx->marks.clear();
+    ctx->event_pool.clear();
+}
+
+void timing_mark(iqm_ctx *ctx, const char *kernel) {
+    if (!ctx->timing) return;
+    // A stream switch or a long run: settle what is recorded so far (the settled mark stays the
+    // start of the next interval).
+    if (ctx->marks.size() >= 16384) timing_collect(ctx);
+    cudaEvent_t ev;
+    if (!ctx->event_pool.empty()) {
+        ev = ctx->event_pool.back();
+        ctx->event_pool.pop_back();
+    } else {
+        IQM_CHECK_CUDA(cudaEventCreate(&ev));
+    }
+    const cudaError_t e = cudaEventRecord(ev, ctx->stream);
+    if (e != cudaSuccess) {
+        ctx->event_pool.push_back(ev);
+        throw Error{IQM_ECUDA, std::string("cudaEventRecord: ") + cudaGetErrorString(e)};
+    }
+    ctx->marks.push_back({kernel, ev});
+}
+
 }  // namespace iqm
+
+extern "C" __attribute__((visibility("default"))) int iqm_set_kernel_timing(iqm_ctx *ctx, int enable) {
+    return iqm::guarded(ctx, [&] {
+        if (ctx->timing) iqm::timing_collect(ctx);
+        iqm::timing_release(ctx);
+        ctx->kernel_ms.clear();
+        ctx->timing = enable != 0;
+    });
+}
+
+extern "C" __attribute__((visibility("default"))) int iqm_kernel_times(iqm_ctx *ctx, char *buf, size_t cap) {
+    return iqm::guarded(ctx, [&] {
+        IQM_REQUIRE(buf && cap > 0, "buffer is NULL");
+        iqm::timing_collect(ctx);
+        std::string out;
+        char line[256];
+        for (const auto &kv : ctx->kernel_ms) {
+            std::snprintf(line, sizeof(line), "%s %ld %.6f\n", kv.first.c_str(), kv.second.first, kv.second.second);
+            out += line;
+        }
+        IQM_REQUIRE(out.size() < cap, "buffer too small for the kernel time report");
+        std::memcpy(buf, out.c_str(), out.size() + 1);
+    });
+}

@@ -14,9 +14,12 @@
 //                      point on (Y+16)/116, feature_filter_horizontal.glsl) and the horizontal CSF
 //                      taps (spatial_prefilter_horizontal.glsl), clamp-to-edge; 4 pixels per thread;
 //                      12 planes out;
-//   flip_vpass_kernel  32x32-pixel output tiles: the 12 planes (+ halo rows, clamp-to-edge) staged in
-//                      shared memory, vertical feature and CSF taps register-blocked 8 rows per
-//                      thread, then YCxCz -> XYZ -> linear RGB (clamped) -> L*a*b* -> Hunt
+//   flip_vcols_kernel  (radii known at compile time) 32-column strips, one warp per (image, plane,
+//                      filter) role walking down the strip with a (2R+1)-row register window, the
+//                      14 filtered values per pixel exchanged through shared memory; or
+//   flip_vpass_kernel  (any radii) 32x32-pixel output tiles: the 12 planes (+ halo rows, clamp-to-edge)
+//                      staged in shared memory, vertical feature and CSF taps register-blocked 8 rows
+//                      per thread; both then YCxCz -> XYZ -> linear RGB (clamped) -> L*a*b* -> Hunt
 //                      (spatial_prefilter.glsl:74-99), HyAB colour error (spatial_detection.glsl),
 //                      feature error (feature_detection.glsl:48-53), combine
 //                      (combine_error_maps.glsl:28) and FP64 pooling; the last CTA of a pair writes
@@ -265,6 +268,63 @@ __device__ __noinline__ ImgTerms per_image(const FlipTaps &T, float d0, float d1
     return o;
 }
 
+// Per-pixel FLIP value from the vertically filtered terms of both images, f[img] = (dx*g,
+// value*edge, ddx*g, value*point, Y*csf0, Cx*csf1, Cz*csf2): feature error
+// (feature_detection.glsl:48-53), HyAB colour error of the Hunt-adjusted L*a*b* values
+// (spatial_detection.glsl:67-82) and their combination (combine_error_maps.glsl:28).
+__device__ __forceinline__ float flip_pixel(const FlipTaps &T, const float (&f)[2][7]) {
+    float lab[2][3], dl[2], ddl[2];
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+        const ImgTerms t = per_image(T, f[m][0], f[m][1], f[m][2], f[m][3], f[m][4], f[m][5], f[m][6]);
+        lab[m][0] = t.L;
+        lab[m][1] = t.a;
+        lab[m][2] = t.b;
+        dl[m] = t.dl;
+        ddl[m] = t.ddl;
+    }
+    const float ed = fabsf(dl[0] - dl[1]), pd = fabsf(ddl[0] - ddl[1]);
+    const float def = sqrtf(rsqrtf(2.0f) * fmaxf(ed, pd));
+    const float d0 = lab[0][0] - lab[1][0], d1 = lab[0][1] - lab[1][1], d2 = lab[0][2] - lab[1][2];
+    const float hy = fabsf(d0) + sqrtf(fmaf(d1, d1, d2 * d2));
+    const float de = pow_nonneg(hy, 0.7f);
+    const float pcc = 0.4f * T.cmax;
+    const float dec = de < pcc ? (0.95f / pcc) * de : 0.95f + ((de - pcc) / (T.cmax - pcc)) * (1.0f - 0.95f);
+    return pow_nonneg(dec, 1.0f - def);
+}
+
+// Pools the CTA's FP64 partial sum; the last CTA of a pair writes the pair's mean.
+template <int NT>
+__device__ __forceinline__ void pool_tile(const FlipArgs &args, const FlipPairDev &P, int pi, int gt, double dsum,
+                                          double *red, int &is_last) {
+    for (int d = 16; d > 0; d >>= 1) dsum += __shfl_down_sync(0xffffffffu, dsum, d);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < NT / 32; i++) t += red[i];
+        args.partials[gt] = t;
+        __threadfence();
+        const unsigned prev = atomicAdd(&args.counters[pi], 1u);
+        is_last = prev == unsigned(P.ntiles - 1);
+    }
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    double t = 0.0;
+    for (int i = threadIdx.x; i < P.ntiles; i += NT) t += __ldcg(&args.partials[P.tile_base + i]);
+    for (int d = 16; d > 0; d >>= 1) t += __shfl_down_sync(0xffffffffu, t, d);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sum = 0.0;
+        for (int i = 0; i < NT / 32; i++) sum += red[i];
+        args.scores[pi] = sum / (double(P.w) * double(P.h));
+        args.counters[pi] = 0u;
+    }
+}
+
 template <int RF, int RC>
 __global__ void __launch_bounds__(VT) flip_vpass_kernel(FlipArgs args, const __grid_constant__ FlipTaps T) {
     extern __shared__ float vs[];  // [NPLANE][rows][VT_COLS]
@@ -337,56 +397,105 @@ __global__ void __launch_bounds__(VT) flip_vpass_kernel(FlipArgs args, const __g
     for (int i = 0; i < VT_RPT; i++) {
         const int y = y0 + r0 + i;
         if (x >= P.w || y >= P.h) continue;
-        float lab[2][3], dl[2], ddl[2];
-#pragma unroll
-        for (int m = 0; m < 2; m++) {
-            const ImgTerms t = per_image(T, acc[i][m][0], acc[i][m][1], acc[i][m][2], acc[i][m][3], acc[i][m][4],
-                                         acc[i][m][5], acc[i][m][6]);
-            lab[m][0] = t.L;
-            lab[m][1] = t.a;
-            lab[m][2] = t.b;
-            dl[m] = t.dl;
-            ddl[m] = t.ddl;
-        }
-        // feature error (feature_detection.glsl:48-53)
-        const float ed = fabsf(dl[0] - dl[1]), pd = fabsf(ddl[0] - ddl[1]);
-        const float def = sqrtf(rsqrtf(2.0f) * fmaxf(ed, pd));
-        // colour error (spatial_detection.glsl:67-82)
-        const float d0 = lab[0][0] - lab[1][0], d1 = lab[0][1] - lab[1][1], d2 = lab[0][2] - lab[1][2];
-        const float hy = fabsf(d0) + sqrtf(fmaf(d1, d1, d2 * d2));
-        const float de = pow_nonneg(hy, 0.7f);
-        const float pcc = 0.4f * T.cmax;
-        const float dec = de < pcc ? (0.95f / pcc) * de : 0.95f + ((de - pcc) / (T.cmax - pcc)) * (1.0f - 0.95f);
-        const float val = pow_nonneg(dec, 1.0f - def);
+        const float val = flip_pixel(T, acc[i]);
         if (P.map) P.map[(long long)y * P.w + x] = val;
         dsum += double(val);
     }
-    for (int d = 16; d > 0; d >>= 1) dsum += __shfl_down_sync(0xffffffffu, dsum, d);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dsum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int i = 0; i < VT / 32; i++) t += red[i];
-        args.partials[gt] = t;
-        __threadfence();
-        const unsigned prev = atomicAdd(&args.counters[pi], 1u);
-        is_last = prev == unsigned(P.ntiles - 1);
+    pool_tile<VT>(args, P, pi, gt, dsum, red, is_last);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Vertical pass for compile-time radii ("column walkers").  Warp w of a CTA runs role w -- one
+// (image, plane, filter) combination -- down the CTA's 32 columns over CW_BLOCKS blocks of
+// K = 2R+1 rows, keeping the last K rows of its plane in a register window whose slots are fixed
+// at compile time (slot = input row mod K), so each output row costs one coalesced load and the
+// filter's FMAs.  After every block the CTA turns the 14 filtered values of each of its K x 32
+// pixels into FLIP values (flip_pixel) from a shared-memory buffer.
+constexpr int CW_ROLES = 14;         // per image: dx*g, value*edge, ddx*g, value*point, Y*csf0, Cx*csf1, Cz*csf2
+constexpr int CW_T = 32 * CW_ROLES;  // 448 threads
+constexpr int CW_BLOCKS = 10;        // K-row blocks per CTA
+
+__host__ __device__ constexpr int cw_rows(int rf, int rc) { return CW_BLOCKS * (2 * (rf > rc ? rf : rc) + 1); }
+
+template <int TS>
+__device__ __forceinline__ float cw_tap(const FlipTaps &T, int i) {
+    return TS < 3 ? T.feat[TS][i] : T.csf[TS - 3][i];
+}
+
+// One block of K output rows of one role: window slot (j + u) % K holds image row y - R + u of
+// output row y = ybase + R + j; image row y - k is weighted by tap k + RAD (|k| <= RAD).
+template <int RAD, int TS, int K>
+__device__ __forceinline__ void cw_block(const FlipTaps &T, float (&win)[K], const float *col, int w, int h,
+                                         int ybase, float *out) {
+    constexpr int R = K / 2;
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+        const int y = min(max(ybase + j + K - 1, 0), h - 1);
+        win[(j + K - 1) % K] = __ldg(col + size_t(y) * size_t(w));
+        float acc = 0.f;
+#pragma unroll
+        for (int u = 0; u < K; u++) {
+            const int k = R - u;
+            if (k >= -RAD && k <= RAD) acc = fmaf(win[(j + u) % K], cw_tap<TS>(T, k + RAD), acc);
+        }
+        out[j * CW_ROLES * 32] = acc;
     }
-    __syncthreads();
-    if (!is_last) return;
-    __threadfence();
-    double t = 0.0;
-    for (int i = threadIdx.x; i < P.ntiles; i += VT) t += __ldcg(&args.partials[P.tile_base + i]);
-    for (int d = 16; d > 0; d >>= 1) t += __shfl_down_sync(0xffffffffu, t, d);
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int i = 0; i < VT / 32; i++) s += red[i];
-        args.scores[pi] = s / double(n);
-        args.counters[pi] = 0u;
+}
+
+template <int RF, int RC>
+__global__ void __launch_bounds__(CW_T, 2) flip_vcols_kernel(FlipArgs args, const __grid_constant__ FlipTaps T) {
+    constexpr int R = RF > RC ? RF : RC;
+    constexpr int K = 2 * R + 1;
+    constexpr int SEG = cw_rows(RF, RC);
+    __shared__ float buf[K][CW_ROLES][32];
+    __shared__ double red[CW_T / 32];
+    __shared__ int is_last;
+    const int gt = blockIdx.x;
+    const int pi = find_tile(args.pairs, args.npairs, gt);
+    const FlipPairDev P = args.pairs[pi];
+    const int local = gt - P.tile_base;
+    const int x0 = (local % P.tiles_x) * 32, y0 = (local / P.tiles_x) * SEG;
+    const int lane = threadIdx.x & 31, role = threadIdx.x >> 5;
+    const int f = role % 7, m = role / 7;
+    // plane of each role within the image's six: dx, ddx, value, Y, Cx, Cz
+    const int pl = m * 6 + (f == 0 ? 0 : f == 1 ? 2 : f == 2 ? 1 : f == 3 ? 2 : f - 1);
+    const size_t n = size_t(P.w) * size_t(P.h);
+    const float *col = args.planes + P.plane_off + size_t(pl) * n + min(x0 + lane, P.w - 1);
+    float win[K];
+#pragma unroll
+    for (int t = 0; t < K - 1; t++) win[t] = __ldg(col + size_t(min(max(y0 - R + t, 0), P.h - 1)) * size_t(P.w));
+    float *out = &buf[0][role][lane];
+    double dsum = 0.0;
+    for (int b = 0; b < CW_BLOCKS; b++) {
+        const int yb = y0 + b * K;
+        if (yb >= P.h) break;  // uniform over the CTA
+        const int ybase = yb - R;
+        switch (f) {
+            case 0: cw_block<RF, 0, K>(T, win, col, P.w, P.h, ybase, out); break;
+            case 1: cw_block<RF, 1, K>(T, win, col, P.w, P.h, ybase, out); break;
+            case 2: cw_block<RF, 0, K>(T, win, col, P.w, P.h, ybase, out); break;
+            case 3: cw_block<RF, 2, K>(T, win, col, P.w, P.h, ybase, out); break;
+            case 4: cw_block<RC, 3, K>(T, win, col, P.w, P.h, ybase, out); break;
+            case 5: cw_block<RC, 4, K>(T, win, col, P.w, P.h, ybase, out); break;
+            default: cw_block<RC, 5, K>(T, win, col, P.w, P.h, ybase, out); break;
+        }
+        __syncthreads();
+        for (int p = threadIdx.x; p < K * 32; p += CW_T) {
+            const int j = p >> 5, c = p & 31;
+            const int y = yb + j, x = x0 + c;
+            if (y >= P.h || x >= P.w) continue;
+            float v[2][7];
+#pragma unroll
+            for (int mm = 0; mm < 2; mm++)
+#pragma unroll
+                for (int q = 0; q < 7; q++) v[mm][q] = buf[j][mm * 7 + q][c];
+            const float val = flip_pixel(T, v);
+            if (P.map) P.map[size_t(y) * size_t(P.w) + x] = val;
+            dsum += double(val);
+        }
+        __syncthreads();
     }
+    pool_tile<CW_T>(args, P, pi, gt, dsum, red, is_last);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -495,6 +604,9 @@ void flip_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_fl
     FlipTaps T{};
     make_taps(ppd_of(params), T);
     const int n = int(pairs.size());
+    // the two viewing set-ups in common use get kernels with their radii built in
+    const int fixed = (T.rf == 7 && T.rc == 8) ? 1 : (T.rf == 9 && T.rc == 10) ? 2 : 0;
+    const int tile_rows = fixed == 1 ? cw_rows(7, 8) : fixed == 2 ? cw_rows(9, 10) : VT_ROWS;
     std::vector<FlipPairDev> hd(n);
     long long segs = 0, plane_floats = 0;
     int tiles = 0;
@@ -508,7 +620,7 @@ void flip_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_fl
         d.w = q.w;
         d.h = q.h;
         d.tiles_x = int(iqm::ceil_div(q.w, VT_COLS));
-        d.ntiles = d.tiles_x * int(iqm::ceil_div(q.h, VT_ROWS));
+        d.ntiles = d.tiles_x * int(iqm::ceil_div(q.h, tile_rows));
         d.tile_base = tiles;
         d.vec_ok = 0;
         d.plane_off = plane_floats;
@@ -532,24 +644,28 @@ void flip_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_fl
     a.scores = d_scores;
     a.total_segs = segs;
     IQM_CHECK_CUDA(cudaMemsetAsync(a.counters, 0, sizeof(unsigned) * n, ctx->stream));
+    iqm::timing_mark(ctx, nullptr);
     const int R = std::max(T.rf, T.rc);
     const size_t smem = sizeof(float) * NPLANE * (VT_ROWS + 2 * R) * VT_COLS;
-    auto run = [&](auto hk, auto vk) {
-        hk<<<unsigned(segs), HT, 0, ctx->stream>>>(a, T);
+    if (fixed == 1) {  // default monitor, 52.1 ppd
+        flip_hpass_kernel<7, 8><<<unsigned(segs), HT, 0, ctx->stream>>>(a, T);
+        iqm::check_launch(ctx, "flip_hpass_kernel");
+        flip_vcols_kernel<7, 8><<<tiles, CW_T, 0, ctx->stream>>>(a, T);
+        iqm::check_launch(ctx, "flip_vcols_kernel");
+    } else if (fixed == 2) {  // 67 ppd
+        flip_hpass_kernel<9, 10><<<unsigned(segs), HT, 0, ctx->stream>>>(a, T);
+        iqm::check_launch(ctx, "flip_hpass_kernel");
+        flip_vcols_kernel<9, 10><<<tiles, CW_T, 0, ctx->stream>>>(a, T);
+        iqm::check_launch(ctx, "flip_vcols_kernel");
+    } else {
+        flip_hpass_kernel<0, 0><<<unsigned(segs), HT, 0, ctx->stream>>>(a, T);
         iqm::check_launch(ctx, "flip_hpass_kernel");
         if (smem > 48 * 1024)
-            IQM_CHECK_CUDA(cudaFuncSetAttribute((const void *)vk, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        vk<<<tiles, VT, smem, ctx->stream>>>(a, T);
-    };
-    // the two viewing set-ups in common use get kernels with their radii built in
-    if (T.rf == 7 && T.rc == 8) {
-        run(flip_hpass_kernel<7, 8>, flip_vpass_kernel<7, 8>);        // default monitor, 52.1 ppd
-    } else if (T.rf == 9 && T.rc == 10) {
-        run(flip_hpass_kernel<9, 10>, flip_vpass_kernel<9, 10>);      // 67 ppd
-    } else {
-        run(flip_hpass_kernel<0, 0>, flip_vpass_kernel<0, 0>);
+            IQM_CHECK_CUDA(cudaFuncSetAttribute((const void *)flip_vpass_kernel<0, 0>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        flip_vpass_kernel<0, 0><<<tiles, VT, smem, ctx->stream>>>(a, T);
+        iqm::check_launch(ctx, "flip_vpass_kernel");
     }
-    iqm::check_launch(ctx, "flip_vpass_kernel");
 }
 
 }  // namespace

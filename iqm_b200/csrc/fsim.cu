@@ -923,6 +923,7 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
         const int w2 = kv.first.first, h2 = kv.first.second;
         const int G = int(kv.second.size());
         iqm::FsimPlan *P = get_plan(ctx, w2, h2);
+        iqm::timing_mark(ctx, nullptr);
         const Shapes s = shapes_for(*P);
         configure_kernels(s);
         const int n = P->n;
@@ -955,6 +956,7 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
         for (int i : kv.second)
             if (hd[i].F != F_uniform) F_uniform = 0;
         IQM_CHECK_CUDA(cudaMemsetAsync(g.counters, 0, sizeof(unsigned) * G, st));
+        iqm::timing_mark(ctx, nullptr);
         launch_ingest(g, F_uniform, tiles, st);
         iqm::check_launch(ctx, "fsim_ingest_kernel");
         with_engine(s.row_eng, [&](auto e) {

@@ -131,9 +131,20 @@ struct iqm_ctx {
 
     std::map<std::pair<int, int>, iqm::FsimPlan *> fsim_plans;  // owned; freed by iqm_release_fsim_plans
     std::map<int, iqm::FftPlan *> fft_plans;  // owned; freed by iqm_release_fft_plans
+
+    // Per-kernel device timing (iqm_set_kernel_timing): an event after every launch and after every
+    // copy or memset the context enqueues; a kernel is charged the interval since the event before it.
+    bool timing = false;
+    std::vector<std::pair<const char *, cudaEvent_t>> marks;  // nullptr name: not a kernel
+    std::vector<cudaEvent_t> event_pool;
+    std::map<std::string, std::pair<long, double>> kernel_ms;  // name -> (launches, total ms)
 };
 
 namespace iqm {
+
+// Records a timing event on the context stream when per-kernel timing is on (ctx.cu); `kernel` is
+// the kernel launched just before, or nullptr after a copy, memset or call start.
+void timing_mark(iqm_ctx *ctx, const char *kernel);
 
 // Run `fn` and convert any failure into a status code recorded on the context.
 template <class F>
@@ -142,6 +153,7 @@ int guarded(iqm_ctx *ctx, F &&fn) {
     try {
         ctx->launches = 0;
         IQM_CHECK_CUDA(cudaSetDevice(ctx->device));
+        timing_mark(ctx, nullptr);
         fn();
         ctx->last_error.clear();
         return IQM_OK;
@@ -161,6 +173,7 @@ inline void check_launch(iqm_ctx *ctx, const char *what) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) throw Error{IQM_ECUDA, std::string(what) + ": " + cudaGetErrorString(e)};
     ctx->launches++;
+    timing_mark(ctx, what);
 }
 
 // Validate a batch of pair descriptors.

@@ -8,7 +8,8 @@ from iqm_b200 import synth
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-5
-ARGS_67 = iqm_b200.FLIPArguments(3840.0, 0.7, 0.7)  # 67.02 pixels per degree
+ARGS_67 = iqm_b200.FLIPArguments(3840.0, 0.7, 0.7)  # 67.02 pixels per degree, radii 9/10
+ARGS_37 = iqm_b200.FLIPArguments(2560.0, 0.5, 0.6)  # 37.2 pixels per degree, radii 5/6 (generic kernel)
 
 
 def test_ppd_matches_reference_formula(rt, o64):
@@ -18,7 +19,7 @@ def test_ppd_matches_reference_formula(rt, o64):
 
 
 @pytest.mark.parametrize("h,w", [(64, 96), (41, 59), (300, 517), (1080, 1920), (5, 7)])
-@pytest.mark.parametrize("args", [ARGS_67, iqm_b200.FLIPArguments()])
+@pytest.mark.parametrize("args", [ARGS_67, iqm_b200.FLIPArguments(), ARGS_37])
 def test_flip_matches_oracle(rt, o64, o32, h, w, args):
     a, b = synth.rgb_blockquant_pair(h, w, config=2, pair=w % 5)
     f = iqm_b200.FLIP(rt)
@@ -30,9 +31,12 @@ def test_flip_matches_oracle(rt, o64, o32, h, w, args):
     assert np.abs(r.image_data - m64).max() <= 1e-4
 
 
-def test_flip_identical_is_zero(rt):
-    a, b = synth.rgb_blockquant_pair(64, 64, config=2, pair=1)
-    assert iqm_b200.FLIP(rt).compute_metric(b, b).mean_flip == 0.0
+@pytest.mark.parametrize("args", [ARGS_67, iqm_b200.FLIPArguments(), ARGS_37])
+def test_flip_identical_is_zero(rt, args):
+    a, b = synth.rgb_blockquant_pair(300, 200, config=2, pair=1)
+    r = iqm_b200.FLIP(rt).compute_metric(b, b, args, want_map=True)
+    assert r.mean_flip == 0.0
+    assert not r.image_data.any()
 
 
 def test_flip_batch_uneven(rt, o64):
