@@ -107,6 +107,21 @@ def load_library(path=LIB_PATH):
     return L
 
 
+def fsim_downscale_factor(w, h):
+    """F = max(1, round(min(w, h) / 256)) (src/gpu/fsim/fsim.cpp:165-168), as the library computes it."""
+    x = min(w, h) / 256.0
+    return max(1, int(np.floor(x + 0.5)))
+
+
+def fsim_plane_size(w, h):
+    """(W', H') of the FSIM working planes: roundf(W / F), roundf(H / F) in float
+    (src/gpu/fsim/fsim.cpp:91-92)."""
+    F = fsim_downscale_factor(w, h)
+    fw = float(np.float32(w) / np.float32(F))
+    fh = float(np.float32(h) / np.float32(F))
+    return int(np.floor(fw + 0.5)), int(np.floor(fh + 0.5))
+
+
 def _img(a):
     """RGBA8 host image (h, w, 4) -> contiguous uint8 array."""
     a = np.ascontiguousarray(a, dtype=np.uint8)
