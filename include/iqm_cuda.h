@@ -169,6 +169,36 @@ int iqm_set_kernel_timing(iqm_ctx *ctx, int enable);
  * into buf (NUL-terminated); IQM_EINVAL if cap is too small. */
 int iqm_kernel_times(iqm_ctx *ctx, char *buf, size_t cap);
 
+/* ---- batches over several metrics ------------------------------------------------------------
+ * The reference evaluates one pair with one metric per invocation (src/main.cpp:271-286, the method
+ * chosen by IQM::Method, src/methods.h:13-19); these run many pairs through several metrics at once.
+ * Scores are laid out metric by metric, in the order below, for the metrics in the mask:
+ * SSIM n doubles, FSIM 2n (FSIM, FSIMc per pair), FLIP n, M-SVD n. */
+#define IQM_METRIC_SSIM 1
+#define IQM_METRIC_FSIM 2
+#define IQM_METRIC_FLIP 4
+#define IQM_METRIC_MSVD 8
+
+/* Host pairs (sizes may differ): upload, evaluate every metric of the mask, copy the scores to the
+ * host and return.  ssim/flip may be NULL for the defaults. */
+int iqm_batch(iqm_ctx *ctx, int metric_mask, const iqm_pair *pairs, int n, const iqm_ssim_params *ssim,
+              const iqm_flip_params *flip, iqm_precision precision, int energy_mode, double *scores);
+
+/* A reusable plan for one fixed batch of device-resident pairs: creation validates the arguments,
+ * runs the batch once (building per-size tables and sizing the plan's own device buffers), with
+ * autotune != 0 times FSIM's launch-shape candidates and keeps the fastest, and captures the whole
+ * launch sequence of every metric into a CUDA graph.  iqm_batch_plan_run replays it on the context
+ * stream (asynchronous; scores land in d_scores).  The pairs' device memory, d_scores and the context
+ * must outlive the plan; a plan's runs must not overlap one another on the GPU. */
+typedef struct iqm_batch_plan iqm_batch_plan;
+int iqm_batch_plan_create(iqm_ctx *ctx, int metric_mask, const iqm_pair *dev_pairs, int n,
+                          const iqm_ssim_params *ssim, const iqm_flip_params *flip, iqm_precision precision,
+                          int energy_mode, int autotune, double *d_scores, iqm_batch_plan **out);
+int iqm_batch_plan_run(iqm_batch_plan *plan);
+/* Text describing the chosen launch shapes, and the kernel launches one run replays. */
+int iqm_batch_plan_info(const iqm_batch_plan *plan, char *buf, size_t cap, int *launches);
+int iqm_batch_plan_destroy(iqm_batch_plan *plan);
+
 #ifdef __cplusplus
 }
 #endif

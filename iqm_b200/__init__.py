@@ -34,8 +34,12 @@ EXPORTS = (
     "iqm_flip_ppd", "iqm_flip", "iqm_fsim", "iqm_ssim_dev", "iqm_msvd_dev", "iqm_flip_dev",
     "iqm_fsim_dev", "iqm_ssim_batch", "iqm_msvd_batch", "iqm_flip_batch", "iqm_fsim_batch",
     "iqm_last_launch_count", "iqm_fsim_plan_constants", "iqm_ssim_noalloc", "iqm_set_kernel_timing",
-    "iqm_kernel_times",
+    "iqm_kernel_times", "iqm_batch", "iqm_batch_plan_create", "iqm_batch_plan_run", "iqm_batch_plan_info",
+    "iqm_batch_plan_destroy",
 )
+
+METRIC_SSIM, METRIC_FSIM, METRIC_FLIP, METRIC_MSVD = 1, 2, 4, 8
+_SCORES = ((METRIC_SSIM, 1), (METRIC_FSIM, 2), (METRIC_FLIP, 1), (METRIC_MSVD, 1))
 
 
 class IQMError(RuntimeError):
@@ -103,6 +107,12 @@ def load_library(path=LIB_PATH):
     L.iqm_ssim_noalloc.argtypes = [vp, vp, ip, ip, ctypes.c_size_t, ctypes.POINTER(SSIMParams), vp, vp, vp]
     L.iqm_set_kernel_timing.argtypes = [vp, ip]
     L.iqm_kernel_times.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+    L.iqm_batch.argtypes = [vp, ip, PP, ip, ctypes.POINTER(SSIMParams), ctypes.POINTER(FLIPParams), ip, ip, dp]
+    L.iqm_batch_plan_create.argtypes = [vp, ip, PP, ip, ctypes.POINTER(SSIMParams), ctypes.POINTER(FLIPParams),
+                                        ip, ip, ip, vp, ctypes.POINTER(vp)]
+    L.iqm_batch_plan_run.argtypes = [vp]
+    L.iqm_batch_plan_info.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ip)]
+    L.iqm_batch_plan_destroy.argtypes = [vp]
     _lib = L
     return L
 
@@ -392,3 +402,79 @@ class FSIM:
         arr = _pairs(dev_pairs)
         self.rt.check(self.rt.L.iqm_fsim_dev(self.rt.h, arr, len(dev_pairs), self.precision, self.energy_mode,
                                              ctypes.c_void_p(d_scores)))
+
+
+# ---------------------------------------------------------------- batches over several metrics
+def _split_scores(mask, n, flat):
+    """Flat metric-by-metric score layout -> {"ssim": (n,), "fsim": (n, 2), "flip": (n,), "msvd": (n,)}."""
+    out, off = {}, 0
+    names = {METRIC_SSIM: "ssim", METRIC_FSIM: "fsim", METRIC_FLIP: "flip", METRIC_MSVD: "msvd"}
+    for flag, k in _SCORES:
+        if mask & flag:
+            v = np.asarray(flat[off:off + k * n])
+            out[names[flag]] = v.reshape(n, 2) if k == 2 else v
+            off += k * n
+    return out
+
+
+def scores_per_pair(mask):
+    return sum(k for flag, k in _SCORES if mask & flag)
+
+
+def _ssim_params(rt, ssim):
+    return ssim if isinstance(ssim, SSIMParams) else (ssim or SSIM(rt)).params()
+
+
+def batch(rt, mask, pairs, ssim=None, flip=None, precision=IQM_FP32, energy_mode=0):
+    """Evaluates host pairs [(image, ref), ...] (RGBA8 arrays, sizes may differ) with every metric in
+    `mask` in one call; returns the per-metric score arrays."""
+    imgs = [(_img(a), _img(b)) for a, b in pairs]
+    for a, b in imgs:
+        _check_same(a, b)
+    items = [(a.ctypes.data, b.ctypes.data, a.shape[1], a.shape[0], a.shape[1] * 4) for a, b in imgs]
+    arr = _pairs(items)
+    n = len(items)
+    out = np.empty(scores_per_pair(mask) * n, np.float64)
+    sp = _ssim_params(rt, ssim)
+    fp = (flip or FLIPArguments()).c()
+    rt.check(rt.L.iqm_batch(rt.h, mask, arr, n, ctypes.byref(sp), ctypes.byref(fp), precision, energy_mode,
+                            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    return _split_scores(mask, n, out)
+
+
+class BatchPlan:
+    """A fixed batch of device-resident pairs evaluated with several metrics by one CUDA-graph
+    replay (iqm_batch_plan_*); FSIM launch shapes autotuned at creation."""
+
+    def __init__(self, rt, mask, dev_pairs, d_scores, ssim=None, flip=None, precision=IQM_FP32, energy_mode=0,
+                 autotune=True):
+        self.rt, self.mask, self.n = rt, mask, len(dev_pairs)
+        arr = _pairs(dev_pairs)
+        sp = _ssim_params(rt, ssim)
+        fp = (flip or FLIPArguments()).c()
+        h = ctypes.c_void_p()
+        rt.check(rt.L.iqm_batch_plan_create(rt.h, mask, arr, self.n, ctypes.byref(sp), ctypes.byref(fp), precision,
+                                            energy_mode, 1 if autotune else 0, ctypes.c_void_p(d_scores),
+                                            ctypes.byref(h)))
+        self.h = h
+
+    def run(self):
+        self.rt.check(self.rt.L.iqm_batch_plan_run(self.h))
+
+    def info(self):
+        buf = ctypes.create_string_buffer(1024)
+        launches = ctypes.c_int()
+        self.rt.L.iqm_batch_plan_info(self.h, buf, len(buf), ctypes.byref(launches))
+        return buf.value.decode(), launches.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.rt.L.iqm_batch_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

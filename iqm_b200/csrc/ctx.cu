@@ -66,6 +66,9 @@ extern "C" __attribute__((visibility("default"))) int iqm_destroy(iqm_ctx *ctx) 
     ctx->pinned.release();
     ctx->ring.release();
     iqm::timing_release(ctx);
+    for (auto st : ctx->side_streams) cudaStreamDestroy(st);
+    for (auto ev : ctx->side_events) cudaEventDestroy(ev);
+    if (ctx->fork_event) cudaEventDestroy(ctx->fork_event);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return IQM_OK;
@@ -102,6 +105,14 @@ extern "C" __attribute__((visibility("default"))) int iqm_last_launch_count(cons
 namespace iqm {
 
 void *upload_bytes(iqm_ctx *ctx, DevBuf &dst, const void *src, size_t bytes) {
+    if (ctx->capturing) {
+        // A batch plan captures a second, identical enqueue: the bytes are already on the device
+        // (uploaded by the uncaptured pass into the plan's own buffer) and a copy node would read a
+        // staging slot that later calls reuse.
+        (void)src;
+        IQM_REQUIRE(dst.ptr && bytes <= dst.cap, "batch plan capture: descriptor buffer not prepared");
+        return dst.ptr;
+    }
     UploadRing &r = ctx->ring;
     const int slot = r.next;
     r.next = (r.next + 1) % UploadRing::SLOTS;
@@ -127,6 +138,21 @@ void *upload_bytes(iqm_ctx *ctx, DevBuf &dst, const void *src, size_t bytes) {
     IQM_CHECK_CUDA(cudaEventRecord(r.ev[slot], ctx->stream));
     timing_mark(ctx, nullptr);
     return d;
+}
+
+void side_streams(iqm_ctx *ctx, int n) {
+    if (!ctx->fork_event) IQM_CHECK_CUDA(cudaEventCreateWithFlags(&ctx->fork_event, cudaEventDisableTiming));
+    while (int(ctx->side_streams.size()) < n) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t ev = nullptr;
+        IQM_CHECK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            cudaStreamDestroy(st);
+            throw Error{IQM_ECUDA, "cudaEventCreate failed"};
+        }
+        ctx->side_streams.push_back(st);
+        ctx->side_events.push_back(ev);
+    }
 }
 
 std::vector<iqm_pair> upload_pairs(iqm_ctx *ctx, const iqm_pair *pairs, int n) {
@@ -187,7 +213,7 @@ static void timing_release(iqm_ctx *ctx) {
 }
 
 void timing_mark(iqm_ctx *ctx, const char *kernel) {
-    if (!ctx->timing) return;
+    if (!ctx->timing || ctx->capturing) return;
     // A stream switch or a long run: settle what is recorded so far (the settled mark stays the
     // start of the next interval).
     if (ctx->marks.size() >= 16384) timing_collect(ctx);

@@ -682,15 +682,18 @@ IQM_API void iqm_flip_default_params(iqm_flip_params *p) {
 
 IQM_API double iqm_flip_ppd(const iqm_flip_params *p) { return ppd_of(resolve(p)); }
 
+void iqm::enqueue_flip_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_flip_params *params,
+                           double *d_scores) {
+    const iqm_flip_params p = resolve(params);
+    check_params(p);
+    iqm::check_pairs(pairs, n, 1, 1);
+    IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
+    flip_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), p, {}, d_scores);
+}
+
 IQM_API int iqm_flip_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_flip_params *params,
                          double *d_scores) {
-    return iqm::guarded(ctx, [&] {
-        const iqm_flip_params p = resolve(params);
-        check_params(p);
-        iqm::check_pairs(pairs, n, 1, 1);
-        IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
-        flip_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), p, {}, d_scores);
-    });
+    return iqm::guarded(ctx, [&] { iqm::enqueue_flip_dev(ctx, pairs, n, params, d_scores); });
 }
 
 IQM_API int iqm_flip_batch(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_flip_params *params,

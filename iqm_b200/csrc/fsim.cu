@@ -28,6 +28,7 @@
 #include <cmath>
 #include <initializer_list>
 #include <map>
+#include <mutex>
 
 #include "fft.cuh"
 #include "fft_plan.cuh"
@@ -673,10 +674,19 @@ void plane_size(int w, int h, int F, int &w2, int &h2) {  // src/gpu/fsim/fsim.c
 }
 
 constexpr size_t SMEM_CAP = 200 * 1024;
+constexpr int kFsimStreams = 8;  // plane-size groups in flight at once
 
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` (never lowers it: launches
+// already enqueued or captured for other plane sizes keep their sizes valid).
 void set_smem(const void *fn, size_t bytes) {
-    if (bytes > 48 * 1024)
-        IQM_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    static std::mutex mu;
+    static std::map<const void *, size_t> current;
+    if (bytes <= 48 * 1024) return;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t &cur = current[fn];
+    if (bytes <= cur) return;
+    IQM_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    cur = bytes;
 }
 
 // Launch shapes of the transform kernels for one plane size.
@@ -720,7 +730,7 @@ int lw_fit(size_t fixed, size_t per_warp) {
     return lw;
 }
 
-Shapes shapes_for(const iqm::FsimPlan &P) {
+Shapes shapes_for(const iqm::FsimPlan &P, const iqm::FsimTune &tune = iqm::FsimTune{}) {
     Shapes s{};
     const size_t f2 = sizeof(float2);
     s.wl_row = iqm::fft_work_len(P.row);
@@ -735,6 +745,7 @@ Shapes shapes_for(const iqm::FsimPlan &P) {
     s.lw_fcols = lw_fit(twc, warp_col);
     s.sm_fcols = twc + (size_t(1) << s.lw_fcols) * warp_col;
     s.lw_icols = lw_fit(twc, warp_col + NB * size_t(P.h2) * f2);
+    if (tune.icols_lw >= 0) s.lw_icols = std::min(s.lw_icols, tune.icols_lw);
     s.sm_icols = twc + (size_t(1) << s.lw_icols) * (warp_col + NB * size_t(P.h2) * f2);
     const size_t per_row = (4 / NB) * warp_row;  // 4/NB warps per row (four scales)
     if (twr + 2 * per_row <= 120 * 1024) {
@@ -744,6 +755,7 @@ Shapes shapes_for(const iqm::FsimPlan &P) {
     } else {
         s.rr = 0;
     }
+    if (s.rr && tune.rows_per_cta >= 1 && tune.rows_per_cta < s.rr) s.rr = tune.rows_per_cta;
     s.sm_irows = s.rr ? twr + s.rr * per_row : (4 * size_t(P.w2) + 2 * s.wl_row) * f2;
     IQM_REQUIRE(s.sm_rows <= SMEM_CAP && s.sm_fcols <= SMEM_CAP && s.sm_icols <= SMEM_CAP && s.sm_irows <= SMEM_CAP,
                 "FSIM plane too large for the shared-memory FFT");
@@ -876,6 +888,13 @@ Layout layout_for(int G, int chunk, int n, int tiles) {
     return L;
 }
 
+// Inverse-pass chunk: the 32 intermediate planes of `chunk` pairs stay within an L2 budget
+// (80 MB unless tuned).
+int chunk_pairs(const iqm::FsimTune &t, int G, int n) {
+    const size_t budget = size_t(t.chunk_mb > 0 ? t.chunk_mb : 80) << 20;
+    return std::max(1, std::min(G, int(budget / (sizeof(float2) * 32 * size_t(n)))));
+}
+
 void launch_ingest(const FsimGroup &g, int F_uniform, int tiles, cudaStream_t st) {
     const dim3 grid(tiles, g.G);
     switch (F_uniform) {
@@ -908,31 +927,81 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
         for (int i : kv.second) ordered.push_back(hd[i]);
     auto *d_desc = static_cast<FsimPairDev *>(
         iqm::upload_bytes(ctx, ctx->desc, ordered.data(), sizeof(FsimPairDev) * n_pairs));
-    // scratch for the largest group layout
-    size_t need = 0;
-    for (auto &kv : groups) {
-        const int n = kv.first.first * kv.first.second;
-        const int G = int(kv.second.size());
-        const int chunk = std::max(1, std::min(G, int((80ull << 20) / (sizeof(float2) * 32 * size_t(n)))));
-        need = std::max(need, layout_for(G, chunk, n, int(iqm::ceil_div(n, FT))).total);
+    // per-size tables first (building one waits for the context stream)
+    struct GroupRun {
+        int w2, h2, G, first, slot, F_uniform, chunk;
+        iqm::FsimPlan *P;
+        Shapes s;
+        Layout L;
+        double cost;
+    };
+    std::vector<GroupRun> runs;
+    {
+        int first = 0;
+        for (auto &kv : groups) {
+            GroupRun r{};
+            r.w2 = kv.first.first;
+            r.h2 = kv.first.second;
+            r.G = int(kv.second.size());
+            r.first = first;
+            r.P = get_plan(ctx, r.w2, r.h2);
+            r.s = shapes_for(*r.P, ctx->fsim_tune);
+            const int n = r.P->n;
+            r.chunk = chunk_pairs(ctx->fsim_tune, r.G, n);
+            r.L = layout_for(r.G, r.chunk, n, int(iqm::ceil_div(n, FT)));
+            r.F_uniform = hd[kv.second[0]].F;
+            for (int i : kv.second)
+                if (hd[i].F != r.F_uniform) r.F_uniform = 0;
+            r.cost = double(r.G) * n * std::log2(double(n) + 2.0);
+            first += r.G;
+            runs.push_back(r);
+        }
     }
-    auto *base = static_cast<uint8_t *>(ctx->scratch.get(need, ctx->stream));
-    cudaStream_t st = ctx->stream;
-    size_t first = 0;
-    for (auto &kv : groups) {
-        const int w2 = kv.first.first, h2 = kv.first.second;
-        const int G = int(kv.second.size());
-        iqm::FsimPlan *P = get_plan(ctx, w2, h2);
-        iqm::timing_mark(ctx, nullptr);
-        const Shapes s = shapes_for(*P);
+    iqm::timing_mark(ctx, nullptr);
+    // Groups are independent: up to kFsimStreams of them run at once on side streams forked from the
+    // context stream and joined back (kept on one stream while per-kernel timing is on).  Each
+    // stream reuses one scratch slot for its groups, which it runs in order.
+    const int S = (runs.size() > 1 && !ctx->timing) ? std::min<int>(int(runs.size()), kFsimStreams) : 1;
+    {
+        std::vector<int> order(runs.size());
+        for (size_t i = 0; i < order.size(); i++) order[i] = int(i);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return runs[a].cost > runs[b].cost; });
+        std::vector<double> load(S, 0.0);
+        for (int i : order) {
+            const int sl = int(std::min_element(load.begin(), load.end()) - load.begin());
+            runs[i].slot = sl;
+            load[sl] += runs[i].cost;
+        }
+    }
+    std::vector<size_t> slot_off(S + 1, 0);
+    {
+        std::vector<size_t> need(S, 0);
+        for (const auto &r : runs) need[r.slot] = std::max(need[r.slot], r.L.total);
+        for (int sl = 0; sl < S; sl++) slot_off[sl + 1] = slot_off[sl] + ((need[sl] + 255) & ~size_t(255));
+    }
+    auto *base0 = static_cast<uint8_t *>(ctx->scratch.get(slot_off[S], ctx->stream));
+    std::vector<cudaStream_t> streams(S, ctx->stream);
+    if (S > 1) {
+        iqm::side_streams(ctx, S);
+        IQM_CHECK_CUDA(cudaEventRecord(ctx->fork_event, ctx->stream));
+        for (int sl = 0; sl < S; sl++) {
+            streams[sl] = ctx->side_streams[sl];
+            IQM_CHECK_CUDA(cudaStreamWaitEvent(streams[sl], ctx->fork_event, 0));
+        }
+    }
+    for (const GroupRun &r : runs) {
+        const int w2 = r.w2, h2 = r.h2, G = r.G;
+        iqm::FsimPlan *P = r.P;
+        const Shapes &s = r.s;
+        cudaStream_t st = streams[r.slot];
+        uint8_t *base = base0 + slot_off[r.slot];
         configure_kernels(s);
         const int n = P->n;
         const int tiles = int(iqm::ceil_div(n, FT));
-        // inverse-pass chunk: the 32 intermediate planes of `chunk` pairs stay within ~80 MB of L2
-        const int chunk = std::max(1, std::min(G, int((80ull << 20) / (sizeof(float2) * 32 * size_t(n)))));
-        const Layout Lc = layout_for(G, chunk, n, tiles);
+        const int chunk = r.chunk;
+        const Layout &Lc = r.L;
         FsimGroup g{};
-        g.pairs = d_desc + first;
+        g.pairs = d_desc + r.first;
         g.G = G;
         g.pair0 = 0;
         g.w2 = w2;
@@ -952,12 +1021,9 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
         g.filters = P->filters;
         g.consts = P->consts;
         g.energy_mode = energy_mode;
-        int F_uniform = hd[kv.second[0]].F;
-        for (int i : kv.second)
-            if (hd[i].F != F_uniform) F_uniform = 0;
         IQM_CHECK_CUDA(cudaMemsetAsync(g.counters, 0, sizeof(unsigned) * G, st));
         iqm::timing_mark(ctx, nullptr);
-        launch_ingest(g, F_uniform, tiles, st);
+        launch_ingest(g, r.F_uniform, tiles, st);
         iqm::check_launch(ctx, "fsim_ingest_kernel");
         with_engine(s.row_eng, [&](auto e) {
             fsim_fwd_rows_kernel<decltype(e)>
@@ -984,7 +1050,12 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
         iqm::check_launch(ctx, "fsim_noise_kernel");
         fsim_final_kernel<<<dim3(tiles, G), FT, 0, st>>>(g);
         iqm::check_launch(ctx, "fsim_final_kernel");
-        first += G;
+    }
+    if (S > 1) {
+        for (int sl = 0; sl < S; sl++) {
+            IQM_CHECK_CUDA(cudaEventRecord(ctx->side_events[sl], streams[sl]));
+            IQM_CHECK_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->side_events[sl], 0));
+        }
     }
 }
 
@@ -1010,13 +1081,16 @@ void iqm_release_fsim_plans(iqm_ctx *ctx) {
 
 #define IQM_API extern "C" __attribute__((visibility("default")))
 
+void iqm::enqueue_fsim_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, iqm_precision precision, int energy_mode,
+                           double *d_scores) {
+    check_fsim_args(pairs, n, precision, energy_mode);
+    IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
+    fsim_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), energy_mode, d_scores);
+}
+
 IQM_API int iqm_fsim_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, iqm_precision precision, int energy_mode,
                          double *d_scores) {
-    return iqm::guarded(ctx, [&] {
-        check_fsim_args(pairs, n, precision, energy_mode);
-        IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
-        fsim_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), energy_mode, d_scores);
-    });
+    return iqm::guarded(ctx, [&] { iqm::enqueue_fsim_dev(ctx, pairs, n, precision, energy_mode, d_scores); });
 }
 
 IQM_API int iqm_fsim_batch(iqm_ctx *ctx, const iqm_pair *pairs, int n, iqm_precision precision, int energy_mode,

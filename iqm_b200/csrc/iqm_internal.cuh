@@ -108,6 +108,14 @@ struct UploadRing {
     }
 };
 
+// Launch-shape choices of the FSIM transform passes (0 / -1 = built-in heuristic).  They change
+// only how work is split over CTAs, never a result bit; batch plans autotune them (plan.cu).
+struct FsimTune {
+    int chunk_mb = 0;     // L2 budget for the inverse-pass intermediates of one chunk of pairs
+    int icols_lw = -1;    // log2 warps per CTA of the inverse column pass (clamped to what fits)
+    int rows_per_cta = 0; // rows per CTA of the inverse row pass (1 or 2, if it fits)
+};
+
 struct FsimPlan;  // per plane-size FSIM constants (fsim.cu)
 struct FftPlan;   // per-length FFT tables (fft.cu)
 
@@ -119,6 +127,12 @@ struct iqm_ctx {
     cudaStream_t stream = nullptr;
     std::string last_error;
     int launches = 0;  // kernel launches enqueued by the last entry point
+    bool capturing = false;  // a batch plan is capturing the stream into a CUDA graph (plan.cu)
+    iqm::FsimTune fsim_tune;
+    // streams that independent work forks onto from `stream` and joins back from (iqm::side_streams)
+    std::vector<cudaStream_t> side_streams;
+    std::vector<cudaEvent_t> side_events;
+    cudaEvent_t fork_event = nullptr;
 
     // named scratch areas (each grow-only)
     iqm::DevBuf desc;      // per-call pair descriptors
@@ -195,8 +209,19 @@ inline void check_pairs(const iqm_pair *pairs, int n, int min_w, int min_h) {
 // through the pinned ring; returns the device pointer.
 void *upload_bytes(iqm_ctx *ctx, DevBuf &dst, const void *src, size_t bytes);
 
+// Makes at least n side streams (with one join event each) and the fork event exist on the context.
+void side_streams(iqm_ctx *ctx, int n);
+
 // Copies host pairs to device memory (inside ctx->images) and rewrites the pointers.
 std::vector<iqm_pair> upload_pairs(iqm_ctx *ctx, const iqm_pair *pairs, int n);
+
+// Validate and enqueue one metric for device-resident pairs on the context stream (the bodies of
+// the iqm_*_dev entry points); batch plans call them directly.
+void enqueue_ssim_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_ssim_params *params, double *d_scores);
+void enqueue_fsim_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, iqm_precision precision, int energy_mode,
+                      double *d_scores);
+void enqueue_flip_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_flip_params *params, double *d_scores);
+void enqueue_msvd_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, double *d_scores);
 
 inline unsigned ceil_div(long a, long b) { return unsigned((a + b - 1) / b); }
 

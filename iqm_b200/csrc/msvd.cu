@@ -267,13 +267,15 @@ void msvd_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const std::v
 // The reference needs at least one 8x8 block slot: n = (W/8)*(H/8) > 0 (it divides by n).
 static void check_msvd_pairs(const iqm_pair *pairs, int n) { iqm::check_pairs(pairs, n, 8, 8); }
 
+void iqm::enqueue_msvd_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, double *d_scores) {
+    check_msvd_pairs(pairs, n);
+    IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
+    msvd_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), {}, d_scores);
+}
+
 extern "C" __attribute__((visibility("default"))) int iqm_msvd_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n,
                                                                   double *d_scores) {
-    return iqm::guarded(ctx, [&] {
-        check_msvd_pairs(pairs, n);
-        IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
-        msvd_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), {}, d_scores);
-    });
+    return iqm::guarded(ctx, [&] { iqm::enqueue_msvd_dev(ctx, pairs, n, d_scores); });
 }
 
 extern "C" __attribute__((visibility("default"))) int iqm_msvd_batch(iqm_ctx *ctx, const iqm_pair *pairs, int n,

@@ -417,16 +417,19 @@ extern "C" __attribute__((visibility("default"))) void iqm_ssim_default_params(i
     p->sigma = 1.5f;
 }
 
+void iqm::enqueue_ssim_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_ssim_params *params,
+                           double *d_scores) {
+    const iqm_ssim_params p = resolve(params);
+    check_params(p);
+    const int R = (p.kernel_size - 1) / 2;
+    iqm::check_pairs(pairs, n, R, R);
+    IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
+    ssim_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), p, {}, d_scores);
+}
+
 extern "C" __attribute__((visibility("default"))) int iqm_ssim_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_ssim_params *params,
                             double *d_scores) {
-    return iqm::guarded(ctx, [&] {
-        const iqm_ssim_params p = resolve(params);
-        check_params(p);
-        const int R = (p.kernel_size - 1) / 2;
-        iqm::check_pairs(pairs, n, R, R);
-        IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
-        ssim_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), p, {}, d_scores);
-    });
+    return iqm::guarded(ctx, [&] { iqm::enqueue_ssim_dev(ctx, pairs, n, params, d_scores); });
 }
 
 extern "C" __attribute__((visibility("default"))) int iqm_ssim_batch(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_ssim_params *params,

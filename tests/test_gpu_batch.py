@@ -1,0 +1,118 @@
+"""Batches over several metrics (iqm_batch) and CUDA-graph batch plans (iqm_batch_plan_*), against
+the per-metric entry points (bit-exact) and the FP64 oracle (|delta| <= 1e-5)."""
+import numpy as np
+import pytest
+
+import iqm_b200
+from iqm_b200 import synth
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+ALL = iqm_b200.METRIC_SSIM | iqm_b200.METRIC_FSIM | iqm_b200.METRIC_FLIP | iqm_b200.METRIC_MSVD
+
+
+def _pairs(sizes, seed_pair=0):
+    return [synth.rgb_blockquant_pair(h, w, config=2, pair=seed_pair + i) for i, (w, h) in enumerate(sizes)]
+
+
+def test_batch_all_metrics_equals_single_metric_calls(rt):
+    sizes = [(128, 96), (301, 170), (64, 64), (480, 270), (97, 211)]
+    pairs = _pairs(sizes)
+    got = iqm_b200.batch(rt, ALL, pairs)
+    assert np.array_equal(got["ssim"], iqm_b200.SSIM(rt).compute_batch(pairs))
+    assert np.array_equal(got["fsim"], np.asarray(iqm_b200.FSIM(rt).compute_batch(pairs)).reshape(-1, 2))
+    assert np.array_equal(got["flip"], iqm_b200.FLIP(rt).compute_batch(pairs))
+    assert np.array_equal(got["msvd"], iqm_b200.SVD(rt).compute_batch(pairs))
+
+
+def test_batch_rejects_bad_mask(rt):
+    a = np.zeros((32, 32, 4), np.uint8)
+    with pytest.raises(iqm_b200.IQMError):
+        iqm_b200.batch(rt, 0, [(a, a)])
+    with pytest.raises(iqm_b200.IQMError):
+        iqm_b200.batch(rt, 16, [(a, a)])
+
+
+def _to_device(pairs):
+    import torch
+    bufs, items = [], []
+    for a, b in pairs:
+        da = torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).cuda()
+        db = torch.from_numpy(np.ascontiguousarray(b).reshape(-1)).cuda()
+        bufs += [da, db]
+        items.append((da.data_ptr(), db.data_ptr(), a.shape[1], a.shape[0], a.shape[1] * 4))
+    return bufs, items
+
+
+def test_plan_replays_match_batch_and_follow_inputs(rt):
+    import torch
+    sizes = [(200, 150), (480, 270), (333, 121), (200, 150)]
+    pairs = _pairs(sizes, seed_pair=10)
+    bufs, items = _to_device(pairs)
+    k = iqm_b200.scores_per_pair(ALL)
+    d_scores = torch.zeros(k * len(pairs), dtype=torch.float64, device="cuda")
+    plan = iqm_b200.BatchPlan(rt, ALL, items, d_scores.data_ptr(), autotune=True)
+    try:
+        info, launches = plan.info()
+        assert "fsim:" in info and launches > 0
+        want = iqm_b200.batch(rt, ALL, pairs)
+        for _ in range(2):
+            d_scores.zero_()
+            torch.cuda.synchronize()
+            plan.run()
+            rt.synchronize()
+            got = iqm_b200._split_scores(ALL, len(pairs), d_scores.cpu().numpy())
+            for m in want:
+                assert np.array_equal(got[m], want[m]), m
+        # same buffers, new content: the replay reads the current pixels
+        new = _pairs(sizes, seed_pair=20)
+        for i, (a, b) in enumerate(new):
+            bufs[2 * i].copy_(torch.from_numpy(np.ascontiguousarray(a).reshape(-1)))
+            bufs[2 * i + 1].copy_(torch.from_numpy(np.ascontiguousarray(b).reshape(-1)))
+        torch.cuda.synchronize()
+        plan.run()
+        rt.synchronize()
+        got = iqm_b200._split_scores(ALL, len(pairs), d_scores.cpu().numpy())
+        want = iqm_b200.batch(rt, ALL, new)
+        for m in want:
+            assert np.array_equal(got[m], want[m]), m
+    finally:
+        plan.close()
+
+
+def test_plan_uneven_batch_matches_oracle(rt, o64):
+    """Uneven sizes drawn uniformly from [256, 2048] (seeded): SSIM on grey pairs, FSIM on RGB
+    pairs, each through its own plan."""
+    import torch
+    sizes = synth.uneven_sizes(6, seed=3000)
+    grey = [synth.grey_pair(h, w, config=3, pair=i) for i, (w, h) in enumerate(sizes)]
+    rgb = [synth.rgb_gain_pair(h, w, config=3, pair=i) for i, (w, h) in enumerate(sizes)]
+    for mask, pairs in ((iqm_b200.METRIC_SSIM, grey), (iqm_b200.METRIC_FSIM, rgb)):
+        bufs, items = _to_device(pairs)
+        k = iqm_b200.scores_per_pair(mask)
+        d_scores = torch.zeros(k * len(pairs), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        plan = iqm_b200.BatchPlan(rt, mask, items, d_scores.data_ptr(), autotune=False)
+        try:
+            plan.run()
+            rt.synchronize()
+            got = d_scores.cpu().numpy()
+        finally:
+            plan.close()
+        for i, (a, b) in enumerate(pairs):
+            if mask == iqm_b200.METRIC_SSIM:
+                assert abs(got[i] - o64.ssim(a, b)) <= TOL
+            else:
+                f, fc = o64.fsim(a, b)
+                assert abs(got[2 * i] - f) <= TOL and abs(got[2 * i + 1] - fc) <= TOL
+
+
+def test_plan_error_leaves_context_usable(rt):
+    import torch
+    tiny = np.zeros((1, 1, 4), np.uint8)
+    bufs, items = _to_device([(tiny, tiny)])
+    d_scores = torch.zeros(2, dtype=torch.float64, device="cuda")
+    with pytest.raises(iqm_b200.IQMError):
+        iqm_b200.BatchPlan(rt, iqm_b200.METRIC_FSIM, items, d_scores.data_ptr())
+    a, b = synth.grey_pair(64, 64, config=0, pair=1)
+    assert 0.0 < iqm_b200.SSIM(rt).compute_metric(a, b).mssim <= 1.0
