@@ -417,27 +417,20 @@ constexpr int CW_BLOCKS = 10;        // K-row blocks per CTA
 
 __host__ __device__ constexpr int cw_rows(int rf, int rc) { return CW_BLOCKS * (2 * (rf > rc ? rf : rc) + 1); }
 
-template <int TS>
-__device__ __forceinline__ float cw_tap(const FlipTaps &T, int i) {
-    return TS < 3 ? T.feat[TS][i] : T.csf[TS - 3][i];
-}
-
-// One block of K output rows of one role: window slot (j + u) % K holds image row y - R + u of
-// output row y = ybase + R + j; image row y - k is weighted by tap k + RAD (|k| <= RAD).
-template <int RAD, int TS, int K>
-__device__ __forceinline__ void cw_block(const FlipTaps &T, float (&win)[K], const float *col, int w, int h,
+// One block of K output rows: window slot (j + u) % K holds image row y - R + u of output row
+// y = ybase + R + j, weighted by taps[u].  Every role runs this one body (one copy of the unrolled
+// code for all warps); a role whose filter is shorter than K has zero taps at the ends, which leave
+// its sums unchanged bit for bit.
+template <int K>
+__device__ __forceinline__ void cw_block(float (&win)[K], const float (&taps)[K], const float *col, int w, int h,
                                          int ybase, float *out) {
-    constexpr int R = K / 2;
 #pragma unroll
     for (int j = 0; j < K; j++) {
         const int y = min(max(ybase + j + K - 1, 0), h - 1);
         win[(j + K - 1) % K] = __ldg(col + size_t(y) * size_t(w));
         float acc = 0.f;
 #pragma unroll
-        for (int u = 0; u < K; u++) {
-            const int k = R - u;
-            if (k >= -RAD && k <= RAD) acc = fmaf(win[(j + u) % K], cw_tap<TS>(T, k + RAD), acc);
-        }
+        for (int u = 0; u < K; u++) acc = fmaf(win[(j + u) % K], taps[u], acc);
         out[j * CW_ROLES * 32] = acc;
     }
 }
@@ -461,6 +454,9 @@ __global__ void __launch_bounds__(CW_T, 2) flip_vcols_kernel(FlipArgs args, cons
     const int pl = m * 6 + (f == 0 ? 0 : f == 1 ? 2 : f == 2 ? 1 : f == 3 ? 2 : f - 1);
     const size_t n = size_t(P.w) * size_t(P.h);
     const float *col = args.planes + P.plane_off + size_t(pl) * n + min(x0 + lane, P.w - 1);
+    // this role's taps: image row y - k weighs tap k + radius; feature roles use g, edge, g, point
+    const float *tap_src = f < 4 ? T.feat[f == 1 ? 1 : f == 3 ? 2 : 0] : T.csf[f - 4];
+    const int rad = f < 4 ? RF : RC;
     float win[K];
 #pragma unroll
     for (int t = 0; t < K - 1; t++) win[t] = __ldg(col + size_t(min(max(y0 - R + t, 0), P.h - 1)) * size_t(P.w));
@@ -469,16 +465,13 @@ __global__ void __launch_bounds__(CW_T, 2) flip_vcols_kernel(FlipArgs args, cons
     for (int b = 0; b < CW_BLOCKS; b++) {
         const int yb = y0 + b * K;
         if (yb >= P.h) break;  // uniform over the CTA
-        const int ybase = yb - R;
-        switch (f) {
-            case 0: cw_block<RF, 0, K>(T, win, col, P.w, P.h, ybase, out); break;
-            case 1: cw_block<RF, 1, K>(T, win, col, P.w, P.h, ybase, out); break;
-            case 2: cw_block<RF, 0, K>(T, win, col, P.w, P.h, ybase, out); break;
-            case 3: cw_block<RF, 2, K>(T, win, col, P.w, P.h, ybase, out); break;
-            case 4: cw_block<RC, 3, K>(T, win, col, P.w, P.h, ybase, out); break;
-            case 5: cw_block<RC, 4, K>(T, win, col, P.w, P.h, ybase, out); break;
-            default: cw_block<RC, 5, K>(T, win, col, P.w, P.h, ybase, out); break;
+        float taps[K];  // reloaded per block so they are not live across the pixel phase
+#pragma unroll
+        for (int u = 0; u < K; u++) {
+            const int k = R - u;
+            taps[u] = (k >= -rad && k <= rad) ? tap_src[k + rad] : 0.f;
         }
+        cw_block<K>(win, taps, col, P.w, P.h, yb - R, out);
         __syncthreads();
         for (int p = threadIdx.x; p < K * 32; p += CW_T) {
             const int j = p >> 5, c = p & 31;

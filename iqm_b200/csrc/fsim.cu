@@ -197,6 +197,7 @@ __global__ void __launch_bounds__(FT) fsim_ingest_kernel(FsimGroup g) {
 // length (FftLen::stw), followed by per-warp work buffers: a warp transforms NB sequences at once
 // (buffer a: NB x wl, buffer b: NB x wl), which keeps the lanes busy on stages with few butterflies.
 constexpr int NB = 1;  // the transform engines run one sequence per warp
+static_assert(NB == 1, "column slabs index with cols == 1 << lw");
 
 __device__ __forceinline__ float2 *warp_area(float2 *base, int warp, int wl) { return base + size_t(warp) * 2 * NB * wl; }
 
@@ -261,7 +262,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_fwd_cols_kernel(FsimGroup g, const
     float2 *S = g.spec + size_t(plane) * g.n;
     // column c lives in warp c / NB, slot c % NB
     for (int idx = threadIdx.x; idx < cols * g.h2; idx += blockDim.x) {
-        const int c = idx % cols, y = idx / cols;
+        const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
         if (c < nc) warp_area(work, c / NB, wl)[(c % NB) * wl + y] = S[size_t(y) * g.w2 + x0 + c];
     }
     __syncthreads();
@@ -273,7 +274,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_fwd_cols_kernel(FsimGroup g, const
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < cols * g.h2; idx += blockDim.x) {
-        const int c = idx % cols, y = idx / cols;
+        const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
         if (c < nc) S[size_t(y) * g.w2 + x0 + c] = warp_area(work, c / NB, wl)[parity * NB * wl + (c % NB) * wl + y];
     }
 }
@@ -298,7 +299,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_cols_kernel(FsimGroup g, const
     float2 *work = Sl + size_t(cols) * h2;  // per warp: a, b of NB x wl each
     const float2 *src = g.spec + size_t(g.pair0 * 2 + plane) * g.n;
     for (int idx = threadIdx.x; idx < cols * h2; idx += blockDim.x) {
-        const int c = idx % cols, y = idx / cols;
+        const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
         if (c < nc) Sl[size_t(c) * h2 + y] = consts_mode ? make_float2(1.f, 0.f) : src[size_t(y) * g.w2 + x0 + c];
     }
     __syncthreads();
@@ -323,7 +324,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_cols_kernel(FsimGroup g, const
         __syncthreads();
         float2 *dst = g.T + (size_t(plane) * 16 + z) * g.n;
         for (int idx = threadIdx.x; idx < cols * h2; idx += blockDim.x) {
-            const int c = idx % cols, y = idx / cols;
+            const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
             if (c < nc) dst[size_t(y) * g.w2 + x0 + c] = warp_area(work, c / NB, wl)[parity * NB * wl + (c % NB) * wl + y];
         }
         __syncthreads();
@@ -391,19 +392,20 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_kernel(FsimGroup g, const
     const float invN = 1.0f / float(g.n);
     if (!consts_mode) {
         const int gp = g.pair0 * 2 + plane;
-        for (int idx = threadIdx.x; idx < rr * w2; idx += blockDim.x) {
-            const int rl = idx / w2, x = idx - rl * w2;
+        for (int rl = 0; rl < rr; rl++) {
             const int y = y0 + rl;
-            if (y >= g.h2) continue;
-            float2 v[4];
+            if (y >= g.h2) break;
+            const size_t row = (size_t(gp) * 4 + o) * g.n + size_t(y) * w2;
+            for (int x = threadIdx.x; x < w2; x += blockDim.x) {
+                float2 v[4];
 #pragma unroll
-            for (int q = 0; q < 4; q++) v[q] = at(rl, q, x);
-            float sA, en, e0;
-            response_sums(v, invN, sA, en, e0);
-            const size_t off = (size_t(gp) * 4 + o) * g.n + size_t(y) * w2 + x;
-            g.amp[off] = sA;
-            g.energy[off] = en;
-            g.eo0[off] = e0;
+                for (int q = 0; q < 4; q++) v[q] = at(rl, q, x);
+                float sA, en, e0;
+                response_sums(v, invN, sA, en, e0);
+                g.amp[row + x] = sA;
+                g.energy[row + x] = en;
+                g.eo0[row + x] = e0;
+            }
         }
     } else {
         const int y = y0;  // rr == 1
