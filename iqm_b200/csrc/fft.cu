@@ -21,13 +21,19 @@ struct FftPlan {
 
 namespace {
 
-// Radices the warp engine computes in registers, and the stage count of the best factorisation.
-const int kRegRadix[] = {2, 3, 4, 5, 8};
+// Radices the engines compute in registers, with an estimate of the instructions one butterfly
+// costs a lane: loads and stores of its p points, p-1 twiddle loads and products, the p-point DFT
+// itself and the per-iteration index work.
+struct RegRadix {
+    int p, cost;
+};
+const RegRadix kRegRadix[] = {{2, 23}, {3, 38}, {4, 49}, {5, 74}, {6, 83}, {8, 113},
+                              {9, 164}, {10, 163}, {12, 185}, {15, 272}};
 
-bool is_reg_radix(int p) {
-    for (int r : kRegRadix)
-        if (r == p) return true;
-    return false;
+int butterfly_cost(int p) {
+    for (const RegRadix &r : kRegRadix)
+        if (r.p == p) return r.cost;
+    return -1;
 }
 
 bool is_prime(int p) {
@@ -37,31 +43,36 @@ bool is_prime(int p) {
     return true;
 }
 
-// Radix sequence for n with the fewest stages (register radices, plus odd primes up to
-// FFT_MAX_GENERIC as direct butterflies, which count double); odd radices first so the first
-// stage's strided writes avoid shared-memory bank conflicts.  False when n has a prime factor
-// above FFT_MAX_GENERIC.
+// Radix sequence for n of least estimated warp time: a radix-p stage has n/p butterflies, which a
+// warp runs 32 at a time, so it costs ceil(n / 32p) times the butterfly's cost, plus a fixed
+// per-stage cost for the shared-memory round trip.  Odd primes up to FFT_MAX_GENERIC without a
+// register kernel run as direct O(p^2) butterflies.  Odd radices come first so the first stage's
+// strided writes avoid shared-memory bank conflicts.  False when n has a prime factor above
+// FFT_MAX_GENERIC.
 bool factor(int n, std::vector<int> &r) {
     r.clear();
     if (n == 1) return true;
-    // best[m] = (cost, radix) for transforming length m
-    std::vector<int> cost(n + 1, 1 << 20), pick(n + 1, 0);
+    constexpr long long kInf = 1LL << 50;
+    std::vector<long long> cost(n + 1, kInf);
+    std::vector<int> pick(n + 1, 0);
     cost[1] = 0;
     for (int m = 2; m <= n; m++) {
         if (n % m) continue;
         for (int p = 2; p <= m && p <= FFT_MAX_GENERIC; p++) {
-            if (m % p) continue;
-            int c;
-            if (is_reg_radix(p)) c = 2;
-            else if (is_prime(p)) c = 5;
-            else continue;
-            if (cost[m / p] + c < cost[m] || (cost[m / p] + c == cost[m] && p > pick[m])) {
-                cost[m] = cost[m / p] + c;
+            if (m % p || cost[m / p] >= kInf) continue;
+            long long w = butterfly_cost(p);
+            if (w < 0) {
+                if (!is_prime(p)) continue;
+                w = 10 + 2 * p + 5 * p * p;
+            }
+            const long long c = cost[m / p] + (long long)((n / p + 31) / 32) * w + 20;
+            if (c < cost[m] || (c == cost[m] && p > pick[m])) {
+                cost[m] = c;
                 pick[m] = p;
             }
         }
     }
-    if (cost[n] >= (1 << 20)) return false;
+    if (cost[n] >= kInf) return false;
     for (int m = n; m > 1; m /= pick[m]) r.push_back(pick[m]);
     std::stable_sort(r.begin(), r.end(), [](int x, int y) { return (x & 1) > (y & 1); });
     return true;

@@ -4,7 +4,8 @@
 // with sign -1 and no scaling, :378 inverse with sign +1 and normalize = 1/N).  Here a transform
 // of length n runs inside one CTA as a Stockham auto-sort FFT: log_p stages, each reading one
 // buffer and writing the other, so no bit reversal is needed.  n is factored into radices
-// 8, 4, 2, 3, 5, 7 and other odd primes up to 61 (an O(p^2) butterfly); a length with a larger
+// computed in registers (2, 3, 4, 5, 6, 8, 9, 10, 12, 15) and other odd primes up to 61 (an O(p^2)
+// butterfly, read from the length's table); a length with a larger
 // prime factor is computed with Bluestein's chirp-z algorithm on a power-of-two length m >= 2n-1.
 //
 // Stage s with radix p and stride L (the product of the earlier radices), butterfly j in [0, n/p):
@@ -129,6 +130,78 @@ __device__ __forceinline__ void dft_small<8>(float2 *v, float s) {
     v[3] = cadd(e[3], t3); v[7] = csub(e[3], t3);
 }
 
+// Composite sizes from the small kernels above.  Coprime N1 x N2 (6, 10, 12, 15): Good-Thomas
+// prime-factor mapping, input n = (N2 n1 + N1 n2) mod N, output k = (N2 a k1 + N1 b k2) mod N with
+// a = N2^-1 mod N1 and b = N1^-1 mod N2, so no twiddles are needed between the two passes.
+__host__ __device__ constexpr int mod_inverse(int x, int m) {
+    for (int i = 1; i < m; i++)
+        if ((x * i) % m == 1) return i;
+    return 1;
+}
+
+template <int N1, int N2>
+__device__ __forceinline__ void dft_pfa(float2 *v, float s) {
+    constexpr int N = N1 * N2;
+    constexpr int A = mod_inverse(N2 % N1, N1), B = mod_inverse(N1 % N2, N2);
+    float2 t[N2][N1];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; n2++) {
+        float2 a[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; n1++) a[n1] = v[(n1 * N2 + n2 * N1) % N];
+        dft_small<N1>(a, s);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; k1++) t[n2][k1] = a[k1];
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) {
+        float2 b[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; n2++) b[n2] = t[n2][k1];
+        dft_small<N2>(b, s);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) v[(k1 * N2 * A + k2 * N1 * B) % N] = b[k2];
+    }
+}
+
+template <>
+__device__ __forceinline__ void dft_small<6>(float2 *v, float s) { dft_pfa<2, 3>(v, s); }
+template <>
+__device__ __forceinline__ void dft_small<10>(float2 *v, float s) { dft_pfa<2, 5>(v, s); }
+template <>
+__device__ __forceinline__ void dft_small<12>(float2 *v, float s) { dft_pfa<4, 3>(v, s); }
+template <>
+__device__ __forceinline__ void dft_small<15>(float2 *v, float s) { dft_pfa<3, 5>(v, s); }
+
+// 9 = 3 x 3 (Cooley-Tukey): n = 3 n1 + n2, k = k1 + 3 k2; inner DFTs over n1, twiddle
+// W9^(n2 k1), outer DFTs over n2.  cos/sin of 2 pi m / 9 for m = 1, 2, 4.
+template <>
+__device__ __forceinline__ void dft_small<9>(float2 *v, float s) {
+    const float2 w1 = make_float2(0.76604444311897804f, s * 0.64278760968653933f);
+    const float2 w2 = make_float2(0.17364817766693035f, s * 0.98480775301220806f);
+    const float2 w4 = make_float2(-0.93969262078590838f, s * 0.34202014332566873f);
+    float2 a[3][3];
+#pragma unroll
+    for (int n2 = 0; n2 < 3; n2++) {
+        a[n2][0] = v[n2];
+        a[n2][1] = v[3 + n2];
+        a[n2][2] = v[6 + n2];
+        dft_small<3>(a[n2], s);
+    }
+    a[1][1] = cmul(a[1][1], w1);
+    a[1][2] = cmul(a[1][2], w2);
+    a[2][1] = cmul(a[2][1], w2);
+    a[2][2] = cmul(a[2][2], w4);
+#pragma unroll
+    for (int k1 = 0; k1 < 3; k1++) {
+        float2 b[3] = {a[0][k1], a[1][k1], a[2][k1]};
+        dft_small<3>(b, s);
+        v[k1] = b[0];
+        v[k1 + 3] = b[1];
+        v[k1 + 6] = b[2];
+    }
+}
+
 // One Stockham stage of radix P over `batch` transforms (buffers `stride` apart).
 template <int P>
 __device__ __forceinline__ void stage_fixed(const float2 *in, float2 *out, int n, int L, const float2 *tw,
@@ -195,7 +268,12 @@ __device__ inline float2 *fft_stockham(float2 *a, float2 *b, int n, int nst, con
             case 3: stage_fixed<3>(in, out, n, L, tw, s, batch, stride); break;
             case 4: stage_fixed<4>(in, out, n, L, tw, s, batch, stride); break;
             case 5: stage_fixed<5>(in, out, n, L, tw, s, batch, stride); break;
+            case 6: stage_fixed<6>(in, out, n, L, tw, s, batch, stride); break;
             case 8: stage_fixed<8>(in, out, n, L, tw, s, batch, stride); break;
+            case 9: stage_fixed<9>(in, out, n, L, tw, s, batch, stride); break;
+            case 10: stage_fixed<10>(in, out, n, L, tw, s, batch, stride); break;
+            case 12: stage_fixed<12>(in, out, n, L, tw, s, batch, stride); break;
+            case 15: stage_fixed<15>(in, out, n, L, tw, s, batch, stride); break;
             default: stage_generic(in, out, n, L, p, tw, s, batch, stride); break;
         }
         L *= p;
@@ -321,7 +399,12 @@ __device__ inline float2 *warp_stockham(float2 *a, float2 *b, int n, int nst, co
             case 3: warp_stage<3>(in, out, n, L, invL, iq, w, s, nb, wl); break;
             case 4: warp_stage<4>(in, out, n, L, invL, iq, w, s, nb, wl); break;
             case 5: warp_stage<5>(in, out, n, L, invL, iq, w, s, nb, wl); break;
+            case 6: warp_stage<6>(in, out, n, L, invL, iq, w, s, nb, wl); break;
             case 8: warp_stage<8>(in, out, n, L, invL, iq, w, s, nb, wl); break;
+            case 9: warp_stage<9>(in, out, n, L, invL, iq, w, s, nb, wl); break;
+            case 10: warp_stage<10>(in, out, n, L, invL, iq, w, s, nb, wl); break;
+            case 12: warp_stage<12>(in, out, n, L, invL, iq, w, s, nb, wl); break;
+            case 15: warp_stage<15>(in, out, n, L, invL, iq, w, s, nb, wl); break;
             default: warp_stage_generic(in, out, n, L, invL, iq, p, w, tw, s, nb, wl); break;
         }
         float2 *t = in;

@@ -217,8 +217,8 @@ struct FixedEngine {
         return FP::run(a, b, stw, s);
     }
 };
-using Engine270 = FixedEngine<iqm::FixedPlan<270, 5, 3, 3, 3, 2>>;
-using Engine480 = FixedEngine<iqm::FixedPlan<480, 5, 3, 8, 4>>;
+using Engine270 = FixedEngine<iqm::FixedPlan<270, 9, 3, 10>>;
+using Engine480 = FixedEngine<iqm::FixedPlan<480, 15, 8, 4>>;
 
 // forward transform (src/gpu/fsim/fsim.cpp:270-368: luma as complex (Y, 0), sign -1, unscaled),
 // NB rows per warp.
@@ -712,8 +712,8 @@ int engine_id(const iqm::FftLen &L) {
             if (L.radix[i++] != r) return false;
         return true;
     };
-    if (is(270, {5, 3, 3, 3, 2})) return 1;
-    if (is(480, {5, 3, 8, 4})) return 2;
+    if (is(270, {9, 3, 10})) return 1;
+    if (is(480, {15, 8, 4})) return 2;
     return 0;
 }
 
