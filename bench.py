@@ -1,15 +1,18 @@
 """Throughput benchmark of the IQM metric path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--metric fsim|ssim|flip|msvd]
-                    [--impl ours|reference] [--pairs B] [--no-cpu-baseline]
+                    [--size 1080p|4k] [--batch] [--impl ours|reference] [--pairs B] [--no-cpu-baseline]
 
-One step = one pass of the metric over a batch of B synthetic 1080p pairs already resident in
-HBM (distinct buffers; the batch is larger than the 126 MB L2, so no flush is needed between
-steps).  `value` is pairs/s over all ranks; `e2e` is the same metric through the host API
-(pinned host images copied in and scores copied out inside the timed region).  With --impl
-reference the CPU restatement of the reference's arithmetic (oracle/, all host threads) is timed
-on the same workload instead.  Under torchrun each rank evaluates its own batch (independent
-pairs, no collective on the data path): weak scaling.
+One step = one pass of the metric over a batch of B synthetic pairs (1920x1080 by default, 3840x2160
+with --size 4k) already resident in HBM (distinct buffers; the batch is larger than the 126 MB L2,
+so no flush is needed between steps).  `value` is pairs/s over all ranks; `e2e` is the same metric
+through the host API (pinned host images copied in and scores copied out inside the timed region).
+With --batch a step is the uneven-size batch instead: 256 pairs with sides uniform in [256, 2048],
+SSIM on grey pairs and FSIM on RGB pairs, each metric one CUDA-graph batch plan replay.  With
+--impl reference the CPU restatement of the reference's arithmetic (oracle/, all host threads) is
+timed on the same workload instead.  Under torchrun each rank evaluates its own batch (independent
+pairs, no collective on the data path): weak scaling; with --batch the 256 pairs are sharded
+longest-processing-time first over the ranks: strong scaling.
 """
 import argparse
 import json
@@ -23,7 +26,15 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-W1080, H1080 = 1920, 1080
+SIZES = {"1080p": (1920, 1080), "4k": (3840, 2160)}
+W, H = SIZES["1080p"]
+SIZE = "1080p"
+
+
+def set_size(name):
+    global W, H, SIZE
+    W, H = SIZES[name]
+    SIZE = name
 
 # metric -> (workload name, synthetic generator name, score count per pair)
 WORKLOADS = {
@@ -35,11 +46,24 @@ WORKLOADS = {
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of each metric's dominant
 # kernel from an ncu capture of this benchmark, with the pairs that launch processed; the summaries
 # under profiles/ give the commands.  Scaled by pairs per launch when the live launch differs.
-TRAFFIC = {}
+TRAFFIC = {
+    # ssim_kernel, 32 pairs: 566,863,104 B read + 3,258,624 B written (profiles/ssim_kernel_1080p.md)
+    "ssim": {"kernel": "ssim_kernel", "bytes_per_launch": 570121728, "pairs_per_launch": 32},
+    # fsim_inv_cols_kernel, one chunk of 2 pairs: 12,486,144 + 13,263,360 B (profiles/fsim_inv_cols_kernel_1080p.md)
+    "fsim": {"kernel": "fsim_inv_cols_kernel", "bytes_per_launch": 25749504, "pairs_per_launch": 2},
+    # flip_vcols_kernel, 16 pairs: 1,642,060,544 + 11,937,024 B (profiles/flip_vcols_kernel_1080p.md)
+    "flip": {"kernel": "flip_vcols_kernel", "bytes_per_launch": 1653997568, "pairs_per_launch": 16},
+    # msvd_block_kernel, 32 pairs: 527,325,440 + 6,860,288 B (profiles/msvd_block_kernel_1080p.md)
+    "msvd": {"kernel": "msvd_block_kernel", "bytes_per_launch": 534185728, "pairs_per_launch": 32},
+}
+
+
+def workload_name(metric):
+    return WORKLOADS[metric][0].replace("1080p", SIZE)
 
 
 def metric_name(metric):
-    return "1080p image pairs/sec (%s)" % metric.upper()
+    return "%s image pairs/sec (%s)" % ("1080p" if SIZE == "1080p" else "4K", metric.upper())
 
 
 def parse():
@@ -49,7 +73,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--metric", default=None)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--pairs", type=int, default=32)
+    ap.add_argument("--pairs", type=int, default=None, help="pairs per step (default 32 at 1080p, 16 at 4K)")
+    ap.add_argument("--size", default="1080p", choices=sorted(SIZES))
+    ap.add_argument("--batch", action="store_true",
+                    help="uneven-size batch: 256 pairs, sides uniform in [256, 2048], SSIM + FSIM through one "
+                         "CUDA-graph batch plan")
     ap.add_argument("--distinct", type=int, default=4, help="distinct synthetic pairs (replicated to --pairs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -64,24 +92,7 @@ def make_pairs(metric, n):
     from iqm_b200 import synth
     gen = getattr(synth, WORKLOADS[metric][1])
     cfg = {"fsim": 1, "ssim": 0, "flip": 2, "msvd": 2}[metric]
-    return [gen(H1080, W1080, config=cfg, pair=i) for i in range(n)]
-
-
-def metric_implemented(metric, device=0):
-    import iqm_b200
-    try:
-        rt = iqm_b200.Runtime(device)
-    except Exception:
-        return False
-    try:
-        a = np.zeros((64, 64, 4), np.uint8)
-        obj = {"fsim": iqm_b200.FSIM, "ssim": iqm_b200.SSIM, "flip": iqm_b200.FLIP, "msvd": iqm_b200.SVD}[metric](rt)
-        obj.compute_metric(a, a)
-        return True
-    except iqm_b200.IQMError as e:
-        return e.code != iqm_b200.IQM_EUNSUPPORTED
-    finally:
-        rt.close()
+    return [gen(H, W, config=cfg, pair=i) for i in range(n)]
 
 
 class Clocks:
@@ -154,7 +165,7 @@ def cpu_baseline(metric, pairs, seconds, one_pair_only=False):
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return {"value": done / el, "unit": "pairs/s", "cores": cores, "kind": "port",
             "sample": "%d pair(s) of the %s workload (%dx%d), %.1f s, oracle FP32 build, OpenMP" % (
-                done, WORKLOADS[metric][0], W1080, H1080, el)}
+                done, workload_name(metric), W, H, el)}
 
 
 def run_reference(args, metric, rank, world):
@@ -176,17 +187,240 @@ def run_reference(args, metric, rank, world):
             "unit": "pairs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded 1/f^2 noise pairs)",
-            "config": {"workload": WORKLOADS[metric][0], "pairs_per_step": 1, "width": W1080, "height": H1080},
+            "config": {"workload": workload_name(metric), "pairs_per_step": 1, "width": W, "height": H},
             "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": "port",
                              "sample": "1 pair per step, oracle FP32 build (reference arithmetic restated), OpenMP"},
             "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
+def batch_pairs(n=256, distinct=2):
+    """The uneven-size batch: n pairs, width and height drawn independently and uniformly from
+    [256, 2048] (seeded); SSIM pairs grey, FSIM pairs RGB, each a crop of one of `distinct`
+    2048x2048 synthetic pairs."""
+    from iqm_b200 import synth
+    sizes = synth.uneven_sizes(n, seed=3000)
+    greys = [synth.grey_pair(2048, 2048, config=3, pair=i) for i in range(distinct)]
+    rgbs = [synth.rgb_gain_pair(2048, 2048, config=3, pair=i) for i in range(distinct)]
+
+    def crop(p, w, h):
+        return np.ascontiguousarray(p[0][:h, :w]), np.ascontiguousarray(p[1][:h, :w])
+
+    grey = [crop(greys[i % distinct], w, h) for i, (w, h) in enumerate(sizes)]
+    rgb = [crop(rgbs[i % distinct], w, h) for i, (w, h) in enumerate(sizes)]
+    return sizes, grey, rgb
+
+
+def run_batch(args, rank, world, local):
+    """--batch: 256 uneven pairs per step, SSIM (grey) + FSIM (RGB), each metric one CUDA-graph batch
+    plan replay; under torchrun the pairs are LPT-sharded over the ranks (strong scaling)."""
+    metric = "uneven-size batch pairs/sec (SSIM+FSIM)"
+    sizes, grey, rgb = batch_pairs()
+    N = len(sizes)
+    total_bytes = sum(8 * w * h for w, h in sizes)  # per metric: both RGBA8 images read once
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from oracle import Oracle
+        o = Oracle("f32")
+        for i in range(max(0, args.warmup)):
+            o.ssim(*grey[i]), o.fsim(*rgb[i])
+        times = []
+        for k in range(args.steps):
+            i = (k * 37) % N
+            t0 = time.perf_counter()
+            o.ssim(*grey[i])
+            o.fsim(*rgb[i])
+            times.append(time.perf_counter() - t0)
+        value = 1.0 / float(np.mean(times))
+        cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+        print(json.dumps({
+            "impl": "reference", "metric": metric, "value": value, "unit": "pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": "batch256_ssim_fsim", "pairs_per_step": 1, "sizes": "uniform [256, 2048]"},
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": "port",
+                             "sample": "1 pair of the batch per step (SSIM grey + FSIM RGB), oracle FP32, OpenMP"},
+            "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+            flush=True)
+        return
+
+    import ctypes
+    import torch
+    import iqm_b200
+    from iqm_b200 import parallel
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    costs = [parallel.pair_cost("fsim", w, h) + parallel.pair_cost("ssim", w, h) for w, h in sizes]
+    mine = parallel.shard_lpt(costs, world)[rank]
+    rt = iqm_b200.Runtime(local)
+    stream = torch.cuda.Stream()
+    rt.set_stream(stream.cuda_stream)
+    bufs = []
+
+    def upload(pairs):
+        items = []
+        for i in mine:
+            a, b = pairs[i]
+            da = torch.from_numpy(a.reshape(-1)).cuda()
+            db = torch.from_numpy(b.reshape(-1)).cuda()
+            bufs.extend([da, db])
+            items.append((da.data_ptr(), db.data_ptr(), a.shape[1], a.shape[0], a.shape[1] * 4))
+        return items
+
+    g_items, c_items = upload(grey), upload(rgb)
+    n = len(mine)
+    d_ssim = torch.zeros(max(1, n), dtype=torch.float64, device="cuda")
+    d_fsim = torch.zeros(max(1, 2 * n), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    plans = []
+    if n:
+        plans.append(iqm_b200.BatchPlan(rt, iqm_b200.METRIC_SSIM, g_items, d_ssim.data_ptr(), autotune=False))
+        plans.append(iqm_b200.BatchPlan(rt, iqm_b200.METRIC_FSIM, c_items, d_fsim.data_ptr(), autotune=True))
+    launches = sum(p.info()[1] for p in plans)
+
+    def step():
+        for p in plans:
+            p.run()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = N / (ms_per_step / 1e3)
+
+    # per-kernel device time from the eager form of the same step (graph replays carry no events)
+    ktimes = {}
+    if n:
+        rt.set_kernel_timing(True)
+        for _ in range(2):
+            iqm_b200.SSIM(rt).compute_dev(g_items, d_ssim.data_ptr())
+            iqm_b200.FSIM(rt).compute_dev(c_items, d_fsim.data_ptr())
+        ktimes = rt.kernel_times()
+        rt.set_kernel_timing(False)
+    ktotal = sum(t for _, t in ktimes.values()) or 1.0
+    roof = None
+    if ktimes:
+        kname, (klaunch, kms) = max(ktimes.items(), key=lambda kv: kv[1][1])
+        my_bytes = sum(8 * sizes[i][0] * sizes[i][1] for i in mine)
+        alg_launch = 2 * my_bytes / max(1, klaunch)  # two timing steps
+        achieved = alg_launch / (kms / max(1, klaunch) / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                "traffic": None, "kernel": kname, "avg_launch_us": 1e3 * kms / max(1, klaunch),
+                "kernel_share": kms / ktotal,
+                "pipeline_frac": 2 * total_bytes / world / (ms_per_step / 1e3) / 1e9 / hbm_peak,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "timing": "CUDA events around every launch of an eager pass (graph replays carry none)"}
+
+    # end to end through the host batch API: pinned host images in, scores out, every step
+    pin_g = [(torch.from_numpy(grey[i][0]).pin_memory(), torch.from_numpy(grey[i][1]).pin_memory()) for i in mine]
+    pin_c = [(torch.from_numpy(rgb[i][0]).pin_memory(), torch.from_numpy(rgb[i][1]).pin_memory()) for i in mine]
+    arr_g = iqm_b200._pairs([(a.data_ptr(), b.data_ptr(), a.shape[1], a.shape[0], a.shape[1] * 4) for a, b in pin_g])
+    arr_c = iqm_b200._pairs([(a.data_ptr(), b.data_ptr(), a.shape[1], a.shape[0], a.shape[1] * 4) for a, b in pin_c])
+    out = np.empty(3 * max(1, n), np.float64)
+    outp = out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    sp = iqm_b200.SSIM(rt).params()
+    fp = iqm_b200.FLIPArguments().c()
+
+    def e2e_step():
+        if n:
+            rt.check(rt.L.iqm_batch(rt.h, iqm_b200.METRIC_SSIM, arr_g, n, ctypes.byref(sp), ctypes.byref(fp), 0, 0,
+                                    outp))
+            rt.check(rt.L.iqm_batch(rt.h, iqm_b200.METRIC_FSIM, arr_c, n, ctypes.byref(sp), ctypes.byref(fp), 0, 0,
+                                    outp))
+
+    e2e_step()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(2, args.steps // 4)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ems], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+    my_in = sum(2 * sizes[i][0] * sizes[i][1] * 4 for i in mine)
+    line = {
+        "metric": metric, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded; crops of 2 distinct 2048x2048 pairs per metric)",
+        "config": {"workload": "batch256_ssim_fsim", "pairs_per_step": N, "sizes": "w, h uniform in [256, 2048]",
+                   "precision": "fp32", "parallelism": "lpt shards" if world > 1 else "single",
+                   "form": "one CUDA-graph batch plan per metric, FSIM shapes autotuned",
+                   "l2": "inputs larger than L2 (%.0f MB per metric per step), no flush" % (total_bytes / 1e6)},
+        "roofline": roof,
+        "kernels": {k: {"launches": c, "avg_us": 1e3 * t / max(1, c), "share": t / ktotal} for k, (c, t) in ktimes.items()},
+        "e2e": {"value": N / (ems / e2e_steps / 1e3), "unit": "pairs/s", "h2d_bytes_per_step": 2 * my_in,
+                "d2h_bytes_per_step": 3 * 8 * n},
+        "gpu_launches": launches * args.steps, "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from oracle import Oracle
+        o = Oracle("f32")
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < args.cpu_seconds:
+            i = (done * 37) % N
+            o.ssim(*grey[i])
+            o.fsim(*rgb[i])
+            done += 1
+        el = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": done / el, "unit": "pairs/s",
+                                "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+                                "kind": "port", "sample": "%d pairs of the batch (SSIM + FSIM), %.1f s, oracle FP32, "
+                                                          "OpenMP" % (done, el)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for p in plans:
+        p.close()
+    rt.close()
+    if dist:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
+    set_size(args.size)
     rank, world, local = dist_env()
-    metric = args.metric or ("fsim" if metric_implemented("fsim", local) else "ssim")
+    if args.batch:
+        run_batch(args, rank, world, local)
+        return
+    metric = args.metric or "fsim"
     if args.impl == "reference":
         run_reference(args, metric, rank, world)
         return
@@ -208,8 +442,8 @@ def main():
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_note = "measured" if "hbm_gbs" in peaks else "fallback"
 
-    B = args.pairs
-    host_pairs = make_pairs(metric, min(args.distinct, B))
+    B = args.pairs or (32 if SIZE == "1080p" else 64)
+    host_pairs = make_pairs(metric, min(args.distinct if SIZE == "1080p" else min(args.distinct, 2), B))
     rt = iqm_b200.Runtime(local)
     stream = torch.cuda.Stream()
     rt.set_stream(stream.cuda_stream)
@@ -218,7 +452,7 @@ def main():
     flip_args = iqm_b200.FLIPArguments(3840.0, 0.7, 0.7)  # 67.02 pixels per degree
 
     # device-resident batch: B distinct buffers (replicas of the distinct synthetic pairs)
-    img_bytes = H1080 * W1080 * 4
+    img_bytes = H * W * 4
     with torch.cuda.stream(stream):
         dev = torch.empty((B, 2, img_bytes), dtype=torch.uint8, device="cuda")
         for i in range(B):
@@ -228,7 +462,7 @@ def main():
         d_scores = torch.zeros(B * nscore, dtype=torch.float64, device="cuda")
     stream.synchronize()
     base = dev.data_ptr()
-    dev_pairs = [(base + (2 * i) * img_bytes, base + (2 * i + 1) * img_bytes, W1080, H1080, W1080 * 4) for i in range(B)]
+    dev_pairs = [(base + (2 * i) * img_bytes, base + (2 * i + 1) * img_bytes, W, H, W * 4) for i in range(B)]
 
     def step():
         if metric == "flip":
@@ -299,7 +533,7 @@ def main():
         pb = torch.from_numpy(b).pin_memory()
         pin.append((pa, pb))
     import ctypes
-    items = [(pa.data_ptr(), pb.data_ptr(), W1080, H1080, W1080 * 4) for pa, pb in pin]
+    items = [(pa.data_ptr(), pb.data_ptr(), W, H, W * 4) for pa, pb in pin]
     arr = iqm_b200._pairs(items)
     out = np.empty(B * nscore, np.float64)
     outp = out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
@@ -343,7 +577,7 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded 1/f^2 noise pairs, %d distinct replicated to %d device buffers)" % (
             len(host_pairs), B),
-        "config": {"workload": WORKLOADS[metric][0], "pairs_per_step": B, "width": W1080, "height": H1080,
+        "config": {"workload": workload_name(metric), "pairs_per_step": B, "width": W, "height": H,
                    "precision": "fp32", "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (%.0f MB per step), no flush" % (alg_bytes / 1e6)},
         "roofline": roof, "kernels": kernels, "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "clocks": clk,

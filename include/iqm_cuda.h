@@ -45,7 +45,8 @@ typedef struct iqm_ctx iqm_ctx;
 
 typedef enum {
     IQM_FP32 = 0,  /* plain FP32 arithmetic, FP64 pooling sums                                   */
-    IQM_MIXED = 1  /* reduced-precision storage / tensor-core form where a metric provides one   */
+    IQM_MIXED = 1  /* reduced-precision storage / tensor-core form; no metric provides one in
+                      this build, so FSIM returns IQM_EUNSUPPORTED for it                          */
 } iqm_precision;
 
 /* ---- context --------------------------------------------------------------------------- */

@@ -1065,6 +1065,8 @@ void check_fsim_args(const iqm_pair *pairs, int n, iqm_precision precision, int 
     iqm::check_pairs(pairs, n, 1, 1);
     IQM_REQUIRE(energy_mode == 0 || energy_mode == 1, "energy_mode must be 0 or 1");
     IQM_REQUIRE(precision == IQM_FP32 || precision == IQM_MIXED, "unknown precision");
+    if (precision == IQM_MIXED)
+        throw iqm::Error{IQM_EUNSUPPORTED, "FSIM: no reduced-precision form in this build (use IQM_FP32)"};
     for (int i = 0; i < n; i++) {
         const int F = downscale_factor(pairs[i].w, pairs[i].h);
         int w2, h2;

@@ -71,3 +71,12 @@ def test_fsim_errors(rt):
     with pytest.raises(iqm_b200.IQMError) as e:
         f.compute_metric(a, a)
     assert e.value.code == iqm_b200.IQM_EINVAL
+
+
+def test_fsim_mixed_precision_is_reported_unsupported(rt):
+    a, b = synth.rgb_gain_pair(64, 80, config=1, pair=1)
+    with pytest.raises(iqm_b200.IQMError) as e:
+        iqm_b200.FSIM(rt, precision=iqm_b200.IQM_MIXED).compute_metric(a, b)
+    assert e.value.code == iqm_b200.IQM_EUNSUPPORTED
+    # the context stays usable
+    assert 0.0 < iqm_b200.FSIM(rt).compute_metric(a, b).fsim <= 1.0
