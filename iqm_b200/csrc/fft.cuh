@@ -228,29 +228,57 @@ __device__ __forceinline__ void stage_fixed(const float2 *in, float2 *out, int n
     }
 }
 
-// Radix-p stage for an odd prime p <= FFT_MAX_GENERIC: direct p-point DFT from the table.
-__device__ __forceinline__ void stage_generic(const float2 *in, float2 *out, int n, int L, int p,
+// Direct p-point DFT (p odd) of butterfly j whose inputs src[j + r q] are already twiddled.  The
+// symmetric pairs a_r = x_r + x_(p-r), b_r = x_r - x_(p-r) overwrite the inputs (each butterfly owns
+// its inputs, and a stage's input buffer is dead after it); then X_qq and X_(p-qq) come together as
+// x_0 + sum a_r cos(t) +- i s sum b_r sin(t), t = 2 pi (r qq mod p) / p, with cos and sin read from
+// the length's table (entry (r qq mod p) q) and the exponent advanced by qq per term.
+__device__ __forceinline__ void odd_dft_inplace(float2 *src, float2 *dst, int j, int q, int p, int L, int base,
+                                                const float2 *tw, float s) {
+    const int h = (p - 1) >> 1;
+    const float2 x0 = src[j];
+    float2 sum = x0;
+    for (int r = 1; r <= h; r++) {
+        const float2 u = src[j + r * q], v = src[j + (p - r) * q];
+        const float2 a = cadd(u, v);
+        src[j + r * q] = a;
+        src[j + (p - r) * q] = csub(u, v);
+        sum = cadd(sum, a);
+    }
+    dst[base] = sum;
+    for (int qq = 1; qq <= h; qq++) {
+        float2 re = x0, im = make_float2(0.f, 0.f);
+        int e = 0;
+        for (int r = 1; r <= h; r++) {
+            e += qq;
+            if (e >= p) e -= p;
+            const float2 w = __ldg(tw + e * q);  // (cos t, -sin t)
+            const float2 a = src[j + r * q], b = src[j + (p - r) * q];
+            re.x = fmaf(a.x, w.x, re.x);
+            re.y = fmaf(a.y, w.x, re.y);
+            im.x = fmaf(b.x, -w.y, im.x);
+            im.y = fmaf(b.y, -w.y, im.y);
+        }
+        dst[base + qq * L] = make_float2(re.x - s * im.y, re.y + s * im.x);
+        dst[base + (p - qq) * L] = make_float2(re.x + s * im.y, re.y - s * im.x);
+    }
+}
+
+// Radix-p stage for an odd prime p <= FFT_MAX_GENERIC without a register kernel.
+__device__ __forceinline__ void stage_generic(float2 *in, float2 *out, int n, int L, int p,
                                               const float2 *tw, float s, int batch, int stride) {
     const int q = n / p;
     const int twstep = n / (L * p);
     const int total = batch * q;
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
         const int t = idx / q, j = idx - t * q;
-        const float2 *src = in + t * stride;
+        float2 *src = in + t * stride;
         float2 *dst = out + t * stride;
         const int k = j % L;
         const int base = (j / L) * L * p + k;
-        for (int qq = 0; qq < p; qq++) {
-            float2 acc = make_float2(0.f, 0.f);
-            for (int r = 0; r < p; r++) {
-                float2 x = src[j + r * q];
-                if (k != 0 && r != 0) x = cmul(x, tw_at(tw, r * k * twstep, s));
-                // exp(s 2 pi i r qq / p) = table entry (r qq mod p) * (n / p)
-                const int e = (r * qq) % p;
-                acc = e ? cadd(acc, cmul(x, tw_at(tw, e * q, s))) : cadd(acc, x);
-            }
-            dst[base + qq * L] = acc;
-        }
+        if (k != 0)
+            for (int r = 1; r < p; r++) src[j + r * q] = cmul(src[j + r * q], tw_at(tw, r * k * twstep, s));
+        odd_dft_inplace(src, dst, j, q, p, L, base, tw, s);
     }
 }
 
@@ -356,32 +384,26 @@ __device__ __forceinline__ void warp_stage(const float2 *in, float2 *out, int n,
     }
 }
 
-// odd prime radix without a register kernel: direct p-point DFT from the length-n table
-__device__ __forceinline__ void warp_stage_generic(const float2 *in, float2 *out, int n, int L, float invL,
+// odd prime radix without a register kernel: twiddle in place, then the direct p-point DFT
+__device__ __forceinline__ void warp_stage_generic(float2 *in, float2 *out, int n, int L, float invL,
                                                    float invq, int p, const float2 *stw, const float2 *tw, float s,
                                                    int nb, int wl) {
     const int q = n / p;
     for (int idx = threadIdx.x & 31; idx < nb * q; idx += 32) {
         const int t = nb > 1 ? __float2int_rz((float(idx) + 0.5f) * invq) : 0;
         const int j = idx - t * q;
-        const float2 *src = in + t * wl;
+        float2 *src = in + t * wl;
         float2 *dst = out + t * wl;
         const int jl = __float2int_rz((float(j) + 0.5f) * invL);
         const int k = j - jl * L;
         const int base = jl * L * p + k;
-        for (int qq = 0; qq < p; qq++) {
-            float2 acc = make_float2(0.f, 0.f);
-            for (int r = 0; r < p; r++) {
-                float2 x = src[j + r * q];
-                if (k != 0 && r != 0) {
-                    const float2 w = stw[k * (p - 1) + r - 1];
-                    x = cmul(x, make_float2(w.x, -s * w.y));
-                }
-                const int e = (r * qq) % p;
-                acc = e ? cadd(acc, cmul(x, tw_at(tw, e * q, s))) : cadd(acc, x);
+        if (k != 0) {
+            for (int r = 1; r < p; r++) {
+                const float2 w = stw[k * (p - 1) + r - 1];
+                src[j + r * q] = cmul(src[j + r * q], make_float2(w.x, -s * w.y));
             }
-            dst[base + qq * L] = acc;
         }
+        odd_dft_inplace(src, dst, j, q, p, L, base, tw, s);
     }
 }
 

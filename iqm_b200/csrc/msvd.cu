@@ -157,29 +157,42 @@ __device__ __forceinline__ void svd8_values(float c[8][8], float s[8]) {
 #undef IQM_CSWAP
 }
 
+// Two lanes per block slot: the even lane takes the block of the distorted image, the odd lane the
+// same block of the reference; the odd lane's singular values reach the even lane by shuffle.  One
+// copy of the SVD code serves both images and twice as many blocks are in flight.
 __global__ void __launch_bounds__(BLOCK_THREADS) msvd_block_kernel(MsvdArgs args) {
-    const int slot = blockIdx.x * BLOCK_THREADS + threadIdx.x;
-    if (slot >= args.total_slots) return;
-    const int pi = find_pair(args.pairs, args.npairs, slot);
-    const MsvdPairDev &P = args.pairs[pi];
-    const int local = slot - P.slot_base;
-    const int bx = local % P.bw, by = local / P.bw;
-    float d = 0.0f;  // slots the reference never computes stay 0 (src/gpu/svd/svd.cpp:44,68-74)
-    if (bx < P.vx && by < P.vy) {
-        float c[8][8], si[8], sr[8];
-        load_block(P.a, P.pitch, 8 * bx, 8 * by, P.vec_ok, c);
-        svd8_values(c, si);
-        load_block(P.b, P.pitch, 8 * bx, 8 * by, P.vec_ok, c);
-        svd8_values(c, sr);
-        float acc = 0.0f;  // shaders/svd/svd.glsl:41-52: float, k = 0..7 in order
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const float t = si[k] - sr[k];
-            acc = fmaf(t, t, acc);
-        }
-        d = sqrtf(acc);
+    const int slot = (blockIdx.x * BLOCK_THREADS + threadIdx.x) >> 1;
+    const int img = threadIdx.x & 1;
+    const bool in_range = slot < args.total_slots;  // both lanes of a slot agree
+    bool computed = false;
+    MsvdPairDev P{};
+    int bx = 0, by = 0;
+    if (in_range) {
+        P = args.pairs[find_pair(args.pairs, args.npairs, slot)];
+        const int local = slot - P.slot_base;
+        bx = local % P.bw;
+        by = local / P.bw;
+        computed = bx < P.vx && by < P.vy;  // other slots stay 0 (src/gpu/svd/svd.cpp:44,68-74)
     }
-    args.dist[slot] = d;
+    // lanes that compute, fixed before the data-dependent sweeps (pairs of lanes agree)
+    const unsigned mask = __ballot_sync(0xffffffffu, computed);
+    if (computed) {
+        {  // one 8x8 block of one image
+            float c[8][8];
+            load_block(img ? P.b : P.a, P.pitch, 8 * bx, 8 * by, P.vec_ok, c);
+            float s[8];
+            svd8_values(c, s);
+            float acc = 0.0f;  // shaders/svd/svd.glsl:41-52: float, k = 0..7 in order
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const float sr = __shfl_xor_sync(mask, s[k], 1);
+                const float t = s[k] - sr;
+                acc = fmaf(t, t, acc);
+            }
+            if (!img) args.dist[slot] = sqrtf(acc);
+        }
+    }
+    if (in_range && !computed && !img) args.dist[slot] = 0.0f;
 }
 
 __global__ void __launch_bounds__(POOL_THREADS) msvd_pool_kernel(MsvdArgs args) {
@@ -256,7 +269,7 @@ void msvd_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const std::v
     a.total_slots = int(total);
     a.dist = static_cast<float *>(ctx->scratch.get(sizeof(float) * size_t(total), ctx->stream));
     a.scores = d_scores;
-    msvd_block_kernel<<<iqm::ceil_div(total, BLOCK_THREADS), BLOCK_THREADS, 0, ctx->stream>>>(a);
+    msvd_block_kernel<<<iqm::ceil_div(2 * total, BLOCK_THREADS), BLOCK_THREADS, 0, ctx->stream>>>(a);
     iqm::check_launch(ctx, "msvd_block_kernel");
     msvd_pool_kernel<<<n, POOL_THREADS, 0, ctx->stream>>>(a);
     iqm::check_launch(ctx, "msvd_pool_kernel");
