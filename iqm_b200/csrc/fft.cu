@@ -49,7 +49,7 @@ bool is_prime(int p) {
 // register kernel run as direct O(p^2) butterflies.  Odd radices come first so the first stage's
 // strided writes avoid shared-memory bank conflicts.  False when n has a prime factor above
 // FFT_MAX_GENERIC.
-bool factor(int n, std::vector<int> &r) {
+bool factor(int n, std::vector<int> &r, long long *total_cost = nullptr) {
     r.clear();
     if (n == 1) return true;
     constexpr long long kInf = 1LL << 50;
@@ -63,7 +63,8 @@ bool factor(int n, std::vector<int> &r) {
             long long w = butterfly_cost(p);
             if (w < 0) {
                 if (!is_prime(p)) continue;
-                w = 10 + 2 * p + 5 * p * p;
+                // in-place twiddles, symmetric pairs, then (p-1)^2/4 steps of 3 loads + 4 FMAs
+                w = 10 + 11 * p + (7 * p * p) / 4;
             }
             const long long c = cost[m / p] + (long long)((n / p + 31) / 32) * w + 20;
             if (c < cost[m] || (c == cost[m] && p > pick[m])) {
@@ -73,6 +74,7 @@ bool factor(int n, std::vector<int> &r) {
         }
     }
     if (cost[n] >= kInf) return false;
+    if (total_cost) *total_cost = cost[n];
     for (int m = n; m > 1; m /= pick[m]) r.push_back(pick[m]);
     std::stable_sort(r.begin(), r.end(), [](int x, int y) { return (x & 1) > (y & 1); });
     return true;
@@ -100,28 +102,32 @@ void stage_tables(int n, const std::vector<int> &r, int *radix, int *stride, flo
     }
 }
 
-// In-place radix-2 FFT in double (host), used only to precompute Bluestein kernels.
-void host_fft_pow2(std::vector<std::complex<double>> &a, int sign) {
-    const int n = int(a.size());
-    for (int i = 1, j = 0; i < n; i++) {
-        int bit = n >> 1;
-        for (; j & bit; bit >>= 1) j ^= bit;
-        j ^= bit;
-        if (i < j) std::swap(a[i], a[j]);
+// Mixed-radix DFT in double (host, decimation in time over the smallest prime factor), used only
+// to precompute Bluestein kernels: out[k] = sum_t in[t stride] exp(sign 2 pi i t k / m).
+void host_dft(const std::complex<double> *in, std::complex<double> *out, int m, int stride, int sign) {
+    if (m == 1) {
+        out[0] = in[0];
+        return;
     }
-    for (int len = 2; len <= n; len <<= 1) {
-        const double ang = sign * 2.0 * M_PI / len;
-        const std::complex<double> wl(std::cos(ang), std::sin(ang));
-        for (int i = 0; i < n; i += len) {
-            std::complex<double> w(1.0, 0.0);
-            for (int k = 0; k < len / 2; k++) {
-                const std::complex<double> u = a[i + k], v = a[i + k + len / 2] * w;
-                a[i + k] = u + v;
-                a[i + k + len / 2] = u - v;
-                w *= wl;
-            }
+    int p = 2;
+    while (m % p) p++;
+    const int q = m / p;
+    std::vector<std::complex<double>> sub(m);
+    for (int r = 0; r < p; r++) host_dft(in + r * stride, sub.data() + r * q, q, stride * p, sign);
+    for (int k = 0; k < m; k++) {
+        std::complex<double> acc = 0.0;
+        for (int r = 0; r < p; r++) {
+            const double a = sign * 2.0 * M_PI * double((long long)r * k % m) / double(m);
+            acc += sub[r * q + k % q] * std::complex<double>(std::cos(a), std::sin(a));
         }
+        out[k] = acc;
     }
+}
+
+bool smooth235(int m) {
+    for (int p : {2, 3, 5})
+        while (m % p == 0) m /= p;
+    return m == 1;
 }
 
 void table(std::vector<float2> &out, int n) {
@@ -144,17 +150,24 @@ const FftLen &fft_len(iqm_ctx *ctx, int n) {
     std::vector<int> r;
     std::vector<float2> tw, mtw, chirp, bf, bi, stw, mstw;
     table(tw, n);
-    if (factor(n, r)) {
+    // Direct plan, or Bluestein on the smallest 2,3,5-smooth m >= 2n-1 when that is estimated cheaper
+    // (two length-m transforms plus three pointwise passes).
+    long long direct_cost = 0, m_cost = 0;
+    const bool direct = factor(n, r, &direct_cost);
+    int m = 2 * n - 1;
+    while (!smooth235(m)) m++;
+    std::vector<int> rm;
+    factor(m, rm, &m_cost);
+    const long long blue_cost = 2 * m_cost + 3 * 12 * (long long)((m + 31) / 32);
+    if (direct && (n <= 2 || direct_cost <= blue_cost)) {
         L.bluestein = 0;
         L.nst = int(r.size());
         stage_tables(n, r, L.radix, L.stride, L.inv_stride, L.inv_q, L.stw_off, L.stw_len, stw);
     } else {
         L.bluestein = 1;
         L.nst = 0;
-        int m = 1;
-        while (m < 2 * n - 1) m <<= 1;
         L.m = m;
-        factor(m, r);
+        r = rm;
         L.mst = int(r.size());
         stage_tables(m, r, L.mradix, L.mstride, L.minv_stride, L.minv_q, L.mstw_off, L.mstw_len, mstw);
         table(mtw, m);
@@ -174,7 +187,9 @@ const FftLen &fft_len(iqm_ctx *ctx, int n) {
                 b[d] = v;
                 if (d) b[m - d] = v;
             }
-            host_fft_pow2(b, -1);
+            std::vector<std::complex<double>> bt(m);
+            host_dft(b.data(), bt.data(), m, 1, -1);
+            b.swap(bt);
             auto &dst = pass == 0 ? bf : bi;
             dst.resize(m);
             for (int k = 0; k < m; k++) dst[k] = make_float2(float(b[k].real() / m), float(b[k].imag() / m));

@@ -4,9 +4,10 @@
 // with sign -1 and no scaling, :378 inverse with sign +1 and normalize = 1/N).  Here a transform
 // of length n runs inside one CTA as a Stockham auto-sort FFT: log_p stages, each reading one
 // buffer and writing the other, so no bit reversal is needed.  n is factored into radices
-// computed in registers (2, 3, 4, 5, 6, 8, 9, 10, 12, 15) and other odd primes up to 61 (an O(p^2)
-// butterfly, read from the length's table); a length with a larger
-// prime factor is computed with Bluestein's chirp-z algorithm on a power-of-two length m >= 2n-1.
+// computed in registers (2, 3, 4, 5, 6, 8, 9, 10, 12, 15) and other odd primes up to 251 (a direct
+// O(p^2) butterfly, read from the length's table); when that is estimated dearer, or a prime factor
+// is larger, the length runs through Bluestein's chirp-z algorithm on the smallest 2,3,5-smooth
+// length m >= 2n-1.
 //
 // Stage s with radix p and stride L (the product of the earlier radices), butterfly j in [0, n/p):
 //   k = j mod L;  v_r = in[j + r n/p] * W^(r k),  W = exp(sign 2 pi i / (L p));
@@ -20,7 +21,7 @@
 namespace iqm {
 
 constexpr int FFT_MAX_STAGES = 16;
-constexpr int FFT_MAX_GENERIC = 61;  // largest prime handled by the direct butterfly
+constexpr int FFT_MAX_GENERIC = 251;  // largest prime the planner may give a direct butterfly
 
 // Device-visible description of one transform length.
 struct FftLen {
