@@ -113,6 +113,7 @@ __global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __g
     __syncthreads();
     // stage YCxCz of columns x0-R .. x0+HSEG+R-1 (clamped to the image), both images
     const int ncols = HSEG + 2 * R;
+#pragma unroll 4
     for (int q = threadIdx.x; q < 2 * ncols; q += HT) {
         const int img = q / ncols, c = q - img * ncols;
         const int x = min(max(x0 - R + c, 0), P.w - 1);
@@ -194,15 +195,26 @@ __global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __g
                 }
             }
         }
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const int x = x0 + xl + i;
-            if (x >= P.w) continue;
-            const long long p = (long long)y * P.w + x;
+        const long long p0 = (long long)y * P.w + x0 + xl;
+        if ((P.w & 3) == 0 && x0 + xl + 3 < P.w) {
+            // 4 consecutive pixels, 16-byte aligned (w, n, plane offsets and xl all multiples of 4)
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                planes[(long long)(img * 6 + c) * n + p] = fa[i][c];
-                planes[(long long)(img * 6 + 3 + c) * n + p] = ca[i][c];
+                *reinterpret_cast<float4 *>(planes + (long long)(img * 6 + c) * n + p0) =
+                    make_float4(fa[0][c], fa[1][c], fa[2][c], fa[3][c]);
+                *reinterpret_cast<float4 *>(planes + (long long)(img * 6 + 3 + c) * n + p0) =
+                    make_float4(ca[0][c], ca[1][c], ca[2][c], ca[3][c]);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int x = x0 + xl + i;
+                if (x >= P.w) continue;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    planes[(long long)(img * 6 + c) * n + p0 + i] = fa[i][c];
+                    planes[(long long)(img * 6 + 3 + c) * n + p0 + i] = ca[i][c];
+                }
             }
         }
     }

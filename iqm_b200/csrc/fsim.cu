@@ -217,6 +217,16 @@ struct FixedEngine {
         return FP::run(a, b, stw, s);
     }
 };
+// Transform length an engine is compiled for (0: any length).
+template <class E>
+struct engine_len {
+    static constexpr int value = 0;
+};
+template <class FP>
+struct engine_len<FixedEngine<FP>> {
+    static constexpr int value = FP::n;
+};
+
 using Engine270 = FixedEngine<iqm::FixedPlan<270, 9, 3, 10>>;
 using Engine480 = FixedEngine<iqm::FixedPlan<480, 15, 8, 4>>;
 
@@ -298,24 +308,50 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_cols_kernel(FsimGroup g, const
     float2 *Sl = sm + ((tl + 1) & ~1);     // cols x h2 spectrum slab (column-major)
     float2 *work = Sl + size_t(cols) * h2;  // per warp: a, b of NB x wl each
     const float2 *src = g.spec + size_t(g.pair0 * 2 + plane) * g.n;
+    const int nbw = min(NB, nc - warp * NB);
+    // With a fixed-length engine (h2 == PN) each lane holds its share of the warp's filter column in
+    // registers, and the next scale's share is loaded while this scale's transform runs.
+    constexpr int PN = engine_len<Eng>::value;
+    constexpr int PV = PN > 0 ? (PN + 31) / 32 : 1;
+    float hnext[PV];
+    auto load_filter = [&](int zz) {
+        const float *H = g.filters + size_t(zz) * g.n + size_t(x0 + warp) * h2;
+#pragma unroll
+        for (int i = 0; i < PV; i++) {
+            const int y = lane + 32 * i;
+            hnext[i] = (y < PN) ? __ldg(H + y) : 0.f;
+        }
+    };
+    if (PN > 0 && nbw > 0) load_filter(o * 4);
     for (int idx = threadIdx.x; idx < cols * h2; idx += blockDim.x) {
         const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
         if (c < nc) Sl[size_t(c) * h2 + y] = consts_mode ? make_float2(1.f, 0.f) : src[size_t(y) * g.w2 + x0 + c];
     }
     __syncthreads();
-    const int nbw = min(NB, nc - warp * NB);
     for (int s = 0; s < 4; s++) {
         const int z = o * 4 + s;
         if (nbw > 0) {
             float2 *a = warp_area(work, warp, wl);
-            for (int t = 0; t < nbw; t++) {
-                const int c = warp * NB + t;
-                const float *H = g.filters + size_t(z) * g.n + size_t(x0 + c) * h2;
-                const float2 *col = Sl + size_t(c) * h2;
+            const float2 *col = Sl + size_t(warp) * h2;  // NB == 1: column `warp` of the slab
+            if constexpr (PN > 0) {
+                float hcur[PV];
+#pragma unroll
+                for (int i = 0; i < PV; i++) hcur[i] = hnext[i];
+                if (s < 3) load_filter(z + 1);
+#pragma unroll
+                for (int i = 0; i < PV; i++) {
+                    const int y = lane + 32 * i;
+                    if (y < PN) {
+                        const float2 v = col[y];
+                        a[y] = make_float2(hcur[i] * v.x, hcur[i] * v.y);
+                    }
+                }
+            } else {
+                const float *H = g.filters + size_t(z) * g.n + size_t(x0 + warp) * h2;
                 for (int y = lane; y < h2; y += 32) {
                     const float hv = __ldg(H + y);
                     const float2 v = col[y];
-                    a[t * wl + y] = make_float2(hv * v.x, hv * v.y);
+                    a[y] = make_float2(hv * v.x, hv * v.y);
                 }
             }
             float2 *res = Eng::run(a, a + NB * wl, L, sm, 1.f, wl);
@@ -345,8 +381,8 @@ __device__ __forceinline__ void response_sums(const float2 v[4], float invN, flo
         sE += re[s];
         sO += im[s];
     }
-    const float xe = sqrtf(sE * sE + sO * sO) + 0.0001f;
-    const float mE = sE / xe, mO = sO / xe;
+    const float rxe = 1.0f / (sqrtf(sE * sE + sO * sO) + 0.0001f);
+    const float mE = sE * rxe, mO = sO * rxe;
     en = 0.f;
 #pragma unroll
     for (int s = 0; s < 4; s++) en += re[s] * mE + im[s] * mO - fabsf(re[s] * mO - im[s] * mE);
