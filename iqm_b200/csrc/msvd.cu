@@ -108,7 +108,9 @@ __device__ __forceinline__ void svd8_values(float c[8][8], float s[8]) {
                 for (int r = 0; r < 8; r++) p = fmaf(c[i][r], c[j][r], p);
                 const double pd = double(p);
                 if (pd * pd > eps2 * double(nrm[i]) * double(nrm[j])) {
-                    const float zeta = (nrm[j] - nrm[i]) / (2.0f * p);
+                    // |p| <= |ci||cj| < 2^20 here, so the fast quotient is accurate to a few ulp; the
+                    // angle only steers the sweep, later rotations remove what it leaves
+                    const float zeta = __fdividef(nrm[j] - nrm[i], 2.0f * p);
                     const float az = fabsf(zeta);
                     // tan(theta): smaller root of t^2 + 2 zeta t - 1 = 0 (1/(2 zeta) once zeta^2 overflows)
                     const float t = copysignf(1.0f, zeta) / (az < 1e18f ? az + sqrtf(fmaf(zeta, zeta, 1.0f)) : 2.0f * az);
