@@ -32,7 +32,7 @@
 namespace {
 
 constexpr int TW = 128;             // output columns per CTA (one vertical strip)
-constexpr int NT = 64;              // threads per CTA; each owns 2 adjacent columns
+constexpr int NT = TW;              // threads per CTA, one output column each
 constexpr int SMEM_COLS = TW + 16;  // staged columns x0-8 .. x0+TW+7 (16-byte aligned start)
 constexpr int NRAW = 8;             // raw RGBA row ring
 constexpr int PF = 6;               // rows prefetched ahead (< NRAW)
@@ -144,6 +144,8 @@ __device__ __forceinline__ void convert_row(Smem &sm, const SsimPairDev &P, int 
 }
 
 template <int R>
+// 8 CTAs of 128 threads per SM (at most 64 registers a thread): the row pipeline is latency-bound,
+// so resident warps matter more than registers per thread.
 __global__ void __launch_bounds__(NT, 8) ssim_kernel(SsimArgs args) {
     using G = Geom<R>;
     constexpr int K = G::K, S = G::S, ROWS = G::ROWS;
@@ -184,16 +186,15 @@ __global__ void __launch_bounds__(NT, 8) ssim_kernel(SsimArgs args) {
     issue_row(sm, P, x0, y0 - R + PF, PF % NRAW);
     cp_async_commit();
 
-    constexpr int OFF = (8 - R) & 1;     // parity fix so float4 reads stay 16-byte aligned
-    constexpr int NV = (2 * R + 4) / 2;  // float4 reads per row (2R+4 float2 values)
-    const int col0 = 2 * tid;            // first of this thread's two tile columns
-    const int start = col0 + 8 - R - OFF;
+    const int col0 = tid;                // this thread's tile column
+    const int start = col0 + 8 - R;      // staged index of its leftmost horizontal tap
     float gsum = 0.f;
 #pragma unroll
     for (int k = 0; k < K; k++) gsum += args.g[k];
-    float rwx[2];
+    constexpr int CPT = 1;
+    float rwx[CPT];
 #pragma unroll
-    for (int c = 0; c < 2; c++) {
+    for (int c = 0; c < CPT; c++) {
         const int x = x0 + col0 + c;
         float s = 0.f;
 #pragma unroll
@@ -204,10 +205,12 @@ __global__ void __launch_bounds__(NT, 8) ssim_kernel(SsimArgs args) {
         rwx[c] = 1.0f / s;
     }
 
-    float2 ring_m[2][K];  // (sum g u, sum g v) of the last K rows, per column
-    float2 ring_s[2][K];  // (sum g u^2, sum g v^2)
+    float2 ring_m[CPT][K];  // (sum g u, sum g v) of the last K rows, per column
+    float2 ring_s[CPT][K];  // (sum g u^2, sum g v^2)
     float acc = 0.f;      // pooled SSIM of this thread
-    const bool col_in[2] = {x0 + col0 < W, x0 + col0 + 1 < W};
+    bool col_in[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; c++) col_in[c] = x0 + col0 + c < W;
 
     for (int jb = 0; jb < ROWS; jb += K) {
 #pragma unroll
@@ -221,20 +224,15 @@ __global__ void __launch_bounds__(NT, 8) ssim_kernel(SsimArgs args) {
             cp_async_commit();
 
             // horizontal taps of row j
-            float2 v[2 * R + 4];
-            const float4 *src = reinterpret_cast<const float4 *>(sm.uv[j & 1] + start);
+            float2 v[K];
 #pragma unroll
-            for (int q = 0; q < NV; q++) {
-                const float4 f = src[q];
-                v[2 * q] = make_float2(f.x, f.y);
-                v[2 * q + 1] = make_float2(f.z, f.w);
-            }
+            for (int q = 0; q < K; q++) v[q] = sm.uv[j & 1][start + q];
 #pragma unroll
-            for (int c = 0; c < 2; c++) {
+            for (int c = 0; c < CPT; c++) {
                 float2 hm = make_float2(0.f, 0.f), hs = make_float2(0.f, 0.f);
 #pragma unroll
                 for (int k = 0; k < K; k++) {
-                    const float2 sv = v[OFF + c + k];
+                    const float2 sv = v[c + k];
                     const float2 gs = __fmul2_rn(make_float2(args.g[k], args.g[k]), sv);
                     hm = __fadd2_rn(hm, gs);
                     hs = __ffma2_rn(gs, sv, hs);
@@ -258,7 +256,7 @@ __global__ void __launch_bounds__(NT, 8) ssim_kernel(SsimArgs args) {
                     const float rwy = 1.0f / wy;
                     const bool pool_y = y >= R && y <= H - R;
 #pragma unroll
-                    for (int c = 0; c < 2; c++) {
+                    for (int c = 0; c < CPT; c++) {
                         float2 mm = make_float2(0.f, 0.f), ms = make_float2(0.f, 0.f);
 #pragma unroll
                         for (int k = 0; k < K; k++) {
