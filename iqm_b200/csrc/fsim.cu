@@ -170,19 +170,68 @@ __global__ void __launch_bounds__(FT) fsim_ingest_kernel(FsimGroup g) {
     for (int img = 0; img < 2; img++) {
         const uint8_t *base = img ? P.b : P.a;
         float sI = 0.f, sQ = 0.f, sY = 0.f;
+        auto add = [&](uint32_t px) {
+            const float r = u8f[px & 0xffu], gg = u8f[(px >> 8) & 0xffu], b = u8f[(px >> 16) & 0xffu];
+            sI += r * 0.596f - gg * 0.274f - b * 0.322f;
+            sQ += r * 0.211f - gg * 0.523f + b * 0.312f;
+            sY += r * 0.299f + gg * 0.587f + b * 0.114f;
+        };
+        if constexpr (FF == 4 || FF == 8) {
+            // the window's F pixels of a row start at byte 4F x - 2F: 8-byte aligned for F = 4,
+            // 16-byte aligned for F = 8 (given an aligned base and pitch); load rows as vectors
+            // when the whole row is inside the image, then sum in the shader's order
+            constexpr int V = FF == 4 ? 2 : 4;  // pixels per vector load
+            const bool vec = ((reinterpret_cast<uintptr_t>(base) | uintptr_t(P.pitch)) & (4 * V - 1)) == 0 &&
+                             xs >= 0 && xs + FF <= P.w;
+            uint32_t px[FF][FF];  // [kk][jj]
+            bool row_ok[FF];
 #pragma unroll
-        for (int jj = 0; jj < F; jj++) {  // x outer, y inner, as fsim_downsample.glsl:46-52
-            const int j = xs + jj;
-            if (j < 0 || j >= P.w) continue;
-#pragma unroll
-            for (int kk = 0; kk < F; kk++) {
+            for (int kk = 0; kk < FF; kk++) {
                 const int k = ys + kk;
-                if (k < 0 || k >= P.h) continue;
-                const uint32_t px = __ldg(reinterpret_cast<const uint32_t *>(base + (long long)k * P.pitch) + j);
-                const float r = u8f[px & 0xffu], gg = u8f[(px >> 8) & 0xffu], b = u8f[(px >> 16) & 0xffu];
-                sI += r * 0.596f - gg * 0.274f - b * 0.322f;
-                sQ += r * 0.211f - gg * 0.523f + b * 0.312f;
-                sY += r * 0.299f + gg * 0.587f + b * 0.114f;
+                row_ok[kk] = k >= 0 && k < P.h;
+                const uint32_t *row = reinterpret_cast<const uint32_t *>(base + (long long)min(max(k, 0), P.h - 1) * P.pitch);
+                if (vec) {
+#pragma unroll
+                    for (int q = 0; q < FF / V; q++) {
+                        if constexpr (V == 2) {
+                            const uint2 t = __ldg(reinterpret_cast<const uint2 *>(row + xs) + q);
+                            px[kk][2 * q] = t.x;
+                            px[kk][2 * q + 1] = t.y;
+                        } else {
+                            const uint4 t = __ldg(reinterpret_cast<const uint4 *>(row + xs) + q);
+                            px[kk][4 * q] = t.x;
+                            px[kk][4 * q + 1] = t.y;
+                            px[kk][4 * q + 2] = t.z;
+                            px[kk][4 * q + 3] = t.w;
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int jj = 0; jj < FF; jj++) {
+                        const int j = xs + jj;
+                        px[kk][jj] = (j >= 0 && j < P.w) ? __ldg(row + j) : 0u;
+                    }
+                }
+            }
+#pragma unroll
+            for (int jj = 0; jj < FF; jj++) {  // x outer, y inner, as fsim_downsample.glsl:46-52
+                const int j = xs + jj;
+                if (j < 0 || j >= P.w) continue;
+#pragma unroll
+                for (int kk = 0; kk < FF; kk++)
+                    if (row_ok[kk]) add(px[kk][jj]);
+            }
+        } else {
+#pragma unroll
+            for (int jj = 0; jj < F; jj++) {  // x outer, y inner, as fsim_downsample.glsl:46-52
+                const int j = xs + jj;
+                if (j < 0 || j >= P.w) continue;
+#pragma unroll
+                for (int kk = 0; kk < F; kk++) {
+                    const int k = ys + kk;
+                    if (k < 0 || k >= P.h) continue;
+                    add(__ldg(reinterpret_cast<const uint32_t *>(base + (long long)k * P.pitch) + j));
+                }
             }
         }
         float *dst = g.yiq + size_t(pi * 2 + img) * 3 * g.n;
