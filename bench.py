@@ -47,14 +47,14 @@ WORKLOADS = {
 # kernel from an ncu capture of this benchmark, with the pairs that launch processed; the summaries
 # under profiles/ give the commands.  Scaled by pairs per launch when the live launch differs.
 TRAFFIC = {
-    # ssim_kernel, 32 pairs: 566,863,104 B read + 3,258,624 B written (profiles/ssim_kernel_1080p.md)
-    "ssim": {"kernel": "ssim_kernel", "bytes_per_launch": 570121728, "pairs_per_launch": 32},
-    # fsim_inv_cols_kernel, one chunk of 2 pairs: 12,486,144 + 13,263,360 B (profiles/fsim_inv_cols_kernel_1080p.md)
-    "fsim": {"kernel": "fsim_inv_cols_kernel", "bytes_per_launch": 25749504, "pairs_per_launch": 2},
-    # flip_vcols_kernel, 16 pairs: 1,642,060,544 + 11,937,024 B (profiles/flip_vcols_kernel_1080p.md)
-    "flip": {"kernel": "flip_vcols_kernel", "bytes_per_launch": 1653997568, "pairs_per_launch": 16},
-    # msvd_block_kernel, 32 pairs: 527,325,440 + 6,860,288 B (profiles/msvd_block_kernel_1080p.md)
-    "msvd": {"kernel": "msvd_block_kernel", "bytes_per_launch": 534185728, "pairs_per_launch": 32},
+    # ssim_kernel, 32 pairs: 567,952,640 B read + 3,802,880 B written (profiles/ssim_kernel_1080p.md)
+    "ssim": {"kernel": "ssim_kernel", "bytes_per_launch": 571755520, "pairs_per_launch": 32},
+    # fsim_inv_cols_kernel, one chunk of 2 pairs: 12,485,632 + 13,392,896 B (profiles/fsim_inv_cols_kernel_1080p.md)
+    "fsim": {"kernel": "fsim_inv_cols_kernel", "bytes_per_launch": 25878528, "pairs_per_launch": 2},
+    # flip_vcols_kernel, 16 pairs: 1,640,862,720 + 11,914,240 B (profiles/flip_vcols_kernel_1080p.md)
+    "flip": {"kernel": "flip_vcols_kernel", "bytes_per_launch": 1652776960, "pairs_per_launch": 16},
+    # msvd_block_kernel, 32 pairs: 527,183,360 + 6,785,792 B (profiles/msvd_block_kernel_1080p.md)
+    "msvd": {"kernel": "msvd_block_kernel", "bytes_per_launch": 533969152, "pairs_per_launch": 32},
 }
 
 
