@@ -47,8 +47,8 @@ WORKLOADS = {
 # kernel from an ncu capture of this benchmark, with the pairs that launch processed; the summaries
 # under profiles/ give the commands.  Scaled by pairs per launch when the live launch differs.
 TRAFFIC = {
-    # ssim_kernel, 32 pairs: 567,952,640 B read + 3,802,880 B written (profiles/ssim_kernel_1080p.md)
-    "ssim": {"kernel": "ssim_kernel", "bytes_per_launch": 571755520, "pairs_per_launch": 32},
+    # ssim_kernel, 32 pairs: 568,007,424 B read + 3,266,560 B written (profiles/ssim_kernel_1080p.md)
+    "ssim": {"kernel": "ssim_kernel", "bytes_per_launch": 571273984, "pairs_per_launch": 32},
     # fsim_inv_cols_kernel, one chunk of 2 pairs: 12,485,632 + 13,392,896 B (profiles/fsim_inv_cols_kernel_1080p.md)
     "fsim": {"kernel": "fsim_inv_cols_kernel", "bytes_per_launch": 25878528, "pairs_per_launch": 2},
     # flip_vcols_kernel, 16 pairs: 1,640,862,720 + 11,914,240 B (profiles/flip_vcols_kernel_1080p.md)
