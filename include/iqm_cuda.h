@@ -170,6 +170,11 @@ int iqm_set_kernel_timing(iqm_ctx *ctx, int enable);
  * into buf (NUL-terminated); IQM_EINVAL if cap is too small. */
 int iqm_kernel_times(iqm_ctx *ctx, char *buf, size_t cap);
 
+/* Page-locked host memory for staging images (the reference keeps images in pageable vectors,
+ * src/input_image.h): copies from it run at full host-link speed and overlap with other work. */
+int iqm_host_alloc(size_t bytes, void **out);
+int iqm_host_free(void *p);
+
 /* ---- batches over several metrics ------------------------------------------------------------
  * The reference evaluates one pair with one metric per invocation (src/main.cpp:271-286, the method
  * chosen by IQM::Method, src/methods.h:13-19); these run many pairs through several metrics at once.

@@ -35,7 +35,7 @@ EXPORTS = (
     "iqm_fsim_dev", "iqm_ssim_batch", "iqm_msvd_batch", "iqm_flip_batch", "iqm_fsim_batch",
     "iqm_last_launch_count", "iqm_fsim_plan_constants", "iqm_ssim_noalloc", "iqm_set_kernel_timing",
     "iqm_kernel_times", "iqm_batch", "iqm_batch_plan_create", "iqm_batch_plan_run", "iqm_batch_plan_info",
-    "iqm_batch_plan_destroy",
+    "iqm_batch_plan_destroy", "iqm_host_alloc", "iqm_host_free",
 )
 
 METRIC_SSIM, METRIC_FSIM, METRIC_FLIP, METRIC_MSVD = 1, 2, 4, 8
@@ -113,6 +113,8 @@ def load_library(path=LIB_PATH):
     L.iqm_batch_plan_run.argtypes = [vp]
     L.iqm_batch_plan_info.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ip)]
     L.iqm_batch_plan_destroy.argtypes = [vp]
+    L.iqm_host_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(vp)]
+    L.iqm_host_free.argtypes = [vp]
     _lib = L
     return L
 

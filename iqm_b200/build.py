@@ -35,7 +35,8 @@ def stale():
     return any(os.path.getmtime(f) > t for f in sources() + headers())
 
 
-HOST_SRC = ["methods.cpp", "args.cpp", "png_io.cpp", "iqm_cuda.cpp", "main.cpp"]
+HOST_SRC = ["methods.cpp", "args.cpp", "png_io.cpp", "iqm_cuda.cpp", "batch_pipeline.cpp", "main.cpp"]
+CUDA_INC = os.path.join(os.path.dirname(os.path.dirname(NVCC)), "include")  # NVTX3 (header-only)
 CLI = os.path.join(HERE, "bin", "IQM")
 CXX = os.environ.get("IQM_CXX", "/usr/bin/g++")
 
@@ -47,8 +48,8 @@ def build_cli(force=False, verbose=False):
     if not force and os.path.exists(CLI) and all(os.path.getmtime(f) <= os.path.getmtime(CLI) for f in deps):
         return CLI
     os.makedirs(os.path.dirname(CLI), exist_ok=True)
-    cmd = [CXX, "-O2", "-std=c++20", "-Wall", "-I", os.path.join(ROOT, "include"), "-o", CLI] + srcs + [
-        "-L", HERE, "-liqm_cuda", "-lz", "-Wl,-rpath,$ORIGIN/.."]
+    cmd = [CXX, "-O2", "-std=c++20", "-Wall", "-I", os.path.join(ROOT, "include"), "-I", CUDA_INC, "-o", CLI] + srcs + [
+        "-L", HERE, "-liqm_cuda", "-lz", "-ldl", "-pthread", "-Wl,-rpath,$ORIGIN/.."]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -102,6 +102,23 @@ extern "C" __attribute__((visibility("default"))) int iqm_device_name(iqm_ctx *c
 
 extern "C" __attribute__((visibility("default"))) int iqm_last_launch_count(const iqm_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
+extern "C" __attribute__((visibility("default"))) int iqm_host_alloc(size_t bytes, void **out) {
+    if (!out) return IQM_EINVAL;
+    *out = nullptr;
+    if (bytes == 0) return IQM_EINVAL;
+    if (cudaMallocHost(out, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return IQM_ENOMEM;
+    }
+    return IQM_OK;
+}
+
+extern "C" __attribute__((visibility("default"))) int iqm_host_free(void *p) {
+    if (!p) return IQM_OK;
+    return cudaFreeHost(p) == cudaSuccess ? IQM_OK : IQM_ECUDA;
+}
+
 namespace iqm {
 
 void *upload_bytes(iqm_ctx *ctx, DevBuf &dst, const void *src, size_t bytes) {

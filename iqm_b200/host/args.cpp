@@ -47,6 +47,7 @@ IQM::Args::Args(const unsigned argc, const char *argv[]) {
         if (std::strcmp(a, "-v") == 0) verbose = true;
     }
     if (!have_method) throw std::runtime_error("missing method");
-    if (!have_input) throw std::runtime_error("missing input");
-    if (!have_ref) throw std::runtime_error("missing reference");
+    const bool batch = options.count("--batch") != 0;  // pairs come from the list file
+    if (!have_input && !batch) throw std::runtime_error("missing input");
+    if (!have_ref && !batch) throw std::runtime_error("missing reference");
 }

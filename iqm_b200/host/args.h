@@ -1,7 +1,9 @@
 // Command-line arguments with the reference's rules (src/args.h:15-24, src/args.cpp:9-61):
 // `--method M --input A --ref B [--output P] [-v]`; every other `KEY VALUE` pair is kept in
-// `options` (FLIP reads FLIP_WIDTH, FLIP_RES, FLIP_DISTANCE from there).  A missing method, input
-// or reference, or an unknown method name, throws std::runtime_error.
+// `options` (FLIP reads FLIP_WIDTH, FLIP_RES, FLIP_DISTANCE from there; the batch and repeat modes
+// of this front end read --batch, --chunk, --threads, --repeat).  A missing method, input or
+// reference (input and reference are not needed with --batch), or an unknown method name, throws
+// std::runtime_error.
 #ifndef IQM_HOST_ARGS_H
 #define IQM_HOST_ARGS_H
 

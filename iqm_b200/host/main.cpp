@@ -2,13 +2,23 @@
 //   IQM --method {SSIM,SVD,FSIM,FLIP,CW_SSIM_CPU} --input A --ref B [--output P] [-v] [KEY VALUE]...
 // Prints "MSSIM: x", "M-SVD: x", "FSIM: x\nFSIMc: y" like the reference, and "FLIP: x" (the
 // reference computes the FLIP map but prints no score).  Errors go to stderr with exit code -1.
+// Two additions for throughput work:
+//   --repeat N   evaluate the pair N times (headless stand-in for the reference's windowed profile
+//                loop, src/profile.cpp:227-283), each iteration inside an NVTX range
+//                "IQM <method> <i>" for Nsight Systems; with -v, per-iteration times to stdout;
+//   --batch LIST evaluate every pair of a list file (batch_pipeline.h).
 #include <chrono>
 #include <iostream>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
+#include <algorithm>
+
 #include "args.h"
+#include "batch_pipeline.h"
 #include "iqm_cuda.hpp"
 #include "png_io.h"
 
@@ -30,6 +40,37 @@ void load_pair(const IQM::Args &args, InputImage &input, InputImage &ref) {
         throw std::runtime_error("Compared images must have the same size");
 }
 
+int repeat_count(const IQM::Args &args) {
+    auto it = args.options.find("--repeat");
+    if (it == args.options.end()) return 1;
+    const int n = std::stoi(it->second);
+    if (n < 1) throw std::runtime_error("--repeat must be >= 1");
+    return n;
+}
+
+// Runs `compute` --repeat times, each in an NVTX range; returns the last result.
+template <class F>
+auto repeated(const IQM::Args &args, F &&compute) {
+    const int n = repeat_count(args);
+    std::vector<double> ms;
+    decltype(compute()) result = {};
+    for (int i = 0; i < n; i++) {
+        const std::string range = std::string("IQM ") + IQM::method_name(args.method) + " " + std::to_string(i);
+        nvtxRangePushA(range.c_str());
+        const auto t0 = clk::now();
+        result = compute();
+        ms.push_back(std::chrono::duration<double, std::milli>(clk::now() - t0).count());
+        nvtxRangePop();
+    }
+    if (n > 1 && args.verbose) {
+        std::vector<double> s = ms;
+        std::sort(s.begin(), s.end());
+        std::cout << "Iterations: " << n << ", min " << s.front() << " ms, median " << s[s.size() / 2]
+                  << " ms, max " << s.back() << " ms" << std::endl;
+    }
+    return result;
+}
+
 void save_map(const IQM::Args &args, unsigned w, unsigned h, const std::vector<float> &map) {
     if (!args.outputPath.has_value()) return;
     if (!IQM::write_grey_png(args.outputPath.value(), int(w), int(h), convertFloatToChar(map)))
@@ -43,7 +84,7 @@ void ssim(const IQM::Args &args) {
     if (args.verbose) std::cout << "Selected device: " << rt.selectedDevice << std::endl;
     IQM::CUDA::SSIM metric(rt);
     const auto start = clk::now();
-    auto result = metric.computeMetric(rt, input, ref);
+    auto result = repeated(args, [&] { return metric.computeMetric(rt, input, ref); });
     const auto end = clk::now();
     std::cout << "MSSIM: " << result.mssim << std::endl;
     if (args.verbose) result.timestamps.print(start, end);
@@ -57,7 +98,7 @@ void svd(const IQM::Args &args) {
     IQM::CUDA::SVD metric(rt);
     if (args.verbose) std::cout << "Selected device: " << rt.selectedDevice << std::endl;
     const auto start = clk::now();
-    auto result = metric.computeMetric(rt, input, ref);
+    auto result = repeated(args, [&] { return metric.computeMetric(rt, input, ref); });
     const auto end = clk::now();
     std::cout << "M-SVD: " << result.msvd << std::endl;
     if (args.verbose) result.timestamps.print(start, end);
@@ -71,7 +112,7 @@ void fsim(const IQM::Args &args) {
     IQM::CUDA::FSIM metric(rt);
     if (args.verbose) std::cout << "Selected device: " << rt.selectedDevice << std::endl;
     const auto start = clk::now();
-    auto result = metric.computeMetric(rt, input, ref);
+    auto result = repeated(args, [&] { return metric.computeMetric(rt, input, ref); });
     const auto end = clk::now();
     std::cout << "FSIM: " << result.fsim << std::endl << "FSIMc: " << result.fsimc << std::endl;
     if (args.verbose) result.timestamps.print(start, end);
@@ -93,7 +134,7 @@ void flip(const IQM::Args &args) {
                   << "FLIP monitor width: " << flip_args.monitor_width << std::endl;
     }
     const auto start = clk::now();
-    auto result = metric.computeMetric(rt, input, ref, flip_args);
+    auto result = repeated(args, [&] { return metric.computeMetric(rt, input, ref, flip_args); });
     const auto end = clk::now();
     std::cout << "FLIP: " << result.mean_flip << std::endl;
     if (args.verbose) result.timestamps.print(start, end);
@@ -105,6 +146,7 @@ int main(int argc, const char **argv) {
     auto args = IQM::Args(argc, argv);
     if (args.verbose) std::cout << "Selected method: " << IQM::method_name(args.method) << std::endl;
     try {
+        if (args.options.count("--batch")) return IQM::run_batch(args);
         switch (args.method) {
             case IQM::Method::SSIM: ssim(args); break;
             case IQM::Method::CW_SSIM_CPU: break;  // the reference's CW-SSIM is an empty stub

@@ -112,3 +112,21 @@ def test_cli_cw_ssim_is_a_no_op(cli, tmp_path):
     r = subprocess.run([cli, "--method", "CW_SSIM_CPU", "--input", "a", "--ref", "b", "-v"], capture_output=True,
                        text=True)
     assert r.returncode == 0 and r.stdout.strip() == "Selected method: CW-SSIM"
+
+
+def test_cli_batch_list_errors(cli, tmp_path):
+    # batch mode needs no --input/--ref, but a readable list of "<input> <ref>" lines
+    r = subprocess.run([cli, "--method", "SSIM", "--batch", str(tmp_path / "missing.txt")], capture_output=True,
+                       text=True)
+    assert r.returncode == 255 and "Failed to open batch list" in r.stderr
+    bad = tmp_path / "bad.txt"
+    bad.write_text("# comment\n\nonly_one_path.png\n")
+    r = subprocess.run([cli, "--method", "SSIM", "--batch", str(bad)], capture_output=True, text=True)
+    assert r.returncode == 255 and "without a reference image" in r.stderr
+    ok = tmp_path / "ok.txt"
+    ok.write_text("a.png b.png\n")
+    r = subprocess.run([cli, "--method", "SSIM", "--batch", str(ok), "--chunk", "0"], capture_output=True, text=True)
+    assert r.returncode == 255 and "--chunk must be >= 1" in r.stderr
+    # CW-SSIM stays a no-op in batch mode (no device needed)
+    r = subprocess.run([cli, "--method", "CW_SSIM_CPU", "--batch", str(ok)], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout == ""

@@ -60,3 +60,44 @@ def test_cli_scores_match_api(cli, rt, tmp_path):
     fl = iqm_b200.FLIP(rt).compute_metric(a, b, iqm_b200.FLIPArguments(3840.0, 0.7, 0.7))
     assert value(out, "FLIP") == pytest.approx(fl.mean_flip, rel=2e-6)
     assert "Selected method: FLIP" in out and "FLIP monitor resolution: 3840" in out and "TOTAL" in out
+
+
+def test_cli_batch_mode_matches_api(cli, rt, tmp_path):
+    """--batch: decode on worker threads into page-locked buffers, one batch call per chunk; every
+    pair's line matches the single-pair API; unreadable or mismatched pairs get an error line and the
+    rest are still evaluated."""
+    sizes = [(96, 130), (64, 64), (121, 77), (200, 150), (96, 130)]
+    lines, want = [], []
+    for i, (h, w) in enumerate(sizes):
+        a, b = synth.rgb_gain_pair(h, w, config=1, pair=i)
+        pa, pb = save(tmp_path, "a%d.png" % i, a), save(tmp_path, "b%d.png" % i, b)
+        lines.append("%s %s" % (pa, pb))
+        want.append(iqm_b200.FSIM(rt).compute_metric(a, b))
+    c, d = synth.rgb_gain_pair(40, 50, config=1, pair=9)
+    pc, pd = save(tmp_path, "c.png", c), save(tmp_path, "d.png", d[:, :48].copy())
+    lines.insert(2, "%s %s" % (pc, pd))                       # size mismatch
+    lines.insert(4, "%s %s" % (str(tmp_path / "nope.png"), pc))  # unreadable
+    lst = tmp_path / "list.txt"
+    lst.write_text("# pairs\n" + "\n".join(lines) + "\n")
+    r = subprocess.run([cli, "--method", "FSIM", "--batch", str(lst), "--chunk", "2", "--threads", "3", "-v"],
+                       capture_output=True, text=True)
+    assert r.returncode == 1, r.stderr
+    out = r.stdout.splitlines()
+    assert len(out) == len(lines)
+    assert "error: Compared images must have the same size" in out[2]
+    assert "error: Failed to load image" in out[4]
+    good = [l for k, l in enumerate(out) if k not in (2, 4)]
+    for l, f in zip(good, want):
+        parts = l.split()
+        assert parts[2] == "FSIM:" and parts[4] == "FSIMc:"
+        assert float(parts[3]) == pytest.approx(f.fsim, rel=2e-6)
+        assert float(parts[5]) == pytest.approx(f.fsimc, rel=2e-6)
+    assert "batch: 7 pairs, 2 failed" in r.stderr
+
+
+def test_cli_repeat_loop(cli, rt, tmp_path):
+    a, b = synth.grey_pair(90, 110, config=0, pair=2)
+    pa, pb = save(tmp_path, "a.png", a), save(tmp_path, "b.png", b)
+    out = run(cli, "--method", "SSIM", "--input", pa, "--ref", pb, "--repeat", "4", "-v")
+    assert "Iterations: 4" in out
+    assert value(out, "MSSIM") == pytest.approx(iqm_b200.SSIM(rt).compute_metric(a, b).mssim, rel=2e-6)
