@@ -343,7 +343,9 @@ __global__ void __launch_bounds__(FT, 1) fsim_fwd_cols_kernel(FsimGroup g, const
 // spectrum x H[o*4+s] (fsim_filter_combinations.glsl:53-56), sign +1.  consts_mode uses a
 // spectrum of ones, i.e. transforms the filters themselves (block 0 of the reference's buffer).
 template <class Eng>
-__global__ void __launch_bounds__(FT, 1) fsim_inv_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int lw, int consts_mode) {
+// Compiled-length engines: 4 CTAs per SM (64 registers; with the largest shared-memory carveout the
+// work buffers of 4 CTAs fit).  The runtime-planned engine needs more registers.
+__global__ void __launch_bounds__(FT, engine_len<Eng>::value ? 4 : 1) fsim_inv_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int lw, int consts_mode) {
     extern __shared__ float2 sm[];
     __shared__ int parity;
     const int tl = iqm::stage_twiddle_len(L);
@@ -768,12 +770,17 @@ constexpr int kFsimStreams = 8;  // plane-size groups in flight at once
 void set_smem(const void *fn, size_t bytes) {
     static std::mutex mu;
     static std::map<const void *, size_t> current;
-    if (bytes <= 48 * 1024) return;
     std::lock_guard<std::mutex> lock(mu);
-    size_t &cur = current[fn];
-    if (bytes <= cur) return;
+    auto it = current.find(fn);
+    if (it == current.end()) {
+        // transform CTAs are shared-memory bound: ask for the largest shared-memory carveout so
+        // as many CTAs fit per SM as registers allow
+        IQM_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        it = current.emplace(fn, 0).first;
+    }
+    if (bytes <= 48 * 1024 || bytes <= it->second) return;
     IQM_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
-    cur = bytes;
+    it->second = bytes;
 }
 
 // Launch shapes of the transform kernels for one plane size.

@@ -82,7 +82,7 @@ def test_cli_batch_mode_matches_api(cli, rt, tmp_path):
     r = subprocess.run([cli, "--method", "FSIM", "--batch", str(lst), "--chunk", "2", "--threads", "3", "-v"],
                        capture_output=True, text=True)
     assert r.returncode == 1, r.stderr
-    out = r.stdout.splitlines()
+    out = [l for l in r.stdout.splitlines() if not l.startswith("Selected method:")]  # -v header line
     assert len(out) == len(lines)
     assert "error: Compared images must have the same size" in out[2]
     assert "error: Failed to load image" in out[4]
