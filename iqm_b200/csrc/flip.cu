@@ -426,6 +426,8 @@ __global__ void __launch_bounds__(VT) flip_vpass_kernel(FlipArgs args, const __g
 constexpr int CW_ROLES = 14;         // per image: dx*g, value*edge, ddx*g, value*point, Y*csf0, Cx*csf1, Cz*csf2
 constexpr int CW_T = 32 * CW_ROLES;  // 448 threads
 constexpr int CW_BLOCKS = 10;        // K-row blocks per CTA
+constexpr int CW_GROUP = 2;          // blocks filtered before each pixel phase (2 x 21 x 32 = 3 pixels a thread)
+static_assert(CW_BLOCKS % CW_GROUP == 0, "a CTA's blocks split into whole groups");
 
 __host__ __device__ constexpr int cw_rows(int rf, int rc) { return CW_BLOCKS * (2 * (rf > rc ? rf : rc) + 1); }
 
@@ -452,7 +454,7 @@ __global__ void __launch_bounds__(CW_T, 2) flip_vcols_kernel(FlipArgs args, cons
     constexpr int R = RF > RC ? RF : RC;
     constexpr int K = 2 * R + 1;
     constexpr int SEG = cw_rows(RF, RC);
-    __shared__ float buf[K][CW_ROLES][32];
+    extern __shared__ float cw_buf[];  // [CW_GROUP * K rows][CW_ROLES][32 columns]
     __shared__ double red[CW_T / 32];
     __shared__ int is_last;
     const int gt = blockIdx.x;
@@ -472,28 +474,33 @@ __global__ void __launch_bounds__(CW_T, 2) flip_vcols_kernel(FlipArgs args, cons
     float win[K];
 #pragma unroll
     for (int t = 0; t < K - 1; t++) win[t] = __ldg(col + size_t(min(max(y0 - R + t, 0), P.h - 1)) * size_t(P.w));
-    float *out = &buf[0][role][lane];
+    float *out = cw_buf + role * 32 + lane;
     double dsum = 0.0;
-    for (int b = 0; b < CW_BLOCKS; b++) {
-        const int yb = y0 + b * K;
-        if (yb >= P.h) break;  // uniform over the CTA
-        float taps[K];  // reloaded per block so they are not live across the pixel phase
+    for (int b = 0; b < CW_BLOCKS; b += CW_GROUP) {
+        const int yg = y0 + b * K;
+        if (yg >= P.h) break;  // uniform over the CTA
+        for (int bb = 0; bb < CW_GROUP; bb++) {
+            const int yb = yg + bb * K;
+            if (yb >= P.h) break;  // uniform; rows past the image are skipped by the pixel phase
+            float taps[K];  // reloaded per block so they are not live across the pixel phase
 #pragma unroll
-        for (int u = 0; u < K; u++) {
-            const int k = R - u;
-            taps[u] = (k >= -rad && k <= rad) ? tap_src[k + rad] : 0.f;
+            for (int u = 0; u < K; u++) {
+                const int k = R - u;
+                taps[u] = (k >= -rad && k <= rad) ? tap_src[k + rad] : 0.f;
+            }
+            cw_block<K>(win, taps, col, P.w, P.h, yb - R, out + bb * K * CW_ROLES * 32);
         }
-        cw_block<K>(win, taps, col, P.w, P.h, yb - R, out);
         __syncthreads();
-        for (int p = threadIdx.x; p < K * 32; p += CW_T) {
+        for (int p = threadIdx.x; p < CW_GROUP * K * 32; p += CW_T) {
             const int j = p >> 5, c = p & 31;
-            const int y = yb + j, x = x0 + c;
+            const int y = yg + j, x = x0 + c;
             if (y >= P.h || x >= P.w) continue;
             float v[2][7];
+            const float *px = cw_buf + j * CW_ROLES * 32 + c;
 #pragma unroll
             for (int mm = 0; mm < 2; mm++)
 #pragma unroll
-                for (int q = 0; q < 7; q++) v[mm][q] = buf[j][mm * 7 + q][c];
+                for (int q = 0; q < 7; q++) v[mm][q] = px[(mm * 7 + q) * 32];
             const float val = flip_pixel(T, v);
             if (P.map) P.map[size_t(y) * size_t(P.w) + x] = val;
             dsum += double(val);
@@ -652,15 +659,23 @@ void flip_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_fl
     iqm::timing_mark(ctx, nullptr);
     const int R = std::max(T.rf, T.rc);
     const size_t smem = sizeof(float) * NPLANE * (VT_ROWS + 2 * R) * VT_COLS;
+    // dynamic shared memory of the column walkers: CW_GROUP blocks of K rows x 14 roles x 32 columns
+    auto cw_smem = [](int rf, int rc) { return sizeof(float) * CW_GROUP * (2 * std::max(rf, rc) + 1) * CW_ROLES * 32; };
     if (fixed == 1) {  // default monitor, 52.1 ppd
         flip_hpass_kernel<7, 8><<<unsigned(segs), HT, 0, ctx->stream>>>(a, T);
         iqm::check_launch(ctx, "flip_hpass_kernel");
-        flip_vcols_kernel<7, 8><<<tiles, CW_T, 0, ctx->stream>>>(a, T);
+        const size_t sm = cw_smem(7, 8);
+        IQM_CHECK_CUDA(cudaFuncSetAttribute((const void *)flip_vcols_kernel<7, 8>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+        flip_vcols_kernel<7, 8><<<tiles, CW_T, sm, ctx->stream>>>(a, T);
         iqm::check_launch(ctx, "flip_vcols_kernel");
     } else if (fixed == 2) {  // 67 ppd
         flip_hpass_kernel<9, 10><<<unsigned(segs), HT, 0, ctx->stream>>>(a, T);
         iqm::check_launch(ctx, "flip_hpass_kernel");
-        flip_vcols_kernel<9, 10><<<tiles, CW_T, 0, ctx->stream>>>(a, T);
+        const size_t sm = cw_smem(9, 10);
+        IQM_CHECK_CUDA(cudaFuncSetAttribute((const void *)flip_vcols_kernel<9, 10>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+        flip_vcols_kernel<9, 10><<<tiles, CW_T, sm, ctx->stream>>>(a, T);
         iqm::check_launch(ctx, "flip_vcols_kernel");
     } else {
         flip_hpass_kernel<0, 0><<<unsigned(segs), HT, 0, ctx->stream>>>(a, T);
