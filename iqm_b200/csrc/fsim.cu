@@ -283,7 +283,7 @@ using Engine480 = FixedEngine<iqm::FixedPlan<480, 15, 8, 4>>;
 // NB rows per warp.
 template <class Eng>
 __global__ void __launch_bounds__(FT, 1) fsim_fwd_rows_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl) {
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(16) float2 sm[];
     const int tl = iqm::stage_twiddle_len(L);
     iqm::stage_twiddles_to_shared(L, sm);
     __syncthreads();
@@ -309,7 +309,7 @@ __device__ __forceinline__ int slab_parity(float2 *res, float2 *a) { return res 
 
 template <class Eng>
 __global__ void __launch_bounds__(FT, 1) fsim_fwd_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int lw) {
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(16) float2 sm[];
     __shared__ int parity;
     const int tl = iqm::stage_twiddle_len(L);
     iqm::stage_twiddles_to_shared(L, sm);
@@ -346,7 +346,7 @@ template <class Eng>
 // Compiled-length engines: 4 CTAs per SM (64 registers; with the largest shared-memory carveout the
 // work buffers of 4 CTAs fit).  The runtime-planned engine needs more registers.
 __global__ void __launch_bounds__(FT, engine_len<Eng>::value ? 4 : 1) fsim_inv_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int lw, int consts_mode) {
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(16) float2 sm[];
     __shared__ int parity;
     const int tl = iqm::stage_twiddle_len(L);
     iqm::stage_twiddles_to_shared(L, sm);
@@ -446,7 +446,7 @@ __device__ __forceinline__ void response_sums(const float2 v[4], float invN, flo
 template <class Eng>
 __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int rr, int consts_mode,
                                                               double *rowsums) {
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(16) float2 sm[];
     __shared__ int parity;
     __shared__ double red[4][FT / 32];
     const int tl = iqm::stage_twiddle_len(L);
@@ -477,7 +477,39 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_kernel(FsimGroup g, const
         return warp_area(work, rl * WPR + s / NB, wl)[parity * NB * wl + (s % NB) * wl + x];
     };
     const float invN = 1.0f / float(g.n);
-    if (!consts_mode) {
+    if (!consts_mode && (w2 & 3) == 0 && rr <= 2) {
+        // 4 consecutive pixels a thread: 16-byte reads of each scale's result, 16-byte stores (rows
+        // of w2 % 4 == 0 pixels keep every quad aligned: plane sizes and row offsets are multiples of 4)
+        const int gp = g.pair0 * 2 + plane;
+        const int qpr = w2 >> 2;  // quads per row
+        for (int idx = threadIdx.x; idx < rr * qpr; idx += blockDim.x) {
+            const int rl = idx >= qpr ? 1 : 0;
+            const int x = (idx - rl * qpr) * 4;
+            const int y = y0 + rl;
+            if (y >= g.h2) continue;
+            float4 oa, oe, o0;
+            float *pa = &oa.x, *pe = &oe.x, *p0 = &o0.x;
+            float2 v[4][4];  // [scale][pixel]
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const float4 *src4 = reinterpret_cast<const float4 *>(&warp_area(work, rl * WPR + q / NB, wl)[parity * NB * wl + (q % NB) * wl + x]);
+                const float4 lo = src4[0], hi = src4[1];
+                v[q][0] = make_float2(lo.x, lo.y);
+                v[q][1] = make_float2(lo.z, lo.w);
+                v[q][2] = make_float2(hi.x, hi.y);
+                v[q][3] = make_float2(hi.z, hi.w);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const float2 w[4] = {v[0][i], v[1][i], v[2][i], v[3][i]};
+                response_sums(w, invN, pa[i], pe[i], p0[i]);
+            }
+            const size_t off = (size_t(gp) * 4 + o) * g.n + size_t(y) * w2 + x;
+            *reinterpret_cast<float4 *>(g.amp + off) = oa;
+            *reinterpret_cast<float4 *>(g.energy + off) = oe;
+            *reinterpret_cast<float4 *>(g.eo0 + off) = o0;
+        }
+    } else if (!consts_mode) {
         const int gp = g.pair0 * 2 + plane;
         for (int rl = 0; rl < rr; rl++) {
             const int y = y0 + rl;
@@ -538,7 +570,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_kernel(FsimGroup g, const
 // CTA transforms one scale at a time with the block-level engine.
 __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_seq_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int consts_mode,
                                                                double *rowsums) {
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(16) float2 sm[];
     __shared__ double red[4][FT / 32];
     const int y = blockIdx.x, o = blockIdx.y, plane = blockIdx.z;
     const int w2 = g.w2;
