@@ -140,6 +140,18 @@ void table(std::vector<float2> &out, int n) {
 
 }  // namespace
 
+bool plan_length(int n, std::vector<int> &r, int &m, std::vector<int> &rm) {
+    // Direct plan, or Bluestein on the smallest 2,3,5-smooth m >= 2n-1 when that is estimated
+    // cheaper (two length-m transforms plus three pointwise passes).
+    long long direct_cost = 0, m_cost = 0;
+    const bool direct = factor(n, r, &direct_cost);
+    m = 2 * n - 1;
+    while (!smooth235(m)) m++;
+    factor(m, rm, &m_cost);
+    const long long blue_cost = 2 * m_cost + 3 * 12 * (long long)((m + 31) / 32);
+    return direct && (n <= 2 || direct_cost <= blue_cost);
+}
+
 const FftLen &fft_len(iqm_ctx *ctx, int n) {
     auto it = ctx->fft_plans.find(n);
     if (it != ctx->fft_plans.end()) return it->second->len;
@@ -150,16 +162,9 @@ const FftLen &fft_len(iqm_ctx *ctx, int n) {
     std::vector<int> r;
     std::vector<float2> tw, mtw, chirp, bf, bi, stw, mstw;
     table(tw, n);
-    // Direct plan, or Bluestein on the smallest 2,3,5-smooth m >= 2n-1 when that is estimated cheaper
-    // (two length-m transforms plus three pointwise passes).
-    long long direct_cost = 0, m_cost = 0;
-    const bool direct = factor(n, r, &direct_cost);
-    int m = 2 * n - 1;
-    while (!smooth235(m)) m++;
+    int m = 0;
     std::vector<int> rm;
-    factor(m, rm, &m_cost);
-    const long long blue_cost = 2 * m_cost + 3 * 12 * (long long)((m + 31) / 32);
-    if (direct && (n <= 2 || direct_cost <= blue_cost)) {
+    if (plan_length(n, r, m, rm)) {
         L.bluestein = 0;
         L.nst = int(r.size());
         stage_tables(n, r, L.radix, L.stride, L.inv_stride, L.inv_q, L.stw_off, L.stw_len, stw);
