@@ -8,7 +8,7 @@
 // here is its mean.
 //
 // Two kernels:
-//   flip_hpass_kernel  one CTA per 256-pixel row segment of both images: RGBA8 -> linear RGB by a
+//   flip_hpass_kernel  one CTA per 512-pixel row segment of both images: RGBA8 -> linear RGB by a
 //                      256-entry table (the sRGB curve of srgb_to_ycxcz.glsl:22-28 on 8-bit inputs),
 //                      -> XYZ -> YCxCz in shared memory, then the horizontal feature taps (g, edge,
 //                      point on (Y+16)/116, feature_filter_horizontal.glsl) and the horizontal CSF
@@ -39,8 +39,8 @@ namespace {
 
 constexpr int MAXR = 32;          // largest supported filter radius (ppd up to ~235)
 constexpr int MAXT = 2 * MAXR + 1;
-constexpr int HSEG = 256;         // pixels per row segment (hpass)
-constexpr int HT = 64;            // hpass threads (4 pixels each)
+constexpr int HSEG = 512;         // pixels per row segment (hpass)
+constexpr int HT = HSEG / 4;      // hpass threads (4 pixels each)
 constexpr int VT_COLS = 32, VT_ROWS = 32, VT_RPT = 8;  // vpass tile and rows per thread
 constexpr int VT = VT_COLS * (VT_ROWS / VT_RPT);        // 128 threads
 constexpr int NPLANE = 12;        // per pair: [img][dx, ddx, value, Y, Cx, Cz]
