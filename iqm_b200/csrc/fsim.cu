@@ -797,18 +797,21 @@ void plane_size(int w, int h, int F, int &w2, int &h2) {  // src/gpu/fsim/fsim.c
 constexpr size_t SMEM_CAP = 200 * 1024;
 constexpr int kFsimStreams = 8;  // plane-size groups in flight at once
 
-// Raises a kernel's dynamic shared-memory limit to at least `bytes` (never lowers it: launches
-// already enqueued or captured for other plane sizes keep their sizes valid).
+// Raises a kernel's dynamic shared-memory limit on the current device to at least `bytes` (never
+// lowers it: launches already enqueued or captured for other plane sizes keep their sizes valid).
 void set_smem(const void *fn, size_t bytes) {
     static std::mutex mu;
-    static std::map<const void *, size_t> current;
+    static std::map<std::pair<int, const void *>, size_t> current;  // kernel attributes are per device
+    int dev = 0;
+    IQM_CHECK_CUDA(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> lock(mu);
-    auto it = current.find(fn);
+    const auto key = std::make_pair(dev, fn);
+    auto it = current.find(key);
     if (it == current.end()) {
         // transform CTAs are shared-memory bound: ask for the largest shared-memory carveout so
         // as many CTAs fit per SM as registers allow
         IQM_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-        it = current.emplace(fn, 0).first;
+        it = current.emplace(key, 0).first;
     }
     if (bytes <= 48 * 1024 || bytes <= it->second) return;
     IQM_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
