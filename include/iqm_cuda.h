@@ -14,7 +14,7 @@
  *   - Plain C types only; no exceptions cross this boundary.  Every call returns IQM_OK (0) or a
  *     negative IQM_E* code, and iqm_last_error() describes the last failure on that context.
  *   - Images are RGBA8, row-major, `row_bytes` apart (>= 4*w); the alpha byte is ignored, as in
- *     the reference's shaders.  "input" is the distorted image, "ref" the reference image
+ *     the reference's shaders.  Sides up to 65536 and fewer than 2^31 pixels per image.  "input" is the distorted image, "ref" the reference image
  *     (the CLI's --input / --ref, src/args.cpp:38-43).
  *   - Host entry points (iqm_ssim, iqm_fsim, iqm_flip, iqm_msvd and the *_batch forms) take host
  *     pointers (pageable or pinned), copy to the device, compute, copy results back and return

@@ -200,7 +200,8 @@ inline void check_pairs(const iqm_pair *pairs, int n, int min_w, int min_h) {
         IQM_REQUIRE(p.w >= min_w && p.h >= min_h,
                     "pair " + std::to_string(i) + ": image too small (" + std::to_string(p.w) + "x" +
                         std::to_string(p.h) + ")");
-        IQM_REQUIRE(p.w <= 65536 && p.h <= 65536, "pair " + std::to_string(i) + ": image too large");
+        IQM_REQUIRE(p.w <= 65536 && p.h <= 65536 && (long long)p.w * p.h < (1LL << 31),
+                    "pair " + std::to_string(i) + ": image too large (at most 65536 per side and 2^31 pixels)");
         IQM_REQUIRE(p.row_bytes >= size_t(p.w) * 4, "pair " + std::to_string(i) + ": row_bytes < 4*w");
     }
 }

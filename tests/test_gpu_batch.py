@@ -116,3 +116,20 @@ def test_plan_error_leaves_context_usable(rt):
         iqm_b200.BatchPlan(rt, iqm_b200.METRIC_FSIM, items, d_scores.data_ptr())
     a, b = synth.grey_pair(64, 64, config=0, pair=1)
     assert 0.0 < iqm_b200.SSIM(rt).compute_metric(a, b).mssim <= 1.0
+
+
+def test_images_of_2_31_pixels_are_rejected(rt):
+    """Pair validation (before any copy or launch) refuses images of 2^31 pixels or more, whose
+    pixel counts would overflow 32-bit plane indices."""
+    import ctypes
+    buf = np.zeros(64, np.uint8)  # never read: validation fails first
+    arr = iqm_b200._pairs([(buf.ctypes.data, buf.ctypes.data, 50000, 50000, 200000)])
+    out = (ctypes.c_double * 4)()
+    sp, fp = iqm_b200.SSIM(rt).params(), iqm_b200.FLIPArguments().c()
+    L = rt.L
+    for rc in (L.iqm_ssim_batch(rt.h, arr, 1, ctypes.byref(sp), out),
+               L.iqm_msvd_batch(rt.h, arr, 1, out),
+               L.iqm_flip_batch(rt.h, arr, 1, ctypes.byref(fp), out),
+               L.iqm_fsim_batch(rt.h, arr, 1, 0, 0, out)):
+        assert rc == iqm_b200.IQM_EINVAL
+        assert "too large" in L.iqm_last_error(rt.h).decode()
