@@ -20,7 +20,8 @@ def test_plan_constants_match_oracle(rt, o64, w2, h2, mode):
     assert np.allclose(aiaj, oaiaj, rtol=1e-4, atol=1e-6 * np.abs(oan2).max())
 
 
-@pytest.mark.parametrize("h,w", [(96, 128), (130, 200), (270, 480), (600, 800), (1080, 1920), (131, 263), (57, 61)])
+@pytest.mark.parametrize("h,w", [(96, 128), (130, 200), (270, 480), (600, 800), (1080, 1920), (131, 263), (57, 61),
+                                 (2160, 3840)])
 def test_fsim_matches_oracle(rt, o64, o32, h, w):
     a, b = synth.rgb_gain_pair(h, w, config=1, pair=w % 7)
     r = iqm_b200.FSIM(rt).compute_metric(a, b)
