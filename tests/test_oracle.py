@@ -129,3 +129,55 @@ def test_flip_ppd_and_taps(o64):
     for c in (1, 2):
         assert t[c][t[c] > 0].sum() == pytest.approx(1.0)
         assert -t[c][t[c] < 0].sum() == pytest.approx(1.0)
+
+
+def _opencv_mssim(img, ref, ks=11, sigma=1.5, k1=0.01, k2=0.03):
+    """MSSIM built from OpenCV's Gaussian kernel and filtering (the classic OpenCV SSIM recipe) with
+    the reference's luma weights (shaders/ssim/ssim_lumapack.glsl: 0.299, 0.581, 0.114 on unorm RGB)
+    and pooled region x, y in [r, dim - r] (src/gpu/ssim/ssim.cpp:386-401).  Inside x, y < dim - r
+    every window lies in the image (OpenCV's filtering applies unchanged); the last pooled column and
+    row are computed directly with the reference's truncated, renormalised window."""
+    import cv2
+
+    def luma(x):
+        x = x.astype(np.float64) / 255.0
+        return 0.299 * x[..., 0] + 0.581 * x[..., 1] + 0.114 * x[..., 2]
+
+    a, b = luma(img), luma(ref)
+    g = cv2.getGaussianKernel(ks, sigma, cv2.CV_64F)
+    blur = lambda x: cv2.sepFilter2D(x, cv2.CV_64F, g, g, borderType=cv2.BORDER_REFLECT)
+    mu_a, mu_b = blur(a), blur(b)
+    var_a = blur(a * a) - mu_a * mu_a
+    var_b = blur(b * b) - mu_b * mu_b
+    cov = blur(a * b) - mu_a * mu_b
+    c1, c2 = k1 * k1, k2 * k2
+    m = ((2 * mu_a * mu_b + c1) * (2 * cov + c2)) / ((mu_a ** 2 + mu_b ** 2 + c1) * (var_a + var_b + c2))
+    r = ks // 2
+    h, w = a.shape
+    # The pooled region's last column (x = w - r) and row (y = h - r) have windows that reach one
+    # pixel past the image; there the reference truncates the window and renormalises its weights.
+    g1 = g[:, 0]
+    for y in range(r, h - r + 1):
+        for x in range(r, w - r + 1):
+            if x < w - r and y < h - r:
+                continue
+            ys, xs = slice(max(0, y - r), min(h, y + r + 1)), slice(max(0, x - r), min(w, x + r + 1))
+            wy = g1[ys.start - (y - r): ys.stop - (y - r)]
+            wx = g1[xs.start - (x - r): xs.stop - (x - r)]
+            wt = np.outer(wy, wx)
+            wt = wt / wt.sum()
+            pa, pb = a[ys, xs], b[ys, xs]
+            ma, mb = (wt * pa).sum(), (wt * pb).sum()
+            va, vb = (wt * (pa - ma) ** 2).sum(), (wt * (pb - mb) ** 2).sum()
+            cv = (wt * (pa - ma) * (pb - mb)).sum()
+            m[y, x] = ((2 * ma * mb + c1) * (2 * cv + c2)) / ((ma * ma + mb * mb + c1) * (va + vb + c2))
+    return float(m[r:h - r + 1, r:w - r + 1].mean())
+
+
+@pytest.mark.parametrize("h,w,ks,sigma", [(64, 80, 11, 1.5), (97, 131, 11, 1.5), (512, 512, 11, 1.5), (70, 90, 7, 1.2)])
+def test_ssim_matches_opencv_gaussian_ssim(o64, o32, h, w, ks, sigma):
+    """Pins the SSIM restatement to an independent third-party Gaussian filter (OpenCV 4.13)."""
+    a, b = synth.rgb_gain_pair(h, w, config=0, pair=w % 5)
+    want = _opencv_mssim(a, b, ks=ks, sigma=sigma)
+    assert abs(o64.ssim(a, b, kernel_size=ks, sigma=sigma) - want) <= 1e-9
+    assert abs(o32.ssim(a, b, kernel_size=ks, sigma=sigma) - want) <= 1e-5
