@@ -543,4 +543,64 @@ struct FixedPlan {
     }
 };
 
+
+// In-place form of the fixed-length engine: every stage first reads all of a lane's butterfly inputs
+// into registers, synchronises the warp, then writes the butterflies' outputs into the same buffer
+// (the same values the two-buffer stage would write), so one transform needs one buffer of N points.
+template <int N, int L, int... Rs>
+struct FixedStagesIP;
+
+template <int N, int L>
+struct FixedStagesIP<N, L> {
+    static __device__ __forceinline__ void run(float2 *, const float2 *, int, float) {}
+};
+
+template <int N, int L, int P, int... Rs>
+struct FixedStagesIP<N, L, P, Rs...> {
+    static __device__ __forceinline__ void run(float2 *buf, const float2 *stw, int stw_off, float s) {
+        constexpr int Q = N / P;
+        constexpr int IT = (Q + 31) / 32;
+        const int lane = threadIdx.x & 31;
+        float2 v[IT][P];
+#pragma unroll
+        for (int it = 0; it < IT; it++) {
+            const int j = lane + 32 * it;
+            if ((Q % 32 == 0) || j < Q) {
+#pragma unroll
+                for (int r = 0; r < P; r++) v[it][r] = buf[j + r * Q];
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int it = 0; it < IT; it++) {
+            const int j = lane + 32 * it;
+            if ((Q % 32 == 0) || j < Q) {
+                const int jl = j / L, k = j - jl * L;
+                if (L > 1 && k != 0) {
+                    const float2 *w = stw + stw_off + k * (P - 1) - 1;
+#pragma unroll
+                    for (int r = 1; r < P; r++) v[it][r] = cmul(v[it][r], make_float2(w[r].x, -s * w[r].y));
+                }
+                dft_small<P>(v[it], s);
+                const int base = jl * L * P + k;
+#pragma unroll
+                for (int r = 0; r < P; r++) buf[base + r * L] = v[it][r];
+            }
+        }
+        __syncwarp();
+        FixedStagesIP<N, L * P, Rs...>::run(buf, stw, stw_off + (P - 1) * L, s);
+    }
+};
+
+template <int N, int... Rs>
+struct FixedPlanIP {
+    static constexpr int n = N;
+    // result in `a`; `b` is not used
+    static __device__ __forceinline__ float2 *run(float2 *a, float2 *, const float2 *stw, float s) {
+        __syncwarp();
+        FixedStagesIP<N, 1, Rs...>::run(a, stw, 0, s);
+        return a;
+    }
+};
+
 }  // namespace iqm

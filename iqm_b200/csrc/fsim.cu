@@ -243,12 +243,12 @@ __global__ void __launch_bounds__(FT) fsim_ingest_kernel(FsimGroup g) {
 
 // ---------------------------------------------------------------------------------------------
 // Transform kernels.  Shared memory of every transform CTA starts with the stage twiddles of its
-// length (FftLen::stw), followed by per-warp work buffers: a warp transforms NB sequences at once
-// (buffer a: NB x wl, buffer b: NB x wl), which keeps the lanes busy on stages with few butterflies.
+// length (FftLen::stw), followed by per-warp work buffers: a warp transforms NB sequences at once in
+// buffer a (NB x wl) and, unless the engine transforms in place, a ping-pong buffer b of the same
+// size.
 constexpr int NB = 1;  // the transform engines run one sequence per warp
 static_assert(NB == 1, "column slabs index with cols == 1 << lw");
 
-__device__ __forceinline__ float2 *warp_area(float2 *base, int warp, int wl) { return base + size_t(warp) * 2 * NB * wl; }
 
 // Transform engines: the runtime-planned warp engine for any length, or a fixed-length one whose
 // radix sequence is compiled in (the host picks it only when it equals the length's own plan, so
@@ -276,8 +276,34 @@ struct engine_len<FixedEngine<FP>> {
     static constexpr int value = FP::n;
 };
 
+// Work buffers a transform needs: two for the ping-pong engines, one for the in-place fixed plans.
+template <class FP>
+struct plan_bufs {
+    static constexpr int value = 2;
+};
+template <int N, int... Rs>
+struct plan_bufs<iqm::FixedPlanIP<N, Rs...>> {
+    static constexpr int value = 1;
+};
+template <class E>
+struct engine_bufs {
+    static constexpr int value = 2;
+};
+template <class FP>
+struct engine_bufs<FixedEngine<FP>> {
+    static constexpr int value = plan_bufs<FP>::value;
+};
+
+// The work area of warp `warp` in a CTA whose warps each hold engine_bufs<E> buffers of wl points.
+template <class E>
+__device__ __forceinline__ float2 *warp_area(float2 *base, int warp, int wl) {
+    return base + size_t(warp) * engine_bufs<E>::value * NB * wl;
+}
+
+// 480 (the row length, whose pass is limited by shared memory) transforms in place; 270 (the column
+// length, whose pass is limited by registers) keeps the two-buffer form.
 using Engine270 = FixedEngine<iqm::FixedPlan<270, 9, 3, 10>>;
-using Engine480 = FixedEngine<iqm::FixedPlan<480, 15, 8, 4>>;
+using Engine480 = FixedEngine<iqm::FixedPlanIP<480, 15, 8, 4>>;
 
 // forward transform (src/gpu/fsim/fsim.cpp:270-368: luma as complex (Y, 0), sign -1, unscaled),
 // NB rows per warp.
@@ -293,7 +319,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_fwd_rows_kernel(FsimGroup g, const
     const int y0 = (blockIdx.x * (blockDim.x >> 5) + warp) * NB;
     if (y0 >= g.h2) return;  // warp-uniform; no block-wide barrier follows
     const int nb = min(NB, g.h2 - y0);
-    float2 *a = warp_area(work, warp, wl), *b = a + NB * wl;
+    float2 *a = warp_area<Eng>(work, warp, wl), *b = a + NB * wl;
     const float *Y = g.yiq + (size_t(plane) * 3 + 2) * g.n + size_t(y0) * g.w2;
     for (int t = 0; t < nb; t++)
         for (int x = lane; x < g.w2; x += 32) a[t * wl + x] = make_float2(Y[size_t(t) * g.w2 + x], 0.f);
@@ -322,19 +348,19 @@ __global__ void __launch_bounds__(FT, 1) fsim_fwd_cols_kernel(FsimGroup g, const
     // column c lives in warp c / NB, slot c % NB
     for (int idx = threadIdx.x; idx < cols * g.h2; idx += blockDim.x) {
         const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
-        if (c < nc) warp_area(work, c / NB, wl)[(c % NB) * wl + y] = S[size_t(y) * g.w2 + x0 + c];
+        if (c < nc) warp_area<Eng>(work, c / NB, wl)[(c % NB) * wl + y] = S[size_t(y) * g.w2 + x0 + c];
     }
     __syncthreads();
     const int nbw = min(NB, nc - warp * NB);
     if (nbw > 0) {
-        float2 *a = warp_area(work, warp, wl);
+        float2 *a = warp_area<Eng>(work, warp, wl);
         float2 *res = Eng::run(a, a + NB * wl, L, sm, -1.f, wl);
         if (warp == 0 && (threadIdx.x & 31) == 0) parity = slab_parity(res, a);
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < cols * g.h2; idx += blockDim.x) {
         const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
-        if (c < nc) S[size_t(y) * g.w2 + x0 + c] = warp_area(work, c / NB, wl)[parity * NB * wl + (c % NB) * wl + y];
+        if (c < nc) S[size_t(y) * g.w2 + x0 + c] = warp_area<Eng>(work, c / NB, wl)[parity * NB * wl + (c % NB) * wl + y];
     }
 }
 
@@ -343,9 +369,10 @@ __global__ void __launch_bounds__(FT, 1) fsim_fwd_cols_kernel(FsimGroup g, const
 // spectrum x H[o*4+s] (fsim_filter_combinations.glsl:53-56), sign +1.  consts_mode uses a
 // spectrum of ones, i.e. transforms the filters themselves (block 0 of the reference's buffer).
 template <class Eng>
-// Compiled-length engines: 4 CTAs per SM (64 registers; with the largest shared-memory carveout the
-// work buffers of 4 CTAs fit).  The runtime-planned engine needs more registers.
-__global__ void __launch_bounds__(FT, engine_len<Eng>::value ? 4 : 1) fsim_inv_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int lw, int consts_mode) {
+// Two-buffer compiled engines: 4 CTAs per SM (64 registers; with the largest shared-memory carveout
+// the work buffers of 4 CTAs fit).  The runtime-planned and in-place engines need more registers here.
+__global__ void __launch_bounds__(FT, engine_len<Eng>::value && engine_bufs<Eng>::value == 2 ? 4 : 1)
+fsim_inv_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int lw, int consts_mode) {
     extern __shared__ __align__(16) float2 sm[];
     __shared__ int parity;
     const int tl = iqm::stage_twiddle_len(L);
@@ -382,7 +409,7 @@ __global__ void __launch_bounds__(FT, engine_len<Eng>::value ? 4 : 1) fsim_inv_c
     for (int s = 0; s < 4; s++) {
         const int z = o * 4 + s;
         if (nbw > 0) {
-            float2 *a = warp_area(work, warp, wl);
+            float2 *a = warp_area<Eng>(work, warp, wl);
             const float2 *col = Sl + size_t(warp) * h2;  // NB == 1: column `warp` of the slab
             if constexpr (PN > 0) {
                 float hcur[PV];
@@ -412,7 +439,7 @@ __global__ void __launch_bounds__(FT, engine_len<Eng>::value ? 4 : 1) fsim_inv_c
         float2 *dst = g.T + (size_t(plane) * 16 + z) * g.n;
         for (int idx = threadIdx.x; idx < cols * h2; idx += blockDim.x) {
             const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
-            if (c < nc) dst[size_t(y) * g.w2 + x0 + c] = warp_area(work, c / NB, wl)[parity * NB * wl + (c % NB) * wl + y];
+            if (c < nc) dst[size_t(y) * g.w2 + x0 + c] = warp_area<Eng>(work, c / NB, wl)[parity * NB * wl + (c % NB) * wl + y];
         }
         __syncthreads();
     }
@@ -444,7 +471,7 @@ __device__ __forceinline__ void response_sums(const float2 v[4], float invN, flo
 // warp (r, h) transforms scales h*NB .. h*NB+NB-1 of row y0 + r.  consts_mode (rr = 1) instead accumulates, per row, sum_s Re_s^2 N and
 // sum_{i<j} Re_i Re_j N (shaders/fsim/fsim_mult_filters.glsl:37-58) over p < ceil(N/2) and all p.
 template <class Eng>
-__global__ void __launch_bounds__(FT, 1) fsim_inv_rows_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int rr, int consts_mode,
+__global__ void __launch_bounds__(FT, engine_len<Eng>::value ? 4 : 1) fsim_inv_rows_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int rr, int consts_mode,
                                                               double *rowsums) {
     extern __shared__ __align__(16) float2 sm[];
     __shared__ int parity;
@@ -462,7 +489,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_kernel(FsimGroup g, const
     {
         const int y = y0 + r;
         if (r < rr && y < g.h2) {
-            float2 *a = warp_area(work, warp, wl);
+            float2 *a = warp_area<Eng>(work, warp, wl);
             for (int t = 0; t < NB; t++) {
                 const float2 *src = g.T + (size_t(plane) * 16 + o * 4 + h * NB + t) * g.n + size_t(y) * w2;
                 for (int x = lane; x < w2; x += 32) a[t * wl + x] = src[x];
@@ -474,7 +501,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_kernel(FsimGroup g, const
     __syncthreads();
     // scale s of row rl: warp rl*WPR + s/NB, slot s%NB
     auto at = [&](int rl, int s, int x) -> float2 {
-        return warp_area(work, rl * WPR + s / NB, wl)[parity * NB * wl + (s % NB) * wl + x];
+        return warp_area<Eng>(work, rl * WPR + s / NB, wl)[parity * NB * wl + (s % NB) * wl + x];
     };
     const float invN = 1.0f / float(g.n);
     if (!consts_mode && (w2 & 3) == 0 && rr <= 2) {
@@ -492,7 +519,7 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_kernel(FsimGroup g, const
             float2 v[4][4];  // [scale][pixel]
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                const float4 *src4 = reinterpret_cast<const float4 *>(&warp_area(work, rl * WPR + q / NB, wl)[parity * NB * wl + (q % NB) * wl + x]);
+                const float4 *src4 = reinterpret_cast<const float4 *>(&warp_area<Eng>(work, rl * WPR + q / NB, wl)[parity * NB * wl + (q % NB) * wl + x]);
                 const float4 lo = src4[0], hi = src4[1];
                 v[q][0] = make_float2(lo.x, lo.y);
                 v[q][1] = make_float2(lo.z, lo.w);
@@ -844,6 +871,12 @@ int engine_id(const iqm::FftLen &L) {
     return 0;
 }
 
+// Work buffers per warp of engine `id` (matches engine_bufs of the types with_engine selects).
+int engine_buffers(int id) { return id == 2 ? 1 : 2; }
+static_assert(engine_bufs<Engine270>::value == 2 && engine_bufs<Engine480>::value == 1 &&
+                  engine_bufs<GenericEngine>::value == 2,
+              "engine_buffers() must match the engines' work buffers");
+
 template <class F>
 void with_engine(int id, F &&f) {
     switch (id) {
@@ -868,7 +901,8 @@ Shapes shapes_for(const iqm::FsimPlan &P, const iqm::FsimTune &tune = iqm::FsimT
     s.col_eng = engine_id(P.col);
     const size_t twr = size_t((iqm::stage_twiddle_len(P.row) + 1) & ~1) * f2;
     const size_t twc = size_t((iqm::stage_twiddle_len(P.col) + 1) & ~1) * f2;
-    const size_t warp_row = 2 * NB * size_t(s.wl_row) * f2, warp_col = 2 * NB * size_t(s.wl_col) * f2;
+    const size_t warp_row = engine_buffers(s.row_eng) * NB * size_t(s.wl_row) * f2;
+    const size_t warp_col = engine_buffers(s.col_eng) * NB * size_t(s.wl_col) * f2;
     s.lw_rows = lw_fit(twr, warp_row);
     s.sm_rows = twr + (size_t(1) << s.lw_rows) * warp_row;
     s.lw_fcols = lw_fit(twc, warp_col);
