@@ -68,6 +68,7 @@ extern "C" __attribute__((visibility("default"))) int iqm_destroy(iqm_ctx *ctx) 
     iqm::timing_release(ctx);
     for (auto st : ctx->side_streams) cudaStreamDestroy(st);
     for (auto ev : ctx->side_events) cudaEventDestroy(ev);
+    for (auto ev : ctx->aux_events) cudaEventDestroy(ev);
     if (ctx->fork_event) cudaEventDestroy(ctx->fork_event);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -170,6 +171,15 @@ void side_streams(iqm_ctx *ctx, int n) {
         ctx->side_streams.push_back(st);
         ctx->side_events.push_back(ev);
     }
+}
+
+cudaEvent_t aux_event(iqm_ctx *ctx, int i) {
+    while (int(ctx->aux_events.size()) <= i) {
+        cudaEvent_t ev = nullptr;
+        IQM_CHECK_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        ctx->aux_events.push_back(ev);
+    }
+    return ctx->aux_events[i];
 }
 
 std::vector<iqm_pair> upload_pairs(iqm_ctx *ctx, const iqm_pair *pairs, int n) {

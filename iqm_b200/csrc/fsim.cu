@@ -823,6 +823,7 @@ void plane_size(int w, int h, int F, int &w2, int &h2) {  // src/gpu/fsim/fsim.c
 
 constexpr size_t SMEM_CAP = 200 * 1024;
 constexpr int kFsimStreams = 8;  // plane-size groups in flight at once
+constexpr bool kOverlapChunks = true;  // alternate inverse-pass chunks between two streams
 
 // Raises a kernel's dynamic shared-memory limit on the current device to at least `bytes` (never
 // lowers it: launches already enqueued or captured for other plane sizes keep their sizes valid).
@@ -1036,13 +1037,14 @@ struct Layout {
 };
 
 // G pairs of the group; chunk pairs' worth of inverse-pass intermediates.
-Layout layout_for(int G, int chunk, int n, int tiles) {
+// nbuf: inverse-pass intermediate buffers (2 when consecutive chunks alternate between two streams).
+Layout layout_for(int G, int chunk, int n, int tiles, int nbuf = 1) {
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     Layout L{};
     size_t off = 0;
     L.yiq = off; off += al(sizeof(float) * size_t(G) * 6 * n);
     L.spec = off; off += al(sizeof(float2) * size_t(G) * 2 * n);
-    L.T = off; off += al(sizeof(float2) * size_t(chunk) * 32 * n);
+    L.T = off; off += al(sizeof(float2) * size_t(nbuf) * chunk * 32 * n);
     L.planes = off; off += al(sizeof(float) * size_t(G) * 24 * n);
     L.thr = off; off += al(sizeof(float) * size_t(G) * 8);
     L.partials = off; off += al(sizeof(double) * size_t(G) * tiles * 3);
@@ -1093,6 +1095,7 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
     // per-size tables first (building one waits for the context stream)
     struct GroupRun {
         int w2, h2, G, first, slot, F_uniform, chunk;
+        bool overlap;  // inverse-pass chunks alternate between two streams and two T buffers
         iqm::FsimPlan *P;
         Shapes s;
         Layout L;
@@ -1111,7 +1114,11 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
             r.s = shapes_for(*r.P, ctx->fsim_tune);
             const int n = r.P->n;
             r.chunk = chunk_pairs(ctx->fsim_tune, r.G, n);
-            r.L = layout_for(r.G, r.chunk, n, int(iqm::ceil_div(n, FT)));
+            // More than one chunk: split the L2 budget over two buffers and let consecutive chunks run
+            // on two streams, so one chunk's column pass fills the other's last partial wave.
+            r.overlap = kOverlapChunks && !ctx->timing && r.G > r.chunk;
+            if (r.overlap) r.chunk = std::max(1, r.chunk / 2);
+            r.L = layout_for(r.G, r.chunk, n, int(iqm::ceil_div(n, FT)), r.overlap ? 2 : 1);
             r.F_uniform = hd[kv.second[0]].F;
             for (int i : kv.second)
                 if (hd[i].F != r.F_uniform) r.F_uniform = 0;
@@ -1144,6 +1151,9 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
     }
     auto *base0 = static_cast<uint8_t *>(ctx->scratch.get(slot_off[S], ctx->stream));
     std::vector<cudaStream_t> streams(S, ctx->stream);
+    bool any_overlap = false;
+    for (const auto &r : runs) any_overlap |= r.overlap;
+    if (any_overlap) iqm::side_streams(ctx, 2 * S);  // streams S .. 2S-1 take the odd chunks
     if (S > 1) {
         iqm::side_streams(ctx, S);
         IQM_CHECK_CUDA(cudaEventRecord(ctx->fork_event, ctx->stream));
@@ -1200,14 +1210,28 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
                     g, P->col, s.wl_col, s.lw_fcols);
         });
         iqm::check_launch(ctx, "fsim_fwd_cols_kernel");
-        for (int c0 = 0; c0 < G; c0 += chunk) {
+        cudaStream_t st2 = st;
+        if (r.overlap) {
+            st2 = ctx->side_streams[S + r.slot];
+            cudaEvent_t fork = iqm::aux_event(ctx, r.slot);
+            IQM_CHECK_CUDA(cudaEventRecord(fork, st));
+            IQM_CHECK_CUDA(cudaStreamWaitEvent(st2, fork, 0));
+        }
+        for (int c0 = 0, k = 0; c0 < G; c0 += chunk, k++) {
             FsimGroup gc = g;
             gc.pair0 = c0;
+            const bool odd = r.overlap && (k & 1);
+            if (odd) gc.T = g.T + size_t(chunk) * 32 * n;
+            cudaStream_t cs = odd ? st2 : st;
             const int cg = std::min(chunk, G - c0);
-            launch_inv_cols(gc, *P, s, 2 * cg, 0, st);
+            launch_inv_cols(gc, *P, s, 2 * cg, 0, cs);
             iqm::check_launch(ctx, "fsim_inv_cols_kernel");
-            launch_inv_rows(gc, *P, s, 2 * cg, 0, nullptr, st);
+            launch_inv_rows(gc, *P, s, 2 * cg, 0, nullptr, cs);
             iqm::check_launch(ctx, "fsim_inv_rows_kernel");
+        }
+        if (r.overlap) {
+            IQM_CHECK_CUDA(cudaEventRecord(ctx->side_events[S + r.slot], st2));
+            IQM_CHECK_CUDA(cudaStreamWaitEvent(st, ctx->side_events[S + r.slot], 0));
         }
         fsim_noise_kernel<<<dim3(8, G), 1024, 0, st>>>(g);
         iqm::check_launch(ctx, "fsim_noise_kernel");

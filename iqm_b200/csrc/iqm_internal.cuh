@@ -133,6 +133,7 @@ struct iqm_ctx {
     std::vector<cudaStream_t> side_streams;
     std::vector<cudaEvent_t> side_events;
     cudaEvent_t fork_event = nullptr;
+    std::vector<cudaEvent_t> aux_events;  // further fork points (iqm::aux_event)
 
     // named scratch areas (each grow-only)
     iqm::DevBuf desc;      // per-call pair descriptors
@@ -212,6 +213,8 @@ void *upload_bytes(iqm_ctx *ctx, DevBuf &dst, const void *src, size_t bytes);
 
 // Makes at least n side streams (with one join event each) and the fork event exist on the context.
 void side_streams(iqm_ctx *ctx, int n);
+// Event i of the context's auxiliary pool (created on first use; timing disabled).
+cudaEvent_t aux_event(iqm_ctx *ctx, int i);
 
 // Copies host pairs to device memory (inside ctx->images) and rewrites the pointers.
 std::vector<iqm_pair> upload_pairs(iqm_ctx *ctx, const iqm_pair *pairs, int n);
