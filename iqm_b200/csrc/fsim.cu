@@ -153,11 +153,12 @@ __global__ void fsim_em_kernel(const float *filters, int n, double *consts) {
 // ---------------------------------------------------------------------------------------------
 // ingest -- shaders/fsim/fsim_downsample.glsl:21-55: RGB x 255 -> (I, Q, Y), F x F box starting
 // at (x F - F/2, y F - F/2), out-of-image samples contribute 0, divided by F^2 always.
+// The shader's unorm load followed by x 255 gives back the byte value exactly in FP32
+// ((b / 255) * 255 == b for every byte b), and the YIQ transform is linear, so each window's channel
+// bytes are summed as integers (exact) and transformed once; the shader's per-sample FP32
+// accumulation differs from this only by its own rounding.
 template <int FF>  // FF = downscale factor when known at compile time, 0 = read it from the pair
 __global__ void __launch_bounds__(FT) fsim_ingest_kernel(FsimGroup g) {
-    __shared__ float u8f[256];  // (b / 255) * 255 in float, as the unorm load followed by * 255.0
-    for (int i = threadIdx.x; i < 256; i += FT) u8f[i] = __fdiv_rn(float(i), 255.0f) * 255.0f;
-    __syncthreads();
     const int pi = blockIdx.y;
     const int p = blockIdx.x * FT + threadIdx.x;
     if (p >= g.n) return;
@@ -166,78 +167,85 @@ __global__ void __launch_bounds__(FT) fsim_ingest_kernel(FsimGroup g) {
     const int F = FF ? FF : P.F;
     const int xs = x * F - F / 2, ys = y * F - F / 2;
     const float scaler = float(F * F);
+    unsigned rb[2] = {0u, 0u}, gs[2] = {0u, 0u};  // FF != 0: R | B << 16 per image (F^2 * 255 < 2^16)
+    unsigned r32[2] = {0u, 0u}, b32[2] = {0u, 0u};  // FF == 0: R and B of a window of any size
+    if constexpr (FF == 4 || FF == 8) {
+        // the window's F pixels of a row start at byte 4F x - 2F: 8-byte aligned for F = 4,
+        // 16-byte aligned for F = 8 (given an aligned base and pitch); rows load as vectors when
+        // the whole row is inside the image
+        constexpr int V = FF == 4 ? 2 : 4;  // pixels per vector load
 #pragma unroll
-    for (int img = 0; img < 2; img++) {
-        const uint8_t *base = img ? P.b : P.a;
-        float sI = 0.f, sQ = 0.f, sY = 0.f;
-        auto add = [&](uint32_t px) {
-            const float r = u8f[px & 0xffu], gg = u8f[(px >> 8) & 0xffu], b = u8f[(px >> 16) & 0xffu];
-            sI += r * 0.596f - gg * 0.274f - b * 0.322f;
-            sQ += r * 0.211f - gg * 0.523f + b * 0.312f;
-            sY += r * 0.299f + gg * 0.587f + b * 0.114f;
-        };
-        if constexpr (FF == 4 || FF == 8) {
-            // the window's F pixels of a row start at byte 4F x - 2F: 8-byte aligned for F = 4,
-            // 16-byte aligned for F = 8 (given an aligned base and pitch); load rows as vectors
-            // when the whole row is inside the image, then sum in the shader's order
-            constexpr int V = FF == 4 ? 2 : 4;  // pixels per vector load
+        for (int img = 0; img < 2; img++) {
+            const uint8_t *base = img ? P.b : P.a;
             const bool vec = ((reinterpret_cast<uintptr_t>(base) | uintptr_t(P.pitch)) & (4 * V - 1)) == 0 &&
                              xs >= 0 && xs + FF <= P.w;
-            uint32_t px[FF][FF];  // [kk][jj]
-            bool row_ok[FF];
 #pragma unroll
             for (int kk = 0; kk < FF; kk++) {
                 const int k = ys + kk;
-                row_ok[kk] = k >= 0 && k < P.h;
-                const uint32_t *row = reinterpret_cast<const uint32_t *>(base + (long long)min(max(k, 0), P.h - 1) * P.pitch);
+                if (k < 0 || k >= P.h) continue;
+                const uint32_t *row = reinterpret_cast<const uint32_t *>(base + (long long)k * P.pitch);
+                uint32_t px[FF];
                 if (vec) {
 #pragma unroll
                     for (int q = 0; q < FF / V; q++) {
                         if constexpr (V == 2) {
                             const uint2 t = __ldg(reinterpret_cast<const uint2 *>(row + xs) + q);
-                            px[kk][2 * q] = t.x;
-                            px[kk][2 * q + 1] = t.y;
+                            px[2 * q] = t.x;
+                            px[2 * q + 1] = t.y;
                         } else {
                             const uint4 t = __ldg(reinterpret_cast<const uint4 *>(row + xs) + q);
-                            px[kk][4 * q] = t.x;
-                            px[kk][4 * q + 1] = t.y;
-                            px[kk][4 * q + 2] = t.z;
-                            px[kk][4 * q + 3] = t.w;
+                            px[4 * q] = t.x;
+                            px[4 * q + 1] = t.y;
+                            px[4 * q + 2] = t.z;
+                            px[4 * q + 3] = t.w;
                         }
                     }
                 } else {
 #pragma unroll
                     for (int jj = 0; jj < FF; jj++) {
                         const int j = xs + jj;
-                        px[kk][jj] = (j >= 0 && j < P.w) ? __ldg(row + j) : 0u;
+                        px[jj] = (j >= 0 && j < P.w) ? __ldg(row + j) : 0u;
                     }
                 }
-            }
 #pragma unroll
-            for (int jj = 0; jj < FF; jj++) {  // x outer, y inner, as fsim_downsample.glsl:46-52
-                const int j = xs + jj;
-                if (j < 0 || j >= P.w) continue;
-#pragma unroll
-                for (int kk = 0; kk < FF; kk++)
-                    if (row_ok[kk]) add(px[kk][jj]);
-            }
-        } else {
-#pragma unroll
-            for (int jj = 0; jj < F; jj++) {  // x outer, y inner, as fsim_downsample.glsl:46-52
-                const int j = xs + jj;
-                if (j < 0 || j >= P.w) continue;
-#pragma unroll
-                for (int kk = 0; kk < F; kk++) {
-                    const int k = ys + kk;
-                    if (k < 0 || k >= P.h) continue;
-                    add(__ldg(reinterpret_cast<const uint32_t *>(base + (long long)k * P.pitch) + j));
+                for (int jj = 0; jj < FF; jj++) {
+                    rb[img] += px[jj] & 0x00ff00ffu;
+                    gs[img] += (px[jj] >> 8) & 0xffu;
                 }
             }
         }
+    } else {
+#pragma unroll
+        for (int img = 0; img < 2; img++) {
+            const uint8_t *base = img ? P.b : P.a;
+            for (int kk = 0; kk < F; kk++) {
+                const int k = ys + kk;
+                if (k < 0 || k >= P.h) continue;
+                const uint32_t *row = reinterpret_cast<const uint32_t *>(base + (long long)k * P.pitch);
+                for (int jj = 0; jj < F; jj++) {
+                    const int j = xs + jj;
+                    if (j < 0 || j >= P.w) continue;
+                    const uint32_t v = __ldg(row + j);
+                    if constexpr (FF == 0) {
+                        r32[img] += v & 0xffu;
+                        b32[img] += (v >> 16) & 0xffu;
+                    } else {
+                        rb[img] += v & 0x00ff00ffu;
+                    }
+                    gs[img] += (v >> 8) & 0xffu;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int img = 0; img < 2; img++) {
+        const float r = float(FF ? rb[img] & 0xffffu : r32[img]);
+        const float b = float(FF ? rb[img] >> 16 : b32[img]);
+        const float gg = float(gs[img]);
         float *dst = g.yiq + size_t(pi * 2 + img) * 3 * g.n;
-        dst[p] = sI / scaler;
-        dst[g.n + p] = sQ / scaler;
-        dst[2 * g.n + p] = sY / scaler;
+        dst[p] = (r * 0.596f - gg * 0.274f - b * 0.322f) / scaler;
+        dst[g.n + p] = (r * 0.211f - gg * 0.523f + b * 0.312f) / scaler;
+        dst[2 * g.n + p] = (r * 0.299f + gg * 0.587f + b * 0.114f) / scaler;
     }
 }
 
@@ -678,13 +686,15 @@ __global__ void fsim_consts_reduce_kernel(const double *rowsums, int h2, double 
 // noise power and threshold -- src/gpu/fsim/steps/fsim_noise_power.cpp:193-205 (upper median of a
 // full sort, mean = -median/ln 0.5, divided by EM_n(o)) and shaders/fsim/fsim_phase_congruency.glsl:
 // 42-53 (estimated noise energy, tau, T = (mu + k sigma)/1.7 with k = 2); evaluated in FP64.
+constexpr int NOISE_STAGE = 7168;  // 28 KB: 16 KB of histogram beside it stays under 48 KB
 __global__ void __launch_bounds__(1024) fsim_noise_kernel(FsimGroup g) {
     __shared__ unsigned hist[iqm::SELECT_BINS];
+    __shared__ unsigned stage[NOISE_STAGE];  // the median's first-digit bucket, when it fits
     const int q = blockIdx.x;   // img*4 + o
     const int pi = blockIdx.y;
     const int o = q & 3;
     const float *v = g.eo0 + (size_t(pi) * 8 + q) * g.n;
-    const float med = iqm::block_select_kth(v, g.n, g.n / 2, hist);
+    const float med = iqm::block_select_kth(v, g.n, g.n / 2, hist, stage, NOISE_STAGE);
     if (threadIdx.x == 0) {
         const double mean = -double(med) / log(0.5);
         const double np = mean / g.consts[o];

@@ -4,7 +4,7 @@
 //   M-SVD median of block distances  (src/gpu/svd/svd.cpp:140-144)
 //   FSIM noise median of |EO|^2      (src/gpu/fsim/steps/fsim_noise_power.cpp:193-203)
 // For non-negative IEEE floats the bit pattern read as uint32 orders exactly like the value, so a
-// three-pass radix select (11 + 11 + 10 bits) over those patterns returns the same element a full
+// three-digit radix select (12 + 10 + 10 bits) over those patterns returns the same element a full
 // ascending sort would put at index k.
 #pragma once
 
@@ -12,65 +12,152 @@
 
 namespace iqm {
 
-constexpr int SELECT_BINS = 2048;
+constexpr int SELECT_BINS = 4096;
+
+namespace detail {
+
+// Calls f(bits, valid) for every element of v[0..n), four per thread and iteration (one 16-byte
+// load when v is 16-byte aligned and the quad is whole).  The trip count is the same for all threads
+// of the block, so f may use full-warp intrinsics; `valid` is false for the padding past n.
+template <typename F>
+__device__ __forceinline__ void for_each_quad(const float *__restrict__ v, int n, F f) {
+    const int nq = (n + 3) >> 2;
+    const bool aligned = (reinterpret_cast<uintptr_t>(v) & 15u) == 0;
+    for (int b0 = 0; b0 < nq; b0 += blockDim.x) {
+        const int q = b0 + threadIdx.x;
+        unsigned u[4] = {0u, 0u, 0u, 0u};
+        bool ok[4] = {false, false, false, false};
+        if (q < nq) {
+            const int i = 4 * q;
+            if (aligned && i + 4 <= n) {
+                const uint4 t = __ldcg(reinterpret_cast<const uint4 *>(v) + q);
+                u[0] = t.x;
+                u[1] = t.y;
+                u[2] = t.z;
+                u[3] = t.w;
+                ok[0] = ok[1] = ok[2] = ok[3] = true;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    if (i + j < n) {
+                        u[j] = __float_as_uint(__ldcg(v + i + j));
+                        ok[j] = true;
+                    }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) f(u[j], ok[j]);
+    }
+}
+
+// Block-wide: finds the digit (bits >> sh) & dm of the k-th smallest element among those whose bits
+// match `prefix` under `mask`, given their histogram of that digit in hist[]; updates the shared
+// prefix, mask and k.
+__device__ __forceinline__ void select_digit(const unsigned *hist, int bins, int sh, unsigned dm, unsigned prefix,
+                                             unsigned mask, unsigned *s_prefix, unsigned *s_mask, unsigned *s_k,
+                                             unsigned *s_warp_tot) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    // exclusive scan over bins: each thread owns a contiguous run of bins
+    const int per = (bins + nt - 1) / nt;
+    const int b0 = tid * per;
+    unsigned local = 0;
+    for (int b = b0; b < b0 + per && b < bins; b++) local += hist[b];
+    unsigned incl = local;
+    const int lane = tid & 31, wid = tid >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_warp_tot[wid] = incl;
+    __syncthreads();
+    unsigned before = 0;
+    for (int w = 0; w < wid; w++) before += s_warp_tot[w];
+    unsigned run = before + incl - local;  // count of values in bins < b0
+    const unsigned kk = *s_k;
+    __syncthreads();
+    if (kk >= run && kk < run + local) {
+        for (int b = b0; b < b0 + per && b < bins; b++) {
+            const unsigned c = hist[b];
+            if (kk < run + c) {
+                *s_prefix = prefix | (unsigned(b) << sh);
+                *s_mask = mask | (dm << sh);
+                *s_k = kk - run;
+                break;
+            }
+            run += c;
+        }
+    }
+    __syncthreads();
+}
+
+}  // namespace detail
 
 // Block-wide: returns the k-th smallest (0-based) of v[0..n) (all >= 0, no NaN).  `hist` is a
-// shared array of SELECT_BINS counters.  Must be called by every thread of the block; blockDim.x
-// must be a multiple of 32 and at most 1024.
-__device__ inline float block_select_kth(const float *__restrict__ v, int n, int k, unsigned *hist) {
-    __shared__ unsigned s_prefix, s_mask, s_k;
+// shared array of SELECT_BINS counters.  With a shared buffer `buf` of `cap` words, the elements
+// of the first digit's bucket are gathered there when they fit, and the last two digits are
+// selected from shared memory (two reads of v instead of three).  Must be called by every thread
+// of the block; blockDim.x must be a multiple of 32 and at most 1024.
+__device__ inline float block_select_kth(const float *__restrict__ v, int n, int k, unsigned *hist,
+                                         unsigned *buf = nullptr, int cap = 0) {
+    __shared__ unsigned s_prefix, s_mask, s_k, s_count;
     __shared__ unsigned s_warp_tot[32];
     const int tid = threadIdx.x, nt = blockDim.x;
     if (tid == 0) {
         s_prefix = 0u;
         s_mask = 0u;
         s_k = unsigned(k);
+        s_count = 0u;
     }
-    const int shifts[3] = {21, 10, 0};
-    const unsigned digit_masks[3] = {0x7ffu, 0x7ffu, 0x3ffu};
-    for (int pass = 0; pass < 3; pass++) {
+    constexpr int shifts[3] = {20, 10, 0};
+    constexpr unsigned digit_masks[3] = {0xfffu, 0x3ffu, 0x3ffu};
+    // first digit over v
+    for (int b = tid; b < SELECT_BINS; b += nt) hist[b] = 0u;
+    __syncthreads();
+    detail::for_each_quad(v, n, [&](unsigned u, bool ok) {
+        if (ok) atomicAdd(&hist[u >> shifts[0]], 1u);
+    });
+    __syncthreads();
+    detail::select_digit(hist, SELECT_BINS, shifts[0], digit_masks[0], 0u, 0u, &s_prefix, &s_mask, &s_k, s_warp_tot);
+    const unsigned bucket = s_prefix >> shifts[0];
+    const bool staged = buf != nullptr && hist[bucket] <= unsigned(cap);  // uniform across the block
+    __syncthreads();
+    int m = n;
+    if (staged) {
+        // gather the bucket (warp-aggregated slots; hist[bucket] <= cap bounds every index)
+        const int lane = tid & 31;
+        detail::for_each_quad(v, n, [&](unsigned u, bool ok) {
+            const bool take = ok && (u >> shifts[0]) == bucket;
+            const unsigned ballot = __ballot_sync(0xffffffffu, take);
+            if (ballot == 0u) return;
+            const int leader = __ffs(ballot) - 1;
+            unsigned base = 0u;
+            if (lane == leader) base = atomicAdd(&s_count, unsigned(__popc(ballot)));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (take) buf[base + __popc(ballot & ((1u << lane) - 1u))] = u;
+        });
+        __syncthreads();
+        m = int(s_count);
+    }
+#pragma unroll
+    for (int pass = 1; pass < 3; pass++) {
         const int sh = shifts[pass];
         const unsigned dm = digit_masks[pass];
         for (int b = tid; b < SELECT_BINS; b += nt) hist[b] = 0u;
         __syncthreads();
         const unsigned prefix = s_prefix, mask = s_mask;
-        for (int i = tid; i < n; i += nt) {
-            const unsigned u = __float_as_uint(v[i]);
-            if ((u & mask) == prefix) atomicAdd(&hist[(u >> sh) & dm], 1u);
-        }
-        __syncthreads();
-        // exclusive scan over bins: each thread owns a contiguous run of bins
-        const int per = (SELECT_BINS + nt - 1) / nt;
-        const int b0 = tid * per;
-        unsigned local = 0;
-        for (int b = b0; b < b0 + per && b < SELECT_BINS; b++) local += hist[b];
-        unsigned incl = local;
-        const int lane = tid & 31, wid = tid >> 5;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        if (lane == 31) s_warp_tot[wid] = incl;
-        __syncthreads();
-        unsigned before = 0;
-        for (int w = 0; w < wid; w++) before += s_warp_tot[w];
-        unsigned run = before + incl - local;  // count of values in bins < b0
-        const unsigned kk = s_k;
-        __syncthreads();
-        if (kk >= run && kk < run + local) {
-            for (int b = b0; b < b0 + per && b < SELECT_BINS; b++) {
-                const unsigned c = hist[b];
-                if (kk < run + c) {
-                    s_prefix = prefix | (unsigned(b) << sh);
-                    s_mask = mask | (dm << sh);
-                    s_k = kk - run;
-                    break;
-                }
-                run += c;
+        if (staged) {
+            for (int i = tid; i < m; i += nt) {
+                const unsigned u = buf[i];
+                if ((u & mask) == prefix) atomicAdd(&hist[(u >> sh) & dm], 1u);
             }
+        } else {
+            detail::for_each_quad(v, n, [&](unsigned u, bool ok) {
+                if (ok && (u & mask) == prefix) atomicAdd(&hist[(u >> sh) & dm], 1u);
+            });
         }
         __syncthreads();
+        detail::select_digit(hist, int(dm) + 1, sh, dm, prefix, mask, &s_prefix, &s_mask, &s_k, s_warp_tot);
     }
     return __uint_as_float(s_prefix);
 }

@@ -56,6 +56,19 @@ def test_fsim_batch_uneven_matches_single(rt, o64):
         assert abs(g[0] - w64[0]) <= TOL and abs(g[1] - w64[1]) <= TOL
 
 
+@pytest.mark.parametrize("count", [3, 9])
+def test_fsim_same_size_batch_matches_single(rt, count):
+    # 1080p planes take one pair per inverse-pass chunk when several chunks are in flight, and
+    # consecutive chunks alternate between two streams.  Every pair's arithmetic is the same in all
+    # schedules, so the scores are identical.
+    pairs = [synth.rgb_gain_pair(1080, 1920, config=1, pair=i) for i in range(count)]
+    f = iqm_b200.FSIM(rt)
+    got = f.compute_batch(pairs)
+    for (a, b), g in zip(pairs, got):
+        single = f.compute_metric(a, b)
+        assert g[0] == single.fsim and g[1] == single.fsimc
+
+
 def test_fsim_deterministic(rt):
     a, b = synth.rgb_gain_pair(270, 480, config=1, pair=5)
     f = iqm_b200.FSIM(rt)
