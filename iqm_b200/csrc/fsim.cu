@@ -732,14 +732,103 @@ __device__ __forceinline__ float grad_at(const float *Y, int x, int y, int w2, i
     return sqrtf(a * a + b * b);
 }
 
+// Similarity terms of one pixel from the two images' phase congruency, gradient magnitude and
+// chroma (fsim_final_multiply.glsl:18-58).
+__device__ __forceinline__ void similarity_terms(float pc1, float pc2, float g1, float g2, float i1, float i2, float q1,
+                                                 float q2, double &s_pcm, double &s_sim, double &s_simc) {
+    const float pcm = fmaxf(pc1, pc2);
+    const float pcsim = (2.0f * pc1 * pc2 + 0.85f) / (pc1 * pc1 + pc2 * pc2 + 0.85f);
+    const float gsim = (2.0f * g1 * g2 + 160.0f) / (g1 * g1 + g2 * g2 + 160.0f);
+    const float isim = (2.0f * i1 * i2 + 200.0f) / (i1 * i1 + i2 * i2 + 200.0f);
+    const float qsim = (2.0f * q1 * q2 + 200.0f) / (q1 * q1 + q2 * q2 + 200.0f);
+    const float sim = gsim * pcsim * pcm;
+    const float simc = gsim * pcsim * powf(fabsf(isim * qsim), 0.03f) * pcm;
+    s_pcm += pcm;
+    s_sim += sim;
+    s_simc += simc;
+}
+
+// PX pixels per thread: 1, or 4 consecutive pixels of one row read with 16-byte loads (w2 a
+// multiple of 4, so every plane starts 16-byte aligned and no quad crosses a row).
+template <int PX>
 __global__ void __launch_bounds__(FT) fsim_final_kernel(FsimGroup g) {
     __shared__ double red[3][FT / 32];
     __shared__ int is_last;
     const int pi = blockIdx.y;
-    const int p = blockIdx.x * FT + threadIdx.x;
+    const int p = (blockIdx.x * FT + threadIdx.x) * PX;
     const int n = g.n;
     double s_pcm = 0.0, s_sim = 0.0, s_simc = 0.0;
-    if (p < n) {
+    if constexpr (PX == 4) {
+        if (p < n) {
+            const int w2 = g.w2, h2 = g.h2;
+            const int x0 = p % w2, y = p / w2;
+            float pc[2][4], gm[2][4], iv[2][4], qv[2][4];
+#pragma unroll
+            for (int img = 0; img < 2; img++) {
+                float et[4] = {0.f, 0.f, 0.f, 0.f}, at[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                for (int o = 0; o < 4; o++) {
+                    const size_t plane = (size_t(pi) * 8 + img * 4 + o) * n;
+                    const float4 e = __ldcs(reinterpret_cast<const float4 *>(g.energy + plane + p));
+                    const float4 a = __ldcs(reinterpret_cast<const float4 *>(g.amp + plane + p));
+                    const float t = g.thr[size_t(pi) * 8 + img * 4 + o];
+                    et[0] += fmaxf(e.x - t, 0.f);
+                    et[1] += fmaxf(e.y - t, 0.f);
+                    et[2] += fmaxf(e.z - t, 0.f);
+                    et[3] += fmaxf(e.w - t, 0.f);
+                    at[0] += a.x;
+                    at[1] += a.y;
+                    at[2] += a.z;
+                    at[3] += a.w;
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++) pc[img][j] = et[j] / at[j];
+                const float *yiq = g.yiq + size_t(pi * 2 + img) * 3 * n;
+                const float4 i4 = *reinterpret_cast<const float4 *>(yiq + p);
+                const float4 q4 = *reinterpret_cast<const float4 *>(yiq + n + p);
+                iv[img][0] = i4.x, iv[img][1] = i4.y, iv[img][2] = i4.z, iv[img][3] = i4.w;
+                qv[img][0] = q4.x, qv[img][1] = q4.y, qv[img][2] = q4.z, qv[img][3] = q4.w;
+                // 3 x 6 luma window around the quad, zero outside the plane (grad_at's skipped samples)
+                const float *Y = yiq + 2 * n;
+                float win[3][6];
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    const int py = y + r - 1;
+                    if (py >= 0 && py < h2) {
+                        const float *row = Y + size_t(py) * w2;
+                        const float4 c = *reinterpret_cast<const float4 *>(row + x0);
+                        win[r][0] = x0 > 0 ? row[x0 - 1] : 0.f;
+                        win[r][1] = c.x, win[r][2] = c.y, win[r][3] = c.z, win[r][4] = c.w;
+                        win[r][5] = x0 + 4 < w2 ? row[x0 + 4] : 0.f;
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 6; c++) win[r][c] = 0.f;
+                    }
+                }
+                const float vert[9] = {3.f, 0.f, -3.f, 10.f, 0.f, -10.f, 3.f, 0.f, -3.f};
+                const float hor[9] = {3.f, 10.f, 3.f, 0.f, 0.f, 0.f, -3.f, -10.f, -3.f};
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    float vs = 0.f, hs = 0.f;
+#pragma unroll
+                    for (int dj = -1; dj < 2; dj++)
+#pragma unroll
+                        for (int dk = -1; dk < 2; dk++) {
+                            const float v = win[dk + 1][q + 1 + dj];
+                            const int idx = (dj + 1) + (dk + 1) * 3;
+                            vs += v * vert[idx];
+                            hs += v * hor[idx];
+                        }
+                    const float a = vs / 16.0f, b = hs / 16.0f;
+                    gm[img][q] = sqrtf(a * a + b * b);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                similarity_terms(pc[0][q], pc[1][q], gm[0][q], gm[1][q], iv[0][q], iv[1][q], qv[0][q], qv[1][q], s_pcm,
+                                 s_sim, s_simc);
+        }
+    } else if (p < n) {
         float pc[2];
 #pragma unroll
         for (int img = 0; img < 2; img++) {
@@ -753,23 +842,12 @@ __global__ void __launch_bounds__(FT) fsim_final_kernel(FsimGroup g) {
             }
             pc[img] = et / at;
         }
-        const float pc1 = pc[0], pc2 = pc[1];
-        const float pcm = fmaxf(pc1, pc2);
-        const float pcsim = (2.0f * pc1 * pc2 + 0.85f) / (pc1 * pc1 + pc2 * pc2 + 0.85f);
         const int x = p % g.w2, y = p / g.w2;
         const float *yiq1 = g.yiq + size_t(pi * 2 + 0) * 3 * n;
         const float *yiq2 = g.yiq + size_t(pi * 2 + 1) * 3 * n;
         const float g1 = grad_at(yiq1 + 2 * n, x, y, g.w2, g.h2);
         const float g2 = grad_at(yiq2 + 2 * n, x, y, g.w2, g.h2);
-        const float gsim = (2.0f * g1 * g2 + 160.0f) / (g1 * g1 + g2 * g2 + 160.0f);
-        const float i1 = yiq1[p], i2 = yiq2[p], q1 = yiq1[n + p], q2 = yiq2[n + p];
-        const float isim = (2.0f * i1 * i2 + 200.0f) / (i1 * i1 + i2 * i2 + 200.0f);
-        const float qsim = (2.0f * q1 * q2 + 200.0f) / (q1 * q1 + q2 * q2 + 200.0f);
-        const float sim = gsim * pcsim * pcm;
-        const float simc = gsim * pcsim * powf(fabsf(isim * qsim), 0.03f) * pcm;
-        s_pcm = pcm;
-        s_sim = sim;
-        s_simc = simc;
+        similarity_terms(pc[0], pc[1], g1, g2, yiq1[p], yiq2[p], yiq1[n + p], yiq2[n + p], s_pcm, s_sim, s_simc);
     }
     double v[3] = {s_pcm, s_sim, s_simc};
 #pragma unroll
@@ -788,7 +866,7 @@ __global__ void __launch_bounds__(FT) fsim_final_kernel(FsimGroup g) {
     if (threadIdx.x == 0) {
         __threadfence();
         const unsigned prev = atomicAdd(&g.counters[pi], 1u);
-        is_last = prev == unsigned(g.tiles - 1);
+        is_last = prev == gridDim.x - 1;
     }
     __syncthreads();
     if (!is_last) return;
@@ -796,7 +874,7 @@ __global__ void __launch_bounds__(FT) fsim_final_kernel(FsimGroup g) {
     {
         double t[3] = {0.0, 0.0, 0.0};
         const double *pp = g.partials + size_t(pi) * g.tiles * 3;
-        for (int i = threadIdx.x; i < g.tiles; i += FT)
+        for (int i = threadIdx.x; i < int(gridDim.x); i += FT)
 #pragma unroll
             for (int q = 0; q < 3; q++) t[q] += __ldcg(pp + size_t(i) * 3 + q);
         __syncthreads();
@@ -1245,7 +1323,10 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
         }
         fsim_noise_kernel<<<dim3(8, G), 1024, 0, st>>>(g);
         iqm::check_launch(ctx, "fsim_noise_kernel");
-        fsim_final_kernel<<<dim3(tiles, G), FT, 0, st>>>(g);
+        if (w2 % 4 == 0)
+            fsim_final_kernel<4><<<dim3(int(iqm::ceil_div(n, 4 * FT)), G), FT, 0, st>>>(g);
+        else
+            fsim_final_kernel<1><<<dim3(tiles, G), FT, 0, st>>>(g);
         iqm::check_launch(ctx, "fsim_final_kernel");
     }
     if (S > 1) {
