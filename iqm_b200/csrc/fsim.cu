@@ -687,7 +687,8 @@ __global__ void fsim_consts_reduce_kernel(const double *rowsums, int h2, double 
 // full sort, mean = -median/ln 0.5, divided by EM_n(o)) and shaders/fsim/fsim_phase_congruency.glsl:
 // 42-53 (estimated noise energy, tau, T = (mu + k sigma)/1.7 with k = 2); evaluated in FP64.
 constexpr int NOISE_STAGE = 7168;  // 28 KB: 16 KB of histogram beside it stays under 48 KB
-__global__ void __launch_bounds__(1024) fsim_noise_kernel(FsimGroup g) {
+// two CTAs per SM: 8 planes x 32 pairs run in one wave on 148 SMs
+__global__ void __launch_bounds__(1024, 2) fsim_noise_kernel(FsimGroup g) {
     __shared__ unsigned hist[iqm::SELECT_BINS];
     __shared__ unsigned stage[NOISE_STAGE];  // the median's first-digit bucket, when it fits
     const int q = blockIdx.x;   // img*4 + o

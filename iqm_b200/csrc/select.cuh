@@ -16,37 +16,42 @@ constexpr int SELECT_BINS = 4096;
 
 namespace detail {
 
-// Calls f(bits, valid) for every element of v[0..n), four per thread and iteration (one 16-byte
-// load when v is 16-byte aligned and the quad is whole).  The trip count is the same for all threads
-// of the block, so f may use full-warp intrinsics; `valid` is false for the padding past n.
+// Calls f(bits, valid) for every element of v[0..n): each thread takes SELECT_UNROLL quads per
+// iteration, issuing their loads (16-byte loads when v is 16-byte aligned and the quad is whole)
+// before any call.  The trip count is the same for all threads of the block, so f may use
+// full-warp intrinsics; `valid` is false for the padding past n, which carries the bit pattern
+// 0xffffffff (a negative NaN, never among the non-negative inputs).
+constexpr int SELECT_UNROLL = 2;  // two quads in flight per thread fit 32 registers
+constexpr unsigned SELECT_PAD = 0xffffffffu;
 template <typename F>
 __device__ __forceinline__ void for_each_quad(const float *__restrict__ v, int n, F f) {
     const int nq = (n + 3) >> 2;
     const bool aligned = (reinterpret_cast<uintptr_t>(v) & 15u) == 0;
-    for (int b0 = 0; b0 < nq; b0 += blockDim.x) {
-        const int q = b0 + threadIdx.x;
-        unsigned u[4] = {0u, 0u, 0u, 0u};
-        bool ok[4] = {false, false, false, false};
-        if (q < nq) {
-            const int i = 4 * q;
-            if (aligned && i + 4 <= n) {
-                const uint4 t = __ldcg(reinterpret_cast<const uint4 *>(v) + q);
-                u[0] = t.x;
-                u[1] = t.y;
-                u[2] = t.z;
-                u[3] = t.w;
-                ok[0] = ok[1] = ok[2] = ok[3] = true;
-            } else {
+    for (int b0 = 0; b0 < nq; b0 += SELECT_UNROLL * blockDim.x) {
+        uint4 u[SELECT_UNROLL];
 #pragma unroll
-                for (int j = 0; j < 4; j++)
-                    if (i + j < n) {
-                        u[j] = __float_as_uint(__ldcg(v + i + j));
-                        ok[j] = true;
-                    }
+        for (int r = 0; r < SELECT_UNROLL; r++) {
+            const int q = b0 + r * blockDim.x + threadIdx.x;
+            const int i = 4 * q;
+            u[r] = make_uint4(SELECT_PAD, SELECT_PAD, SELECT_PAD, SELECT_PAD);
+            if (q < nq) {
+                if (aligned && i + 4 <= n) {
+                    u[r] = __ldcg(reinterpret_cast<const uint4 *>(v) + q);
+                } else {
+                    if (i < n) u[r].x = __float_as_uint(__ldcg(v + i));
+                    if (i + 1 < n) u[r].y = __float_as_uint(__ldcg(v + i + 1));
+                    if (i + 2 < n) u[r].z = __float_as_uint(__ldcg(v + i + 2));
+                    if (i + 3 < n) u[r].w = __float_as_uint(__ldcg(v + i + 3));
+                }
             }
         }
 #pragma unroll
-        for (int j = 0; j < 4; j++) f(u[j], ok[j]);
+        for (int r = 0; r < SELECT_UNROLL; r++) {
+            f(u[r].x, u[r].x != SELECT_PAD);
+            f(u[r].y, u[r].y != SELECT_PAD);
+            f(u[r].z, u[r].z != SELECT_PAD);
+            f(u[r].w, u[r].w != SELECT_PAD);
+        }
     }
 }
 
