@@ -8,9 +8,11 @@
 //
 // Here, per group of pairs with the same W'xH', seven kernels:
 //   fsim_ingest_kernel      full-resolution RGBA8 -> I, Q, Y planes of both images (box F x F)
-//   fsim_fwd_rows_kernel    forward FFT along x of the two luma planes (shared-memory Stockham)
+//   fsim_fwd_rows_kernel    forward FFT along x of a pair's two luma planes packed as one complex
+//                           plane Y_img + i Y_ref (shared-memory Stockham)
 //   fsim_fwd_cols_kernel    forward FFT along y
-//   fsim_inv_cols_kernel    spectrum x log-Gabor_s x angular_o, inverse FFT along y (32 planes)
+//   fsim_inv_cols_kernel    each image's spectrum separated from the packed one (Hermitian halves),
+//                           x log-Gabor_s x angular_o, inverse FFT along y (32 planes)
 //   fsim_inv_rows_kernel    inverse FFT along x of the 4 scales of one orientation, scaled 1/N,
 //                           fused with the response sums of fsim_sum_filter_responses.glsl and
 //                           the |EO(s=0)|^2 values of fsim_pack_for_median.glsl
@@ -73,7 +75,7 @@ struct FsimGroup {
     int pair0;      // group index of the first pair of this launch (inverse-pass chunks)
     int w2, h2, n;
     float *yiq;     // G x 2 x 3 x n   (I, Q, Y)
-    float2 *spec;   // G x 2 x n
+    float2 *spec;   // G x n: per pair the spectrum of Y_img + i Y_ref
     float2 *T;      // chunk x 2 x 16 x n  (after the column pass of the inverse transform)
     float *amp;     // G x 8 x n       (img*4 + o)
     float *energy;  // G x 8 x n
@@ -323,16 +325,19 @@ __global__ void __launch_bounds__(FT, 1) fsim_fwd_rows_kernel(FsimGroup g, const
     __syncthreads();
     float2 *work = sm + ((tl + 1) & ~1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int plane = blockIdx.y;  // pair*2 + img
+    // the two real luma planes of a pair transform together as one complex plane Y_img + i Y_ref
+    const int pair = blockIdx.y;
     const int y0 = (blockIdx.x * (blockDim.x >> 5) + warp) * NB;
     if (y0 >= g.h2) return;  // warp-uniform; no block-wide barrier follows
     const int nb = min(NB, g.h2 - y0);
     float2 *a = warp_area<Eng>(work, warp, wl), *b = a + NB * wl;
-    const float *Y = g.yiq + (size_t(plane) * 3 + 2) * g.n + size_t(y0) * g.w2;
+    const float *Y1 = g.yiq + (size_t(pair * 2) * 3 + 2) * g.n + size_t(y0) * g.w2;
+    const float *Y2 = Y1 + size_t(3) * g.n;  // the pair's second image
     for (int t = 0; t < nb; t++)
-        for (int x = lane; x < g.w2; x += 32) a[t * wl + x] = make_float2(Y[size_t(t) * g.w2 + x], 0.f);
+        for (int x = lane; x < g.w2; x += 32)
+            a[t * wl + x] = make_float2(Y1[size_t(t) * g.w2 + x], Y2[size_t(t) * g.w2 + x]);
     const float2 *res = Eng::run(a, b, L, sm, -1.f, wl);
-    float2 *S = g.spec + size_t(plane) * g.n + size_t(y0) * g.w2;
+    float2 *S = g.spec + size_t(pair) * g.n + size_t(y0) * g.w2;
     for (int t = 0; t < nb; t++)
         for (int x = lane; x < g.w2; x += 32) S[size_t(t) * g.w2 + x] = res[t * wl + x];
 }
@@ -349,10 +354,10 @@ __global__ void __launch_bounds__(FT, 1) fsim_fwd_cols_kernel(FsimGroup g, const
     iqm::stage_twiddles_to_shared(L, sm);
     float2 *work = sm + ((tl + 1) & ~1);
     const int nw = 1 << lw, cols = NB * nw, warp = threadIdx.x >> 5;
-    const int plane = blockIdx.y;
+    const int pair = blockIdx.y;
     const int x0 = blockIdx.x * cols;
     const int nc = min(cols, g.w2 - x0);
-    float2 *S = g.spec + size_t(plane) * g.n;
+    float2 *S = g.spec + size_t(pair) * g.n;
     // column c lives in warp c / NB, slot c % NB
     for (int idx = threadIdx.x; idx < cols * g.h2; idx += blockDim.x) {
         const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
@@ -393,7 +398,8 @@ fsim_inv_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int 
     const int h2 = g.h2;
     float2 *Sl = sm + ((tl + 1) & ~1);     // cols x h2 spectrum slab (column-major)
     float2 *work = Sl + size_t(cols) * h2;  // per warp: a, b of NB x wl each
-    const float2 *src = g.spec + size_t(g.pair0 * 2 + plane) * g.n;
+    const int img = plane & 1;
+    const float2 *src = g.spec + size_t(g.pair0 + (plane >> 1)) * g.n;  // the pair's packed spectrum
     const int nbw = min(NB, nc - warp * NB);
     // With a fixed-length engine (h2 == PN) each lane holds its share of the warp's filter column in
     // registers, and the next scale's share is loaded while this scale's transform runs.
@@ -411,7 +417,17 @@ fsim_inv_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int 
     if (PN > 0 && nbw > 0) load_filter(o * 4);
     for (int idx = threadIdx.x; idx < cols * h2; idx += blockDim.x) {
         const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
-        if (c < nc) Sl[size_t(c) * h2 + y] = consts_mode ? make_float2(1.f, 0.f) : src[size_t(y) * g.w2 + x0 + c];
+        if (c >= nc) continue;
+        float2 v = make_float2(1.f, 0.f);
+        if (!consts_mode) {
+            const int x = x0 + c;
+            // Z = F(Y_img + i Y_ref): F(Y_img) = (Z(k) + conj Z(-k)) / 2, F(Y_ref) = (Z(k) - conj Z(-k)) / 2i
+            const float2 z = src[size_t(y) * g.w2 + x];
+            const float2 m = src[size_t(y ? h2 - y : 0) * g.w2 + (x ? g.w2 - x : 0)];
+            v = img == 0 ? make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y))
+                         : make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
+        }
+        Sl[size_t(c) * h2 + y] = v;
     }
     __syncthreads();
     for (int s = 0; s < 4; s++) {
@@ -1132,7 +1148,7 @@ Layout layout_for(int G, int chunk, int n, int tiles, int nbuf = 1) {
     Layout L{};
     size_t off = 0;
     L.yiq = off; off += al(sizeof(float) * size_t(G) * 6 * n);
-    L.spec = off; off += al(sizeof(float2) * size_t(G) * 2 * n);
+    L.spec = off; off += al(sizeof(float2) * size_t(G) * n);
     L.T = off; off += al(sizeof(float2) * size_t(nbuf) * chunk * 32 * n);
     L.planes = off; off += al(sizeof(float) * size_t(G) * 24 * n);
     L.thr = off; off += al(sizeof(float) * size_t(G) * 8);
@@ -1289,13 +1305,13 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
         iqm::check_launch(ctx, "fsim_ingest_kernel");
         with_engine(s.row_eng, [&](auto e) {
             fsim_fwd_rows_kernel<decltype(e)>
-                <<<dim3(iqm::ceil_div(h2, NB << s.lw_rows), 2 * G), 32 << s.lw_rows, s.sm_rows, st>>>(g, P->row,
+                <<<dim3(iqm::ceil_div(h2, NB << s.lw_rows), G), 32 << s.lw_rows, s.sm_rows, st>>>(g, P->row,
                                                                                                     s.wl_row);
         });
         iqm::check_launch(ctx, "fsim_fwd_rows_kernel");
         with_engine(s.col_eng, [&](auto e) {
             fsim_fwd_cols_kernel<decltype(e)>
-                <<<dim3(iqm::ceil_div(w2, NB << s.lw_fcols), 2 * G), 32 << s.lw_fcols, s.sm_fcols, st>>>(
+                <<<dim3(iqm::ceil_div(w2, NB << s.lw_fcols), G), 32 << s.lw_fcols, s.sm_fcols, st>>>(
                     g, P->col, s.wl_col, s.lw_fcols);
         });
         iqm::check_launch(ctx, "fsim_fwd_cols_kernel");
