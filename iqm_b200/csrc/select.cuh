@@ -16,41 +16,87 @@ constexpr int SELECT_BINS = 4096;
 
 namespace detail {
 
-// Calls f(bits, valid) for every element of v[0..n): each thread takes SELECT_UNROLL quads per
-// iteration, issuing their loads (16-byte loads when v is 16-byte aligned and the quad is whole)
-// before any call.  The trip count is the same for all threads of the block, so f may use
-// full-warp intrinsics; `valid` is false for the padding past n, which carries the bit pattern
-// 0xffffffff (a negative NaN, never among the non-negative inputs).
 constexpr int SELECT_UNROLL = 2;  // two quads in flight per thread fit 32 registers
+// Padding past n: the bit pattern of a negative NaN, never among the non-negative inputs.
 constexpr unsigned SELECT_PAD = 0xffffffffu;
+
+// Loads the thread's SELECT_UNROLL quads of the block iteration starting at quad b0 (16-byte loads
+// when v is 16-byte aligned and the quad is whole; SELECT_PAD past n).
+__device__ __forceinline__ void load_quads(const float *__restrict__ v, int n, int nq, bool aligned, int b0,
+                                           uint4 (&u)[SELECT_UNROLL]) {
+#pragma unroll
+    for (int r = 0; r < SELECT_UNROLL; r++) {
+        const int q = b0 + r * blockDim.x + threadIdx.x;
+        const int i = 4 * q;
+        u[r] = make_uint4(SELECT_PAD, SELECT_PAD, SELECT_PAD, SELECT_PAD);
+        if (q < nq) {
+            if (aligned && i + 4 <= n) {
+                u[r] = __ldcg(reinterpret_cast<const uint4 *>(v) + q);
+            } else {
+                if (i < n) u[r].x = __float_as_uint(__ldcg(v + i));
+                if (i + 1 < n) u[r].y = __float_as_uint(__ldcg(v + i + 1));
+                if (i + 2 < n) u[r].z = __float_as_uint(__ldcg(v + i + 2));
+                if (i + 3 < n) u[r].w = __float_as_uint(__ldcg(v + i + 3));
+            }
+        }
+    }
+}
+
+// Calls f(bits, valid) for every element of v[0..n), each thread's loads of an iteration issued
+// before any call; `valid` is false for the padding.  The trip count is the same for all threads of
+// the block, so f may use full-warp intrinsics.
 template <typename F>
 __device__ __forceinline__ void for_each_quad(const float *__restrict__ v, int n, F f) {
     const int nq = (n + 3) >> 2;
     const bool aligned = (reinterpret_cast<uintptr_t>(v) & 15u) == 0;
     for (int b0 = 0; b0 < nq; b0 += SELECT_UNROLL * blockDim.x) {
         uint4 u[SELECT_UNROLL];
-#pragma unroll
-        for (int r = 0; r < SELECT_UNROLL; r++) {
-            const int q = b0 + r * blockDim.x + threadIdx.x;
-            const int i = 4 * q;
-            u[r] = make_uint4(SELECT_PAD, SELECT_PAD, SELECT_PAD, SELECT_PAD);
-            if (q < nq) {
-                if (aligned && i + 4 <= n) {
-                    u[r] = __ldcg(reinterpret_cast<const uint4 *>(v) + q);
-                } else {
-                    if (i < n) u[r].x = __float_as_uint(__ldcg(v + i));
-                    if (i + 1 < n) u[r].y = __float_as_uint(__ldcg(v + i + 1));
-                    if (i + 2 < n) u[r].z = __float_as_uint(__ldcg(v + i + 2));
-                    if (i + 3 < n) u[r].w = __float_as_uint(__ldcg(v + i + 3));
-                }
-            }
-        }
+        load_quads(v, n, nq, aligned, b0, u);
 #pragma unroll
         for (int r = 0; r < SELECT_UNROLL; r++) {
             f(u[r].x, u[r].x != SELECT_PAD);
             f(u[r].y, u[r].y != SELECT_PAD);
             f(u[r].z, u[r].z != SELECT_PAD);
             f(u[r].w, u[r].w != SELECT_PAD);
+        }
+    }
+}
+
+// Block-wide: appends every element of v[0..n) whose bits >> sh equal `digit` to buf (in no
+// particular order), counting in *count.  Each thread counts its matches among its quads, a warp scan
+// turns the counts into slots, and one atomic per warp and iteration reserves them.  The caller
+// guarantees that the matches fit buf.
+__device__ __forceinline__ void gather_digit(const float *__restrict__ v, int n, int sh, unsigned digit,
+                                             unsigned *buf, unsigned *count) {
+    const int nq = (n + 3) >> 2;
+    const bool aligned = (reinterpret_cast<uintptr_t>(v) & 15u) == 0;
+    const int lane = threadIdx.x & 31;
+    auto hit = [&](unsigned x) { return x != SELECT_PAD && (x >> sh) == digit; };
+    for (int b0 = 0; b0 < nq; b0 += SELECT_UNROLL * blockDim.x) {
+        uint4 u[SELECT_UNROLL];
+        load_quads(v, n, nq, aligned, b0, u);
+        unsigned cnt = 0;
+#pragma unroll
+        for (int r = 0; r < SELECT_UNROLL; r++)
+            cnt += unsigned(hit(u[r].x)) + unsigned(hit(u[r].y)) + unsigned(hit(u[r].z)) + unsigned(hit(u[r].w));
+        unsigned incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
+        if (total == 0u) continue;  // warp-uniform
+        unsigned base = 0u;
+        if (lane == 31) base = atomicAdd(count, total);
+        unsigned pos = __shfl_sync(0xffffffffu, base, 31) + incl - cnt;
+        if (cnt == 0u) continue;
+#pragma unroll
+        for (int r = 0; r < SELECT_UNROLL; r++) {
+            if (hit(u[r].x)) buf[pos++] = u[r].x;
+            if (hit(u[r].y)) buf[pos++] = u[r].y;
+            if (hit(u[r].z)) buf[pos++] = u[r].z;
+            if (hit(u[r].w)) buf[pos++] = u[r].w;
         }
     }
 }
@@ -129,18 +175,8 @@ __device__ inline float block_select_kth(const float *__restrict__ v, int n, int
     __syncthreads();
     int m = n;
     if (staged) {
-        // gather the bucket (warp-aggregated slots; hist[bucket] <= cap bounds every index)
-        const int lane = tid & 31;
-        detail::for_each_quad(v, n, [&](unsigned u, bool ok) {
-            const bool take = ok && (u >> shifts[0]) == bucket;
-            const unsigned ballot = __ballot_sync(0xffffffffu, take);
-            if (ballot == 0u) return;
-            const int leader = __ffs(ballot) - 1;
-            unsigned base = 0u;
-            if (lane == leader) base = atomicAdd(&s_count, unsigned(__popc(ballot)));
-            base = __shfl_sync(0xffffffffu, base, leader);
-            if (take) buf[base + __popc(ballot & ((1u << lane) - 1u))] = u;
-        });
+        // gather the bucket (hist[bucket] <= cap bounds every slot)
+        detail::gather_digit(v, n, shifts[0], bucket, buf, &s_count);
         __syncthreads();
         m = int(s_count);
     }
