@@ -31,6 +31,7 @@
 #include <initializer_list>
 #include <map>
 #include <mutex>
+#include <tuple>
 
 #include "fft.cuh"
 #include "fft_plan.cuh"
@@ -469,6 +470,52 @@ fsim_inv_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int 
     }
 }
 
+// CTA-wide form of the inverse column pass for long columns (runtime-planned lengths whose per-warp
+// work buffers would leave few warps per SM): the whole CTA transforms `cb` adjacent columns at once
+// with the block-level engine, one scale after another; the cb-column slab keeps the global loads and
+// stores in row segments.
+__global__ void __launch_bounds__(FT, 1)
+fsim_inv_cols_seq_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int cb) {
+    extern __shared__ __align__(16) float2 sm[];
+    const int o = blockIdx.y;
+    const int plane = blockIdx.z;  // chunk-local pair*2 + img
+    const int img = plane & 1;
+    const int w2 = g.w2, h2 = g.h2;
+    const int x0 = blockIdx.x * cb;
+    const int nc = min(cb, w2 - x0);
+    float2 *Sl = sm;                   // nc x h2 separated spectrum (column-major)
+    float2 *a = Sl + size_t(cb) * h2;  // nc x wl
+    float2 *b = a + size_t(cb) * wl;   // nc x wl
+    const float2 *src = g.spec + size_t(g.pair0 + (plane >> 1)) * g.n;  // the pair's packed spectrum
+    for (int idx = threadIdx.x; idx < nc * h2; idx += blockDim.x) {
+        const int y = idx / nc, c = idx - y * nc;
+        const int x = x0 + c;
+        const float2 z = src[size_t(y) * w2 + x];
+        const float2 m = src[size_t(y ? h2 - y : 0) * w2 + (x ? w2 - x : 0)];
+        Sl[size_t(c) * h2 + y] = img == 0 ? make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y))
+                                          : make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
+    }
+    __syncthreads();
+    for (int s = 0; s < 4; s++) {
+        const int z = o * 4 + s;
+        const float *H = g.filters + size_t(z) * g.n + size_t(x0) * h2;  // column-major filter plane
+        for (int idx = threadIdx.x; idx < nc * h2; idx += blockDim.x) {
+            const int c = idx / h2, y = idx - c * h2;
+            const float hv = __ldg(H + idx);
+            const float2 v = Sl[idx];
+            a[size_t(c) * wl + y] = make_float2(hv * v.x, hv * v.y);
+        }
+        __syncthreads();
+        const float2 *res = iqm::fft_run(a, b, L, 1.f, nc, wl);
+        float2 *dst = g.T + (size_t(plane) * 16 + z) * g.n;
+        for (int idx = threadIdx.x; idx < nc * h2; idx += blockDim.x) {
+            const int y = idx / nc, c = idx - y * nc;
+            dst[size_t(y) * w2 + x0 + c] = res[size_t(c) * wl + y];
+        }
+        __syncthreads();
+    }
+}
+
 // Per-pixel response sums of one orientation from its 4 scales (scaled by 1/N here), as
 // shaders/fsim/fsim_sum_filter_responses.glsl:43-80 and fsim_pack_for_median.glsl:39-43.
 __device__ __forceinline__ void response_sums(const float2 v[4], float invN, float &sA, float &en, float &e0) {
@@ -618,20 +665,26 @@ __global__ void __launch_bounds__(FT, engine_len<Eng>::value ? 4 : 1) fsim_inv_r
 }
 
 // Sequential form of pass 2 for rows too long for four warp buffers (Bluestein lengths): the whole
-// CTA transforms one scale at a time with the block-level engine.
-__global__ void __launch_bounds__(FT, 1) fsim_inv_rows_seq_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int consts_mode,
-                                                               double *rowsums) {
+// CTA transforms `sb` scales at a time (1, 2 or 4) with the block-level engine.
+__global__ void __launch_bounds__(FT, 1) fsim_inv_rows_seq_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int sb,
+                                                               int consts_mode, double *rowsums) {
     extern __shared__ __align__(16) float2 sm[];
     __shared__ double red[4][FT / 32];
     const int y = blockIdx.x, o = blockIdx.y, plane = blockIdx.z;
     const int w2 = g.w2;
     const float2 *src = g.T + (size_t(plane) * 16 + o * 4) * g.n + size_t(y) * w2;
     float2 *keep = sm;  // 4 x w2
-    float2 *a = sm + 4 * w2, *b = a + wl;
-    for (int s = 0; s < 4; s++) {
-        for (int x = threadIdx.x; x < w2; x += FT) a[x] = src[size_t(s) * g.n + x];
-        const float2 *res = iqm::fft_run(a, b, L, 1.f, 1, wl);
-        for (int x = threadIdx.x; x < w2; x += FT) keep[s * w2 + x] = res[x];
+    float2 *a = sm + 4 * w2, *b = a + size_t(sb) * wl;  // sb x wl each
+    for (int s0 = 0; s0 < 4; s0 += sb) {
+        for (int idx = threadIdx.x; idx < sb * w2; idx += FT) {
+            const int t = idx / w2, x = idx - t * w2;
+            a[size_t(t) * wl + x] = src[size_t(s0 + t) * g.n + x];
+        }
+        const float2 *res = iqm::fft_run(a, b, L, 1.f, sb, wl);
+        for (int idx = threadIdx.x; idx < sb * w2; idx += FT) {
+            const int t = idx / w2, x = idx - t * w2;
+            keep[(s0 + t) * w2 + x] = res[size_t(t) * wl + x];
+        }
         __syncthreads();
     }
     const float invN = 1.0f / float(g.n);
@@ -958,8 +1011,10 @@ struct Shapes {
     int lw_fcols;         // log2 warps per CTA, forward columns (NB columns per warp)
     int lw_icols;         // log2 warps per CTA, inverse columns
     int rr;               // rows per CTA in the inverse row pass (0: sequential kernel)
+    int icols_cb;         // columns per CTA of the CTA-wide inverse column pass (0: warp kernel)
+    int seq_sb;           // scales per engine call of the sequential row kernel
     int row_eng, col_eng; // transform engine of the row / column length (engine_id)
-    size_t sm_rows, sm_fcols, sm_icols, sm_irows;
+    size_t sm_rows, sm_fcols, sm_icols, sm_irows, sm_icols_seq;
 };
 
 // Compiled transform engine serving a length: 1 (270) or 2 (480) when the length's own plan is
@@ -992,6 +1047,29 @@ void with_engine(int id, F &&f) {
     }
 }
 
+// Warps of a kernel resident per SM at this block size and dynamic shared memory (raises the
+// kernel's shared-memory limit first, as a launch would).  Memoised per device: plane shapes are
+// chosen on every enqueue.
+int resident_warps(const void *fn, int threads, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, const void *, int, size_t>, int> known;
+    int dev = 0;
+    IQM_CHECK_CUDA(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(dev, fn, threads, smem);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = known.find(key);
+        if (it != known.end()) return it->second;
+    }
+    set_smem(fn, smem);
+    int blocks = 0;
+    IQM_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, threads, smem));
+    const int warps = blocks * threads / 32;
+    std::lock_guard<std::mutex> lock(mu);
+    known[key] = warps;
+    return warps;
+}
+
 int lw_fit(size_t fixed, size_t per_warp) {
     int lw = 3;  // up to 8 warps
     while (lw > 0 && fixed + (size_t(1) << lw) * per_warp > 160 * 1024) lw--;
@@ -1016,6 +1094,23 @@ Shapes shapes_for(const iqm::FsimPlan &P, const iqm::FsimTune &tune = iqm::FsimT
     s.lw_icols = lw_fit(twc, warp_col + NB * size_t(P.h2) * f2);
     if (tune.icols_lw >= 0) s.lw_icols = std::min(s.lw_icols, tune.icols_lw);
     s.sm_icols = twc + (size_t(1) << s.lw_icols) * (warp_col + NB * size_t(P.h2) * f2);
+    // Runtime-planned columns: the CTA-wide column kernel (cb columns per CTA, the most warps resident
+    // per SM) when it keeps at least twice as many warps resident as the warp kernel, whose per-warp
+    // work buffers grow with the length.
+    if (s.col_eng == 0) {
+        const int w_warp = resident_warps((const void *)fsim_inv_cols_kernel<GenericEngine>, 32 << s.lw_icols, s.sm_icols);
+        int best = 0;
+        for (int cb : {4, 2, 1}) {
+            const size_t sm = size_t(cb) * (size_t(P.h2) + 2 * size_t(s.wl_col)) * f2;
+            if (sm > SMEM_CAP) continue;
+            const int w = resident_warps((const void *)fsim_inv_cols_seq_kernel, FT, sm);
+            if (w >= 2 * w_warp && w > best) {
+                best = w;
+                s.icols_cb = cb;
+                s.sm_icols_seq = sm;
+            }
+        }
+    }
     const size_t per_row = (4 / NB) * warp_row;  // 4/NB warps per row (four scales)
     if (twr + 2 * per_row <= 120 * 1024) {
         s.rr = 2;
@@ -1025,7 +1120,22 @@ Shapes shapes_for(const iqm::FsimPlan &P, const iqm::FsimTune &tune = iqm::FsimT
         s.rr = 0;
     }
     if (s.rr && tune.rows_per_cta >= 1 && tune.rows_per_cta < s.rr) s.rr = tune.rows_per_cta;
-    s.sm_irows = s.rr ? twr + s.rr * per_row : (4 * size_t(P.w2) + 2 * s.wl_row) * f2;
+    // The sequential row kernel transforms seq_sb scales per engine call: the choice with the most
+    // transforms in flight per SM, and on a tie the one with more CTAs per SM.
+    s.seq_sb = 1;
+    if (!s.rr) {
+        int best = -1;
+        for (int sb : {1, 2, 4}) {
+            const size_t sm = (4 * size_t(P.w2) + 2 * size_t(sb) * s.wl_row) * f2;
+            if (sm > SMEM_CAP) continue;
+            const int inflight = resident_warps((const void *)fsim_inv_rows_seq_kernel, FT, sm) / (FT / 32) * sb;
+            if (inflight > best) {
+                best = inflight;
+                s.seq_sb = sb;
+            }
+        }
+    }
+    s.sm_irows = s.rr ? twr + s.rr * per_row : (4 * size_t(P.w2) + 2 * size_t(s.seq_sb) * s.wl_row) * f2;
     IQM_REQUIRE(s.sm_rows <= SMEM_CAP && s.sm_fcols <= SMEM_CAP && s.sm_icols <= SMEM_CAP && s.sm_irows <= SMEM_CAP,
                 "FSIM plane too large for the shared-memory FFT");
     return s;
@@ -1045,6 +1155,7 @@ void configure_kernels(const Shapes &s) {
     if (!s.rr) {
         set_smem((const void *)fsim_inv_rows_seq_kernel, s.sm_irows);
     }
+    if (s.icols_cb) set_smem((const void *)fsim_inv_cols_seq_kernel, s.sm_icols_seq);
 }
 
 void launch_inv_rows(const FsimGroup &g, const iqm::FsimPlan &P, const Shapes &s, int planes, int consts_mode,
@@ -1062,13 +1173,18 @@ void launch_inv_rows(const FsimGroup &g, const iqm::FsimPlan &P, const Shapes &s
                 g, P.row, s.wl_row, 1, 1, rowsums);
         });
     } else {
-        fsim_inv_rows_seq_kernel<<<dim3(P.h2, 4, planes), FT, s.sm_irows, st>>>(g, P.row, s.wl_row, consts_mode,
-                                                                                 rowsums);
+        fsim_inv_rows_seq_kernel<<<dim3(P.h2, 4, planes), FT, s.sm_irows, st>>>(g, P.row, s.wl_row, s.seq_sb,
+                                                                                 consts_mode, rowsums);
     }
 }
 
 void launch_inv_cols(const FsimGroup &g, const iqm::FsimPlan &P, const Shapes &s, int planes, int consts_mode,
                      cudaStream_t st) {
+    if (s.icols_cb && !consts_mode) {
+        fsim_inv_cols_seq_kernel<<<dim3(iqm::ceil_div(P.w2, s.icols_cb), 4, planes), FT, s.sm_icols_seq, st>>>(
+            g, P.col, s.wl_col, s.icols_cb);
+        return;
+    }
     const int nw = 1 << s.lw_icols;
     with_engine(s.col_eng, [&](auto e) {
         fsim_inv_cols_kernel<decltype(e)><<<dim3(iqm::ceil_div(P.w2, NB * nw), 4, planes), 32 * nw, s.sm_icols, st>>>(
