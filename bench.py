@@ -49,8 +49,8 @@ WORKLOADS = {
 TRAFFIC = {
     # ssim_kernel, 32 pairs: 568,007,424 B read + 3,266,560 B written (profiles/ssim_kernel_1080p.md)
     "ssim": {"kernel": "ssim_kernel", "bytes_per_launch": 571273984, "pairs_per_launch": 32},
-    # fsim_inv_cols_kernel, one chunk of 2 pairs: 12,462,848 + 12,870,656 B (profiles/fsim_inv_cols_kernel_1080p.md)
-    "fsim": {"kernel": "fsim_inv_cols_kernel", "bytes_per_launch": 25333504, "pairs_per_launch": 2},
+    # fsim_inv_cols_kernel, one chunk of 2 pairs: 10,389,760 + 12,827,904 B (profiles/fsim_inv_cols_kernel_1080p.md)
+    "fsim": {"kernel": "fsim_inv_cols_kernel", "bytes_per_launch": 23217664, "pairs_per_launch": 2},
     # flip_vcols_kernel, 16 pairs: 1,628,939,776 + 18,826,752 B (profiles/flip_vcols_kernel_1080p.md)
     "flip": {"kernel": "flip_vcols_kernel", "bytes_per_launch": 1647766528, "pairs_per_launch": 16},
     # msvd_block_kernel, 32 pairs: 527,183,360 + 6,785,792 B (profiles/msvd_block_kernel_1080p.md)
