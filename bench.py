@@ -53,8 +53,8 @@ TRAFFIC = {
     "fsim": {"kernel": "fsim_inv_cols_kernel", "bytes_per_launch": 23217664, "pairs_per_launch": 2},
     # flip_vcols_kernel, 16 pairs: 1,628,939,776 + 18,826,752 B (profiles/flip_vcols_kernel_1080p.md)
     "flip": {"kernel": "flip_vcols_kernel", "bytes_per_launch": 1647766528, "pairs_per_launch": 16},
-    # msvd_block_kernel, 32 pairs: 527,183,360 + 6,785,792 B (profiles/msvd_block_kernel_1080p.md)
-    "msvd": {"kernel": "msvd_block_kernel", "bytes_per_launch": 533969152, "pairs_per_launch": 32},
+    # msvd_block_kernel, 32 pairs: 528,075,776 + 6,771,712 B (profiles/msvd_block_kernel_1080p.md)
+    "msvd": {"kernel": "msvd_block_kernel", "bytes_per_launch": 534847488, "pairs_per_launch": 32},
 }
 
 
