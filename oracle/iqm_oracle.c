@@ -2,7 +2,8 @@
  * iqm_oracle.c -- CPU restatement of cadik/IQM's metric arithmetic.
  *
  * TEST INFRASTRUCTURE ONLY.  Nothing in the product library links, loads or calls this file;
- * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it, as the checker.
+ * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it, as the reference that
+ * GPU results are compared with.
  *
  * The same source is compiled twice:
  *   -DORACLE_F32  -> liboracle_f32.so : arithmetic in float, in the order the reference's GLSL

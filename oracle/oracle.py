@@ -1,7 +1,8 @@
 """ctypes front end of the CPU oracle (oracle/iqm_oracle.c).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
-leg, as the checker.  The product library never imports, links or calls anything here.
+leg, as the reference that GPU results are compared with.  The product library never imports,
+links or calls anything here.
 
 Two builds of the same C source are exposed:
   Oracle("f32") -- float arithmetic in the reference's order (reference-faithful restatement)
