@@ -981,7 +981,11 @@ void plane_size(int w, int h, int F, int &w2, int &h2) {  // src/gpu/fsim/fsim.c
 
 constexpr size_t SMEM_CAP = 200 * 1024;
 constexpr int kFsimStreams = 8;  // plane-size groups in flight at once
-constexpr bool kOverlapChunks = true;  // alternate inverse-pass chunks between two streams
+constexpr bool kOverlapChunks = true;  // rotate inverse-pass chunks over several streams
+// Streams (and L2-sized buffers) the chunks rotate over: two fill each other's partial waves; three
+// measured 2% slower (the third chunk's planes crowd the L2).
+constexpr int kChunkStreams = 2;
+static_assert(kChunkStreams >= 1 && kChunkStreams <= 8, "chunk streams");
 
 // Raises a kernel's dynamic shared-memory limit on the current device to at least `bytes` (never
 // lowers it: launches already enqueued or captured for other plane sizes keep their sizes valid).
@@ -1338,8 +1342,8 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
             // More than one chunk: split the L2 budget over two buffers and let consecutive chunks run
             // on two streams, so one chunk's column pass fills the other's last partial wave.
             r.overlap = kOverlapChunks && !ctx->timing && r.G > r.chunk;
-            if (r.overlap) r.chunk = std::max(1, r.chunk / 2);
-            r.L = layout_for(r.G, r.chunk, n, int(iqm::ceil_div(n, FT)), r.overlap ? 2 : 1);
+            if (r.overlap) r.chunk = std::max(1, r.chunk / kChunkStreams);
+            r.L = layout_for(r.G, r.chunk, n, int(iqm::ceil_div(n, FT)), r.overlap ? kChunkStreams : 1);
             r.F_uniform = hd[kv.second[0]].F;
             for (int i : kv.second)
                 if (hd[i].F != r.F_uniform) r.F_uniform = 0;
@@ -1374,7 +1378,7 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
     std::vector<cudaStream_t> streams(S, ctx->stream);
     bool any_overlap = false;
     for (const auto &r : runs) any_overlap |= r.overlap;
-    if (any_overlap) iqm::side_streams(ctx, 2 * S);  // streams S .. 2S-1 take the odd chunks
+    if (any_overlap) iqm::side_streams(ctx, kChunkStreams * S);  // streams j*S + slot take chunks k = j mod N
     if (S > 1) {
         iqm::side_streams(ctx, S);
         IQM_CHECK_CUDA(cudaEventRecord(ctx->fork_event, ctx->stream));
@@ -1431,28 +1435,32 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
                     g, P->col, s.wl_col, s.lw_fcols);
         });
         iqm::check_launch(ctx, "fsim_fwd_cols_kernel");
-        cudaStream_t st2 = st;
+        // chunk k runs on stream k mod N of this slot (0: the group's stream) with buffer k mod N
+        const int nst = r.overlap ? kChunkStreams : 1;
+        cudaStream_t cstream[8] = {st};
         if (r.overlap) {
-            st2 = ctx->side_streams[S + r.slot];
             cudaEvent_t fork = iqm::aux_event(ctx, r.slot);
             IQM_CHECK_CUDA(cudaEventRecord(fork, st));
-            IQM_CHECK_CUDA(cudaStreamWaitEvent(st2, fork, 0));
+            for (int j = 1; j < nst; j++) {
+                cstream[j] = ctx->side_streams[j * S + r.slot];
+                IQM_CHECK_CUDA(cudaStreamWaitEvent(cstream[j], fork, 0));
+            }
         }
         for (int c0 = 0, k = 0; c0 < G; c0 += chunk, k++) {
             FsimGroup gc = g;
             gc.pair0 = c0;
-            const bool odd = r.overlap && (k & 1);
-            if (odd) gc.T = g.T + size_t(chunk) * 32 * n;
-            cudaStream_t cs = odd ? st2 : st;
+            const int j = k % nst;
+            gc.T = g.T + size_t(j) * chunk * 32 * n;
+            cudaStream_t cs = cstream[j];
             const int cg = std::min(chunk, G - c0);
             launch_inv_cols(gc, *P, s, 2 * cg, 0, cs);
             iqm::check_launch(ctx, "fsim_inv_cols_kernel");
             launch_inv_rows(gc, *P, s, 2 * cg, 0, nullptr, cs);
             iqm::check_launch(ctx, "fsim_inv_rows_kernel");
         }
-        if (r.overlap) {
-            IQM_CHECK_CUDA(cudaEventRecord(ctx->side_events[S + r.slot], st2));
-            IQM_CHECK_CUDA(cudaStreamWaitEvent(st, ctx->side_events[S + r.slot], 0));
+        for (int j = 1; j < nst; j++) {
+            IQM_CHECK_CUDA(cudaEventRecord(ctx->side_events[j * S + r.slot], cstream[j]));
+            IQM_CHECK_CUDA(cudaStreamWaitEvent(st, ctx->side_events[j * S + r.slot], 0));
         }
         fsim_noise_kernel<<<dim3(8, G), 1024, 0, st>>>(g);
         iqm::check_launch(ctx, "fsim_noise_kernel");
