@@ -319,7 +319,8 @@ using Engine480 = FixedEngine<iqm::FixedPlanIP<480, 15, 8, 4>>;
 // forward transform (src/gpu/fsim/fsim.cpp:270-368: luma as complex (Y, 0), sign -1, unscaled),
 // NB rows per warp.
 template <class Eng>
-__global__ void __launch_bounds__(FT, 1) fsim_fwd_rows_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl) {
+// Compiled engines: 4 CTAs per SM (62 registers with the 480-point engine, no spills).
+__global__ void __launch_bounds__(FT, engine_len<Eng>::value ? 4 : 1) fsim_fwd_rows_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl) {
     extern __shared__ __align__(16) float2 sm[];
     const int tl = iqm::stage_twiddle_len(L);
     iqm::stage_twiddles_to_shared(L, sm);
@@ -348,7 +349,10 @@ __global__ void __launch_bounds__(FT, 1) fsim_fwd_rows_kernel(FsimGroup g, const
 __device__ __forceinline__ int slab_parity(float2 *res, float2 *a) { return res == a ? 0 : 1; }
 
 template <class Eng>
-__global__ void __launch_bounds__(FT, 1) fsim_fwd_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int lw) {
+// Compiled engines: 5 CTAs per SM with the two-buffer 270-point engine (48 registers), 4 with the
+// in-place 480-point one (63 registers); no spills either way.
+__global__ void __launch_bounds__(FT, engine_len<Eng>::value ? (engine_bufs<Eng>::value == 2 ? 5 : 4) : 1)
+fsim_fwd_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int lw) {
     extern __shared__ __align__(16) float2 sm[];
     __shared__ int parity;
     const int tl = iqm::stage_twiddle_len(L);
