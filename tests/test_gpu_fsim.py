@@ -23,8 +23,9 @@ def test_plan_constants_match_oracle(rt, o64, w2, h2, mode):
 @pytest.mark.parametrize("h,w", [(96, 128), (130, 200), (270, 480), (480, 270), (600, 800), (1080, 1920), (1920, 1080),
                                  (131, 263), (57, 61), (2160, 3840),
                                  # full-resolution planes with long runtime-planned transforms, which run
-                                 # CTA-wide: rows of 1100, columns of 1100, a 1031-point Bluestein row
-                                 (300, 1100), (1100, 300), (290, 1031)])
+                                 # CTA-wide: rows of 1100; columns of 1100 in groups of four (the last of a
+                                 # 301-wide plane holds one); a 1031-point Bluestein row
+                                 (300, 1100), (1100, 301), (290, 1031)])
 def test_fsim_matches_oracle(rt, o64, o32, h, w):
     a, b = synth.rgb_gain_pair(h, w, config=1, pair=w % 7)
     r = iqm_b200.FSIM(rt).compute_metric(a, b)
