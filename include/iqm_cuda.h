@@ -86,9 +86,14 @@ int iqm_ssim(iqm_ctx *ctx, const uint8_t *rgba_in, const uint8_t *rgba_ref, int 
  * GPU which loads the library holds until the process exits, so the image may span at most
  * IQM_SSIM_NOALLOC_MAX_TILES tiles of 128 columns x 122 rows (11-tap window; e.g. 7680x4320 uses
  * 2160); larger images return IQM_EINVAL.  The first call on a device looks up that array's device
- * address with the device current, so make it before any stream capture.  All calls share the one
- * array: calls that overlap on the GPU (other streams, other threads) race -- serialise them.
- * Returns IQM_OK, IQM_EINVAL (null pointer, size or parameter out of range) or IQM_ECUDA. */
+ * address with the device current, so make it before any stream capture.  The address is kept for
+ * the device's primary context (the one the CUDA runtime uses): callers in other driver-API
+ * contexts, or after cudaDeviceReset, are not supported.  All calls share the one array: calls
+ * that overlap on the GPU (other streams, other threads) race -- serialise them.  `d_in`, `d_ref`,
+ * `row_bytes` and `d_map` must be multiples of 4 and `d_mssim` of 8 (else IQM_EINVAL, before any
+ * launch).  Returns IQM_OK, IQM_EINVAL (null or misaligned pointer, size or parameter out of
+ * range) or IQM_ECUDA (a launch of this call failed; errors pending from the caller's earlier work
+ * are left pending, not reported or cleared). */
 #define IQM_SSIM_NOALLOC_MAX_TILES 4096
 int iqm_ssim_noalloc(const uint8_t *d_in, const uint8_t *d_ref, int w, int h, size_t row_bytes,
                      const iqm_ssim_params *params, float *d_map, double *d_mssim, void *cuda_stream);
@@ -137,7 +142,8 @@ typedef struct {
 
 /* Device-resident forms: `pairs` is a HOST array of n descriptors whose pointers are DEVICE
  * pointers; scores go to DEVICE memory (`d_scores`, n doubles; FSIM writes 2n: fsim then fsimc
- * per pair).  Enqueued on the context stream; no host synchronisation. */
+ * per pair).  Enqueued on the context stream; no host synchronisation.  The images are read in
+ * place, so each image pointer and row_bytes must be a multiple of 4 (IQM_EINVAL otherwise). */
 int iqm_ssim_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_ssim_params *params,
                  double *d_scores);
 int iqm_msvd_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, double *d_scores);

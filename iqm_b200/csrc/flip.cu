@@ -707,6 +707,7 @@ void iqm::enqueue_flip_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm
     const iqm_flip_params p = resolve(params);
     check_params(p);
     iqm::check_pairs(pairs, n, 1, 1);
+    iqm::check_dev_alignment(pairs, n);
     IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
     flip_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), p, {}, d_scores);
 }

@@ -1509,6 +1509,7 @@ void iqm_release_fsim_plans(iqm_ctx *ctx) {
 void iqm::enqueue_fsim_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, iqm_precision precision, int energy_mode,
                            double *d_scores) {
     check_fsim_args(pairs, n, precision, energy_mode);
+    iqm::check_dev_alignment(pairs, n);
     IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
     fsim_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), energy_mode, d_scores);
 }

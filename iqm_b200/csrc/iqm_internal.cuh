@@ -207,6 +207,18 @@ inline void check_pairs(const iqm_pair *pairs, int n, int min_w, int min_h) {
     }
 }
 
+// Device-resident pairs are read in place with 4-byte pixel loads (and wider ones when the base and
+// pitch allow), so both image pointers and the pitch must be multiples of 4; anything else is
+// rejected here instead of faulting on the GPU.  Host entry points repack into aligned buffers.
+inline void check_dev_alignment(const iqm_pair *pairs, int n) {
+    for (int i = 0; i < n; i++) {
+        const iqm_pair &p = pairs[i];
+        IQM_REQUIRE(((reinterpret_cast<uintptr_t>(p.input) | reinterpret_cast<uintptr_t>(p.ref) |
+                      uintptr_t(p.row_bytes)) & 3u) == 0,
+                    "pair " + std::to_string(i) + ": device image pointers and row_bytes must be multiples of 4");
+    }
+}
+
 // Copies `bytes` from host memory to `dst` (grown as needed) on the context stream, staging
 // through the pinned ring; returns the device pointer.
 void *upload_bytes(iqm_ctx *ctx, DevBuf &dst, const void *src, size_t bytes);

@@ -285,6 +285,7 @@ static void check_msvd_pairs(const iqm_pair *pairs, int n) { iqm::check_pairs(pa
 
 void iqm::enqueue_msvd_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, double *d_scores) {
     check_msvd_pairs(pairs, n);
+    iqm::check_dev_alignment(pairs, n);
     IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
     msvd_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), {}, d_scores);
 }

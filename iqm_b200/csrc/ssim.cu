@@ -72,7 +72,7 @@ struct SsimArgs {
     float c1, c2;
 };
 
-// shaders/ssim/ssim_lumapack.glsl:155-157 (G weight 0.581 as in the reference) on unorm bytes
+// shaders/ssim/ssim_lumapack.glsl:19-21 (G weight 0.581 as in the reference) on unorm bytes
 __device__ __forceinline__ float luma_u8(uint32_t px) {
     float r = float(px & 0xffu) * (1.0f / 255.0f);
     float g = float((px >> 8) & 0xffu) * (1.0f / 255.0f);
@@ -422,6 +422,7 @@ void iqm::enqueue_ssim_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm
     check_params(p);
     const int R = (p.kernel_size - 1) / 2;
     iqm::check_pairs(pairs, n, R, R);
+    iqm::check_dev_alignment(pairs, n);
     IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
     ssim_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), p, {}, d_scores);
 }
@@ -501,12 +502,28 @@ __global__ void ssim_noalloc_setup_kernel(NoallocScratch *s, SsimPairDev d) {
     s->counter = 0u;
 }
 
+// Launches ssim_kernel<R> and returns that launch's own status.  cudaLaunchKernel reports errors of
+// this launch only, so an error left pending by the caller's earlier work is neither returned nor
+// cleared here; a failed launch's own error is cleared before returning.
+template <int R>
+cudaError_t launch_ssim_checked(SsimArgs &a, int total_tiles, cudaStream_t st) {
+    void *args[] = {&a};
+    const cudaError_t e = cudaLaunchKernel((const void *)ssim_kernel<R>, dim3(total_tiles), dim3(NT), args, 0, st);
+    if (e != cudaSuccess) cudaGetLastError();
+    return e;
+}
+
 }  // namespace
 
 extern "C" __attribute__((visibility("default"))) int iqm_ssim_noalloc(
     const uint8_t *d_in, const uint8_t *d_ref, int w, int h, size_t row_bytes, const iqm_ssim_params *params,
     float *d_map, double *d_mssim, void *cuda_stream) {
     if (!d_in || !d_ref || !d_mssim) return IQM_EINVAL;
+    // pixels are read as 4-byte words, the score as a double and the map as floats: misaligned
+    // pointers would fault on the GPU, so they are refused before any launch
+    if (((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_ref) | uintptr_t(row_bytes) |
+          reinterpret_cast<uintptr_t>(d_map)) & 3u) != 0 || (reinterpret_cast<uintptr_t>(d_mssim) & 7u) != 0)
+        return IQM_EINVAL;
     const iqm_ssim_params p = resolve(params);
     try {
         check_params(p);
@@ -527,7 +544,7 @@ extern "C" __attribute__((visibility("default"))) int iqm_ssim_noalloc(
         if (!g_noalloc_addr[dev]) {
             void *a = nullptr;
             if (cudaGetSymbolAddress(&a, g_ssim_noalloc_scratch) != cudaSuccess || !a) {
-                cudaGetLastError();
+                cudaGetLastError();  // this lookup's own error
                 return IQM_ECUDA;
             }
             g_noalloc_addr[dev] = a;
@@ -549,7 +566,15 @@ extern "C" __attribute__((visibility("default"))) int iqm_ssim_noalloc(
     d.ntiles = int(tiles);
     d.vec_ok = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_ref) | uintptr_t(row_bytes)) &
                 15u) == 0;
-    ssim_noalloc_setup_kernel<<<1, 1, 0, st>>>(s, d);
+    {
+        void *args[] = {&s, &d};
+        const cudaError_t e =
+            cudaLaunchKernel((const void *)ssim_noalloc_setup_kernel, dim3(1), dim3(1), args, 0, st);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return IQM_ECUDA;  // the SSIM kernel is not launched without its descriptor
+        }
+    }
 
     SsimArgs a{};
     a.pairs = &s->desc;
@@ -561,14 +586,15 @@ extern "C" __attribute__((visibility("default"))) int iqm_ssim_noalloc(
     for (int k = -R; k <= R; k++) a.g[k + R] = float(std::exp(-double(k * k) / (2.0 * double(p.sigma) * p.sigma)));
     a.c1 = p.k1 * p.k1;
     a.c2 = p.k2 * p.k2;
+    cudaError_t e;
     switch (R) {
-        case 1: launch_ssim<1>(a, int(tiles), st); break;
-        case 2: launch_ssim<2>(a, int(tiles), st); break;
-        case 3: launch_ssim<3>(a, int(tiles), st); break;
-        case 4: launch_ssim<4>(a, int(tiles), st); break;
-        case 5: launch_ssim<5>(a, int(tiles), st); break;
-        case 6: launch_ssim<6>(a, int(tiles), st); break;
-        default: launch_ssim<7>(a, int(tiles), st); break;
+        case 1: e = launch_ssim_checked<1>(a, int(tiles), st); break;
+        case 2: e = launch_ssim_checked<2>(a, int(tiles), st); break;
+        case 3: e = launch_ssim_checked<3>(a, int(tiles), st); break;
+        case 4: e = launch_ssim_checked<4>(a, int(tiles), st); break;
+        case 5: e = launch_ssim_checked<5>(a, int(tiles), st); break;
+        case 6: e = launch_ssim_checked<6>(a, int(tiles), st); break;
+        default: e = launch_ssim_checked<7>(a, int(tiles), st); break;
     }
-    return cudaGetLastError() == cudaSuccess ? IQM_OK : IQM_ECUDA;
+    return e == cudaSuccess ? IQM_OK : IQM_ECUDA;
 }

@@ -194,7 +194,7 @@ void oracle_fft2(double *data, int w, int h, int sign, int normalize) {
 /* SSIM                                                                                        */
 /* ========================================================================================== */
 
-/* shaders/ssim/ssim_lumapack.glsl:155-157 -- note 0.581 for green (sic) on unorm [0,1] */
+/* shaders/ssim/ssim_lumapack.glsl:19-21 -- note 0.581 for green (sic) on unorm [0,1] */
 static inline real ssim_luma(const uint8_t *p) {
     real r = (real)p[0] / R(255.0), g = (real)p[1] / R(255.0), b = (real)p[2] / R(255.0);
     return R(0.299) * r + R(0.581) * g + R(0.114) * b;

@@ -133,3 +133,19 @@ def test_images_of_2_31_pixels_are_rejected(rt):
                L.iqm_fsim_batch(rt.h, arr, 1, 0, 0, out)):
         assert rc == iqm_b200.IQM_EINVAL
         assert "too large" in L.iqm_last_error(rt.h).decode()
+
+
+def test_dev_entry_points_reject_misaligned_images(rt):
+    """Device-resident images are read in place with 4-byte loads: a pointer or pitch that is not a
+    multiple of 4 is refused with IQM_EINVAL before anything is enqueued."""
+    import torch
+    w, h = 64, 64
+    buf = torch.zeros(w * h * 4 + 64, dtype=torch.uint8, device="cuda")
+    d_scores = torch.zeros(4, dtype=torch.float64, device="cuda")
+    base = buf.data_ptr()
+    metrics = [iqm_b200.SSIM(rt), iqm_b200.SVD(rt), iqm_b200.FLIP(rt), iqm_b200.FSIM(rt)]
+    for item in ((base + 1, base, w, h, 4 * w), (base, base + 2, w, h, 4 * w), (base, base, w, h - 1, 4 * w + 2)):
+        for m in metrics:
+            with pytest.raises(iqm_b200.IQMError) as e:
+                m.compute_dev([item], d_scores.data_ptr())
+            assert e.value.code == iqm_b200.IQM_EINVAL
