@@ -181,3 +181,46 @@ def test_ssim_matches_opencv_gaussian_ssim(o64, o32, h, w, ks, sigma):
     want = _opencv_mssim(a, b, ks=ks, sigma=sigma)
     assert abs(o64.ssim(a, b, kernel_size=ks, sigma=sigma) - want) <= 1e-9
     assert abs(o32.ssim(a, b, kernel_size=ks, sigma=sigma) - want) <= 1e-5
+
+
+# ---- second, independent restatement (oracle/np_restatement.py): whole-plane numpy from the shaders
+@pytest.fixture(scope="module")
+def npr():
+    import np_restatement
+    return np_restatement
+
+
+@pytest.mark.parametrize("h,w", [(96, 128), (270, 480), (1080, 1920), (57, 61), (131, 263), (263, 131),
+                                 (2160, 3840), (300, 2048)])
+@pytest.mark.parametrize("energy_full", [False, True])
+def test_fsim_two_restatements_agree(o64, npr, h, w, energy_full):
+    """FSIM/FSIMc of the C oracle and of the independent numpy restatement: every shader read twice
+    (downscale F = 1, 4, 8 and odd plane sizes for the integer n/2 frequency grid, both ways of
+    pooling the noise-energy estimates)."""
+    a, b = synth.rgb_gain_pair(h, w, config=1, pair=7)
+    want = npr.fsim(a, b, energy_full=energy_full)
+    got = o64.fsim(a, b, energy_full=energy_full)
+    assert np.abs(np.asarray(got) - np.asarray(want)).max() <= 1e-9, (got, want)
+
+
+def test_fsim_restatements_agree_on_size_constants(o64, npr):
+    for w2, h2 in ((480, 270), (61, 57), (131, 263)):
+        H = npr.fsim_filters(w2, h2)
+        for full in (False, True):
+            em, an2, aiaj = npr.fsim_noise_constants(H, full)
+            cem, can2, caiaj = o64.fsim_constants(w2, h2, full)
+            assert np.allclose(em, cem, rtol=1e-12) and np.allclose(an2, can2, rtol=1e-9)
+            assert np.allclose(aiaj, caiaj, rtol=1e-9, atol=1e-9 * np.abs(can2).max())
+
+
+@pytest.mark.parametrize("h,w", [(96, 128), (131, 263), (270, 480)])
+@pytest.mark.parametrize("ppd", [67.0, 52.127, 37.0])
+def test_flip_two_restatements_agree(o64, npr, h, w, ppd):
+    """Mean FLIP of the C oracle and of the independent numpy restatement."""
+    a, b = synth.rgb_blockquant_pair(h, w, config=2, pair=1)
+    assert abs(o64.flip(a, b, ppd=ppd) - npr.flip(a, b, ppd)) <= 1e-9
+
+
+def test_flip_ppd_two_restatements_agree(o64, npr):
+    for r, d, wd in ((2560, 0.7, 0.6), (3840, 0.7, 0.7), (1920, 0.5, 0.53)):
+        assert npr.flip_ppd(r, d, wd) == o64.flip_ppd(r, d, wd)
