@@ -56,6 +56,12 @@ TRAFFIC = {
     # msvd_block_kernel, 32 pairs: 528,075,776 + 6,771,712 B (profiles/msvd_block_kernel_1080p.md)
     "msvd": {"kernel": "msvd_block_kernel", "bytes_per_launch": 534847488, "pairs_per_launch": 32},
 }
+# Executed tensor-core work of the mixed FSIM forms on 480x270 planes (1080p and 4K pairs): per pair
+# 32 inverse transforms of each of the 480 columns (270 = 15 x 18: 27 m16n8k16 tiles) and of each
+# of the 270 rows (480 = 16 x 30: 48 tiles), 2 * 16 * 8 * 16 = 4096 flops a tile, times the products
+# per tile (3 with split-precision operands, 1 with single FP16 operands).
+MMA_TILES_PER_PAIR = {"fsim_inv_cols_mma_kernel": 32 * 480 * 27, "fsim_inv_rows_mma_kernel": 32 * 270 * 48}
+MMA_PRODUCTS = {"mixed": 3, "mixed_fast": 1}
 
 
 def workload_name(metric):
@@ -79,6 +85,9 @@ def parse():
                     help="uneven-size batch: 256 pairs, sides uniform in [256, 2048], SSIM + FSIM through one "
                          "CUDA-graph batch plan")
     ap.add_argument("--distinct", type=int, default=4, help="distinct synthetic pairs (replicated to --pairs)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed", "mixed_fast"],
+                    help="FSIM form: FP32 transforms, or tensor-core transforms with FP16 planes "
+                         "(split-precision hi + lo products, or single products)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     return ap.parse_args()
@@ -441,6 +450,8 @@ def main():
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_note = "measured" if "hbm_gbs" in peaks else "fallback"
+    tensor_peak = float(peaks.get("bf16_tflops", 1590.0))
+    tensor_note = "measured" if "bf16_tflops" in peaks else "fallback"
 
     B = args.pairs or (32 if SIZE == "1080p" else 64)
     host_pairs = make_pairs(metric, min(args.distinct if SIZE == "1080p" else min(args.distinct, 2), B))
@@ -448,6 +459,9 @@ def main():
     stream = torch.cuda.Stream()
     rt.set_stream(stream.cuda_stream)
     obj = {"fsim": iqm_b200.FSIM, "ssim": iqm_b200.SSIM, "flip": iqm_b200.FLIP, "msvd": iqm_b200.SVD}[metric](rt)
+    prec = {"fp32": iqm_b200.IQM_FP32, "mixed": iqm_b200.IQM_MIXED, "mixed_fast": iqm_b200.IQM_MIXED_FAST}[args.precision]
+    if metric == "fsim":
+        obj.precision = prec
     nscore = WORKLOADS[metric][2]
     flip_args = iqm_b200.FLIPArguments(3840.0, 0.7, 0.7)  # 67.02 pixels per degree
 
@@ -523,6 +537,18 @@ def main():
             "avg_launch_us": avg_s * 1e6, "kernel_share": ktimes[kname][1] / ktotal,
             "pipeline_frac": alg_bytes / (ms_per_step / 1e3) / 1e9 / hbm_peak,
             "timing": "CUDA events on the library stream around every launch, second pass of the K steps"}
+    if metric == "fsim" and args.precision in MMA_PRODUCTS:
+        # tensor pipe of the tensor-core kernels: executed MMA flops per launch / average launch time
+        tens = {}
+        for k, tiles in MMA_TILES_PER_PAIR.items():
+            if k not in ktimes:
+                continue
+            n_l, t_ms = ktimes[k]
+            flops = B * args.steps * tiles * 4096 * MMA_PRODUCTS[args.precision] / max(1, n_l)
+            achieved_t = flops / (t_ms / max(1, n_l) / 1e3) / 1e12
+            tens[k] = {"achieved": achieved_t, "peak": tensor_peak, "unit": "TFLOP/s", "frac": achieved_t / tensor_peak,
+                       "flops_per_launch": flops, "peak_source": tensor_note + " dense bf16 (burst)"}
+        roof["tensor"] = tens
 
     # end to end: host API with pinned host images and host scores
     e2e = None
@@ -578,7 +604,8 @@ def main():
         "data": "synthetic (seeded 1/f^2 noise pairs, %d distinct replicated to %d device buffers)" % (
             len(host_pairs), B),
         "config": {"workload": workload_name(metric), "pairs_per_step": B, "width": W, "height": H,
-                   "precision": "fp32", "parallelism": "replicas" if world > 1 else "single",
+                   "precision": args.precision if metric == "fsim" else "fp32",
+                   "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (%.0f MB per step), no flush" % (alg_bytes / 1e6)},
         "roofline": roof, "kernels": kernels, "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "clocks": clk,
     }

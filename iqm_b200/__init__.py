@@ -25,7 +25,8 @@ IQM_ENOMEM = -3
 IQM_EUNSUPPORTED = -4
 
 IQM_FP32 = 0
-IQM_MIXED = 1
+IQM_MIXED = 1       # tensor-core transforms, split-precision (hi + lo) FP16 products
+IQM_MIXED_FAST = 2  # tensor-core transforms, single FP16 products
 
 # every symbol include/iqm_cuda.h declares
 EXPORTS = (

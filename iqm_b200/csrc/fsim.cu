@@ -33,6 +33,7 @@
 #include <mutex>
 #include <tuple>
 
+#include "dft_mma.cuh"
 #include "fft.cuh"
 #include "fft_plan.cuh"
 #include "iqm_internal.cuh"
@@ -78,6 +79,7 @@ struct FsimGroup {
     float *yiq;     // G x 2 x 3 x n   (I, Q, Y)
     float2 *spec;   // G x n: per pair the spectrum of Y_img + i Y_ref
     float2 *T;      // chunk x 2 x 16 x n  (after the column pass of the inverse transform)
+    __half2 *Th;    // the same planes in FP16 (mixed precision; shares T's memory)
     float *amp;     // G x 8 x n       (img*4 + o)
     float *energy;  // G x 8 x n
     float *eo0;     // G x 8 x n       |EO(s=0, o)|^2
@@ -742,6 +744,163 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_seq_kernel(FsimGroup g, c
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Mixed precision (IQM_MIXED, IQM_MIXED_FAST): the inverse passes on the tensor cores.  Each
+// transform is a two-factor DFT computed with FP16 mma.sync tiles and FP32 accumulation
+// (dft_mma.cuh); the spectrum is scaled by 1/N as the column pass loads it, so every FP16 operand
+// and the FP16 intermediate planes between the passes stay in range, and the row pass produces the
+// normalised responses directly.  Both kernels are persistent: each warp builds its transform's
+// constant fragments once and the CTAs stride over (columns or rows, orientation, plane) items.
+
+// Column pass: a work item is MCW adjacent columns of one (orientation, plane); warp c transforms
+// column c for the orientation's 4 scales.  The separated spectrum slab sits in shared memory with
+// each column stored as N1 segments of N2 points padded to a stride of SEG (conflict-free loads by
+// the engine's lane pattern); outputs are staged per scale as FP16 rows of MCW columns and written
+// row by row.
+constexpr int MCW = 8;
+template <class Dft>
+struct MmaColGeom {
+    static constexpr int H = Dft::N;                                      // column length
+    static constexpr int SEG = Dft::N2 + ((4 - Dft::N2 % 16) + 16) % 16;  // N2 padded to 4 mod 16
+    static constexpr int SLAB = Dft::N1 * SEG;                            // padded column, float2
+    static constexpr int SP = MCW + 1;                                    // staging row stride, half2
+    static constexpr size_t smem = sizeof(float2) * MCW * SLAB + sizeof(__half2) * 4 * H * SP;
+};
+
+template <class Dft>
+__global__ void __launch_bounds__(32 * MCW, 2) fsim_inv_cols_mma_kernel(FsimGroup g, int items) {
+    using Gm = MmaColGeom<Dft>;
+    constexpr int H = Gm::H;
+    extern __shared__ __align__(16) float2 sm[];
+    float2 *Sl = sm;
+    __half2 *stage = reinterpret_cast<__half2 *>(Sl + MCW * Gm::SLAB);
+    const int warp = threadIdx.x >> 5;
+    Dft dft;
+    dft.init(1.f);
+    const int ngroups = (g.w2 + MCW - 1) / MCW;
+    const float invN = 1.0f / float(g.n);
+    for (int item = blockIdx.x; item < items; item += gridDim.x) {
+        const int cg = item % ngroups;
+        const int o = (item / ngroups) & 3;
+        const int plane = item / (ngroups * 4);  // chunk-local pair*2 + img
+        const int x0 = cg * MCW, nc = min(MCW, g.w2 - x0), img = plane & 1;
+        const float2 *src = g.spec + size_t(g.pair0 + (plane >> 1)) * g.n;
+        for (int idx = threadIdx.x; idx < MCW * H; idx += blockDim.x) {
+            const int y = idx / MCW, c = idx - y * MCW;
+            float2 v = make_float2(0.f, 0.f);
+            if (c < nc) {
+                const int x = x0 + c;
+                // Z = F(Y_img + i Y_ref): F(Y_img) = (Z(k) + conj Z(-k)) / 2, F(Y_ref) = (Z(k) - conj Z(-k)) / 2i
+                const float2 z = src[size_t(y) * g.w2 + x];
+                const float2 m = src[size_t(y ? H - y : 0) * g.w2 + (x ? g.w2 - x : 0)];
+                const float hs = 0.5f * invN;
+                v = img == 0 ? make_float2(hs * (z.x + m.x), hs * (z.y - m.y)) : make_float2(hs * (z.y + m.y), hs * (m.x - z.x));
+            }
+            Sl[c * Gm::SLAB + (y / Dft::N2) * Gm::SEG + y % Dft::N2] = v;
+        }
+        __syncthreads();
+        if (warp < nc) {  // warp-uniform
+            const float2 *col = Sl + warp * Gm::SLAB;
+#pragma unroll 1
+            for (int s = 0; s < 4; s++) {
+                const float *Hz = g.filters + size_t(o * 4 + s) * g.n + size_t(x0 + warp) * H;
+                __half2 *st = stage + s * H * Gm::SP + warp;
+                dft.run(
+                    [&](int n1, int n2) {
+                        const float h = __ldg(Hz + Dft::N2 * n1 + n2);
+                        const float2 v = col[n1 * Gm::SEG + n2];
+                        return make_float2(h * v.x, h * v.y);
+                    },
+                    [&](int k, float2 v) { st[k * Gm::SP] = __floats2half2_rn(v.x, v.y); });
+            }
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < 4 * H * MCW; idx += blockDim.x) {
+            const int r = idx / MCW, c = idx - r * MCW;  // r = s * H + y
+            const int s = r / H, y = r - s * H;
+            if (c < nc)
+                g.Th[(size_t(plane) * 16 + o * 4 + s) * g.n + size_t(y) * g.w2 + x0 + c] = stage[r * Gm::SP + c];
+        }
+        // the next item's first barrier orders these staging reads before its staging writes
+    }
+}
+
+// Row pass: a work item is MRR rows of one (orientation, plane); warp (r, s) transforms row r for
+// scale s, reading its FP16 inputs straight from the intermediate planes, and leaves the outputs
+// in shared memory (each group of N1 outputs padded to RS, conflict-free stores); then the CTA
+// forms the response sums of 4 consecutive pixels per thread, as fsim_inv_rows_kernel does.
+constexpr int MRR = 2;
+template <class Dft>
+struct MmaRowGeom {
+    static constexpr int W = Dft::N;
+    static constexpr int RS = Dft::N1 + ((4 - Dft::N1 % 16) + 16) % 16;  // N1 padded to 4 mod 16
+    static constexpr int RL = RS * Dft::N2;
+    static constexpr size_t smem = sizeof(float2) * MRR * 4 * RL;
+    static_assert(Dft::N1 % 4 == 0 && RL % 4 == 0, "4-pixel epilogue needs N1 % 4 == 0");
+};
+
+template <class Dft>
+__global__ void __launch_bounds__(32 * 4 * MRR, 1) fsim_inv_rows_mma_kernel(FsimGroup g, int items) {
+    using Gm = MmaRowGeom<Dft>;
+    constexpr int W = Gm::W;
+    extern __shared__ __align__(16) float2 sm[];
+    const int warp = threadIdx.x >> 5;
+    const int r = warp >> 2, sc = warp & 3;
+    Dft dft;
+    dft.init(1.f);
+    const int nrg = (g.h2 + MRR - 1) / MRR;
+    for (int item = blockIdx.x; item < items; item += gridDim.x) {
+        const int yg = item % nrg;
+        const int o = (item / nrg) & 3;
+        const int plane = item / (nrg * 4);
+        const int y = yg * MRR + r;
+        if (y < g.h2) {  // warp-uniform
+            const __half2 *src = g.Th + (size_t(plane) * 16 + o * 4 + sc) * g.n + size_t(y) * W;
+            float2 *dst = sm + (r * 4 + sc) * Gm::RL;
+            dft.run([&](int n1, int n2) { return __half22float2(src[Dft::N2 * n1 + n2]); },
+                    [&](int k, float2 v) { dst[(k % Dft::N1) + Gm::RS * (k / Dft::N1)] = v; });
+        }
+        __syncthreads();
+        const int gp = g.pair0 * 2 + plane;
+        constexpr int QPR = W / 4;
+        for (int idx = threadIdx.x; idx < MRR * QPR; idx += blockDim.x) {
+            const int rl = idx / QPR;
+            const int x = (idx - rl * QPR) * 4;
+            const int yy = yg * MRR + rl;
+            if (yy >= g.h2) continue;
+            const int si = (x % Dft::N1) + Gm::RS * (x / Dft::N1);  // 4 consecutive outputs
+            float2 v[4][4];  // [scale][pixel]
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const float4 *p = reinterpret_cast<const float4 *>(sm + (rl * 4 + q) * Gm::RL + si);
+                const float4 lo = p[0], hi = p[1];
+                v[q][0] = make_float2(lo.x, lo.y);
+                v[q][1] = make_float2(lo.z, lo.w);
+                v[q][2] = make_float2(hi.x, hi.y);
+                v[q][3] = make_float2(hi.z, hi.w);
+            }
+            float4 oa, oe, o0;
+            float *pa = &oa.x, *pe = &oe.x, *p0 = &o0.x;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const float2 w[4] = {v[0][i], v[1][i], v[2][i], v[3][i]};
+                response_sums(w, 1.0f, pa[i], pe[i], p0[i]);  // already normalised
+            }
+            const size_t off = (size_t(gp) * 4 + o) * g.n + size_t(yy) * W + x;
+            *reinterpret_cast<float4 *>(g.amp + off) = oa;
+            *reinterpret_cast<float4 *>(g.energy + off) = oe;
+            *reinterpret_cast<float4 *>(g.eo0 + off) = o0;
+        }
+        __syncthreads();  // staging reads done before the next item's transforms overwrite it
+    }
+}
+
+// Tensor-core transform engines of the mixed forms: 270 = 15 x 18 (columns), 480 = 16 x 30 (rows).
+template <int SPLIT>
+using MmaCol270 = iqm::MmaDft<15, 18, SPLIT>;
+template <int SPLIT>
+using MmaRow480 = iqm::MmaDft<16, 30, SPLIT>;
+
 // sum the per-row constants in row order -> an2[mode][o], aiaj[mode][o]
 __global__ void fsim_consts_reduce_kernel(const double *rowsums, int h2, double *consts) {
     const int o = threadIdx.x;  // 4 threads
@@ -1267,13 +1426,14 @@ struct Layout {
 
 // G pairs of the group; chunk pairs' worth of inverse-pass intermediates.
 // nbuf: inverse-pass intermediate buffers (2 when consecutive chunks alternate between two streams).
-Layout layout_for(int G, int chunk, int n, int tiles, int nbuf = 1) {
+// tbytes: bytes per element of the intermediate planes (8: FP32 complex, 4: FP16 complex).
+Layout layout_for(int G, int chunk, int n, int tiles, int nbuf = 1, size_t tbytes = sizeof(float2)) {
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     Layout L{};
     size_t off = 0;
     L.yiq = off; off += al(sizeof(float) * size_t(G) * 6 * n);
     L.spec = off; off += al(sizeof(float2) * size_t(G) * n);
-    L.T = off; off += al(sizeof(float2) * size_t(nbuf) * chunk * 32 * n);
+    L.T = off; off += al(tbytes * size_t(nbuf) * chunk * 32 * n);
     L.planes = off; off += al(sizeof(float) * size_t(G) * 24 * n);
     L.thr = off; off += al(sizeof(float) * size_t(G) * 8);
     L.partials = off; off += al(sizeof(double) * size_t(G) * tiles * 3);
@@ -1284,9 +1444,39 @@ Layout layout_for(int G, int chunk, int n, int tiles, int nbuf = 1) {
 
 // Inverse-pass chunk: the 32 intermediate planes of `chunk` pairs stay within an L2 budget
 // (80 MB unless tuned).
-int chunk_pairs(const iqm::FsimTune &t, int G, int n) {
+int chunk_pairs(const iqm::FsimTune &t, int G, int n, size_t tbytes = sizeof(float2)) {
     const size_t budget = size_t(t.chunk_mb > 0 ? t.chunk_mb : 80) << 20;
-    return std::max(1, std::min(G, int(budget / (sizeof(float2) * 32 * size_t(n)))));
+    return std::max(1, std::min(G, int(budget / (tbytes * 32 * size_t(n)))));
+}
+
+// Tensor-core transform engines of the mixed forms exist for 480 x 270 planes (1080p and 4K pairs
+// downscale to them); other plane sizes run the FP32 transforms in the mixed forms too.
+bool mma_plane(int w2, int h2) { return w2 == 480 && h2 == 270; }
+
+// CTAs of a persistent kernel: the items, or as many CTAs as fit on the device at once.
+int persistent_grid(const void *fn, int threads, size_t smem, int items) {
+    int dev = 0, sms = 0, per_sm = 0;
+    IQM_CHECK_CUDA(cudaGetDevice(&dev));
+    IQM_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    set_smem(fn, smem);
+    IQM_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+    return std::max(1, std::min(items, sms * std::max(1, per_sm)));
+}
+
+template <int SPLIT>
+void launch_inv_mma(const FsimGroup &g, int planes, cudaStream_t st, iqm_ctx *ctx) {
+    using C = MmaCol270<SPLIT>;
+    using R = MmaRow480<SPLIT>;
+    const int citems = int(iqm::ceil_div(g.w2, MCW)) * 4 * planes;
+    const size_t csm = MmaColGeom<C>::smem;
+    const int cgrid = persistent_grid((const void *)fsim_inv_cols_mma_kernel<C>, 32 * MCW, csm, citems);
+    fsim_inv_cols_mma_kernel<C><<<cgrid, 32 * MCW, csm, st>>>(g, citems);
+    iqm::check_launch(ctx, "fsim_inv_cols_mma_kernel");
+    const int ritems = int(iqm::ceil_div(g.h2, MRR)) * 4 * planes;
+    const size_t rsm = MmaRowGeom<R>::smem;
+    const int rgrid = persistent_grid((const void *)fsim_inv_rows_mma_kernel<R>, 32 * 4 * MRR, rsm, ritems);
+    fsim_inv_rows_mma_kernel<R><<<rgrid, 32 * 4 * MRR, rsm, st>>>(g, ritems);
+    iqm::check_launch(ctx, "fsim_inv_rows_mma_kernel");
 }
 
 void launch_ingest(const FsimGroup &g, int F_uniform, int tiles, cudaStream_t st) {
@@ -1301,7 +1491,9 @@ void launch_ingest(const FsimGroup &g, int F_uniform, int tiles, cudaStream_t st
 }
 
 // Enqueue FSIM for device-resident pairs; scores[2*i], scores[2*i+1] = FSIM, FSIMc of pair i.
-void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_mode, double *d_scores) {
+// mma: 0 = FP32 transforms; 1 or 3 = tensor-core transforms with that many products per tile
+// (1: FP16 operands, 3: split-precision hi + lo operands) where the plane size has MMA engines.
+void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_mode, int mma, double *d_scores) {
     const int n_pairs = int(pairs.size());
     // group by plane size, keeping the caller's order inside each group
     std::map<std::pair<int, int>, std::vector<int>> groups;
@@ -1324,6 +1516,7 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
     // per-size tables first (building one waits for the context stream)
     struct GroupRun {
         int w2, h2, G, first, slot, F_uniform, chunk;
+        int mma;       // tensor-core inverse passes (0: FP32 engines), FP16 intermediate planes
         bool overlap;  // inverse-pass chunks alternate between two streams and two T buffers
         iqm::FsimPlan *P;
         Shapes s;
@@ -1342,12 +1535,14 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
             r.P = get_plan(ctx, r.w2, r.h2);
             r.s = shapes_for(*r.P, ctx->fsim_tune);
             const int n = r.P->n;
-            r.chunk = chunk_pairs(ctx->fsim_tune, r.G, n);
+            r.mma = mma_plane(r.w2, r.h2) ? mma : 0;
+            const size_t tbytes = r.mma ? sizeof(__half2) : sizeof(float2);
+            r.chunk = chunk_pairs(ctx->fsim_tune, r.G, n, tbytes);
             // More than one chunk: split the L2 budget over two buffers and let consecutive chunks run
             // on two streams, so one chunk's column pass fills the other's last partial wave.
             r.overlap = kOverlapChunks && !ctx->timing && r.G > r.chunk;
             if (r.overlap) r.chunk = std::max(1, r.chunk / kChunkStreams);
-            r.L = layout_for(r.G, r.chunk, n, int(iqm::ceil_div(n, FT)), r.overlap ? kChunkStreams : 1);
+            r.L = layout_for(r.G, r.chunk, n, int(iqm::ceil_div(n, FT)), r.overlap ? kChunkStreams : 1, tbytes);
             r.F_uniform = hd[kv.second[0]].F;
             for (int i : kv.second)
                 if (hd[i].F != r.F_uniform) r.F_uniform = 0;
@@ -1454,9 +1649,18 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
             FsimGroup gc = g;
             gc.pair0 = c0;
             const int j = k % nst;
-            gc.T = g.T + size_t(j) * chunk * 32 * n;
             cudaStream_t cs = cstream[j];
             const int cg = std::min(chunk, G - c0);
+            if (r.mma) {
+                gc.Th = reinterpret_cast<__half2 *>(g.T) + size_t(j) * chunk * 32 * n;
+                gc.T = nullptr;
+                if (r.mma == 3)
+                    launch_inv_mma<3>(gc, 2 * cg, cs, ctx);
+                else
+                    launch_inv_mma<1>(gc, 2 * cg, cs, ctx);
+                continue;
+            }
+            gc.T = g.T + size_t(j) * chunk * 32 * n;
             launch_inv_cols(gc, *P, s, 2 * cg, 0, cs);
             iqm::check_launch(ctx, "fsim_inv_cols_kernel");
             launch_inv_rows(gc, *P, s, 2 * cg, 0, nullptr, cs);
@@ -1485,9 +1689,7 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
 void check_fsim_args(const iqm_pair *pairs, int n, iqm_precision precision, int energy_mode) {
     iqm::check_pairs(pairs, n, 1, 1);
     IQM_REQUIRE(energy_mode == 0 || energy_mode == 1, "energy_mode must be 0 or 1");
-    IQM_REQUIRE(precision == IQM_FP32 || precision == IQM_MIXED, "unknown precision");
-    if (precision == IQM_MIXED)
-        throw iqm::Error{IQM_EUNSUPPORTED, "FSIM: no reduced-precision form in this build (use IQM_FP32)"};
+    IQM_REQUIRE(precision == IQM_FP32 || precision == IQM_MIXED || precision == IQM_MIXED_FAST, "unknown precision");
     for (int i = 0; i < n; i++) {
         const int F = downscale_factor(pairs[i].w, pairs[i].h);
         int w2, h2;
@@ -1496,6 +1698,9 @@ void check_fsim_args(const iqm_pair *pairs, int n, iqm_precision precision, int 
                     "pair " + std::to_string(i) + ": FSIM plane size out of range");
     }
 }
+
+// Products per tensor-core tile of the mixed forms (0: the FP32 form).
+int mma_terms(iqm_precision p) { return p == IQM_MIXED ? 3 : p == IQM_MIXED_FAST ? 1 : 0; }
 
 }  // namespace
 
@@ -1511,7 +1716,7 @@ void iqm::enqueue_fsim_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, iqm_preci
     check_fsim_args(pairs, n, precision, energy_mode);
     iqm::check_dev_alignment(pairs, n);
     IQM_REQUIRE(d_scores != nullptr, "d_scores is NULL");
-    fsim_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), energy_mode, d_scores);
+    fsim_enqueue(ctx, std::vector<iqm_pair>(pairs, pairs + n), energy_mode, mma_terms(precision), d_scores);
 }
 
 IQM_API int iqm_fsim_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, iqm_precision precision, int energy_mode,
@@ -1526,7 +1731,7 @@ IQM_API int iqm_fsim_batch(iqm_ctx *ctx, const iqm_pair *pairs, int n, iqm_preci
         IQM_REQUIRE(scores != nullptr, "scores is NULL");
         auto dev = iqm::upload_pairs(ctx, pairs, n);
         auto *d_scores = static_cast<double *>(ctx->scores.get(sizeof(double) * 2 * n, ctx->stream));
-        fsim_enqueue(ctx, dev, energy_mode, d_scores);
+        fsim_enqueue(ctx, dev, energy_mode, mma_terms(precision), d_scores);
         IQM_CHECK_CUDA(cudaMemcpyAsync(scores, d_scores, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, ctx->stream));
         IQM_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
     });
@@ -1540,7 +1745,7 @@ IQM_API int iqm_fsim(iqm_ctx *ctx, const uint8_t *rgba_in, const uint8_t *rgba_r
         check_fsim_args(&hp, 1, precision, energy_mode);
         auto dev = iqm::upload_pairs(ctx, &hp, 1);
         auto *d_scores = static_cast<double *>(ctx->scores.get(sizeof(double) * 2, ctx->stream));
-        fsim_enqueue(ctx, dev, energy_mode, d_scores);
+        fsim_enqueue(ctx, dev, energy_mode, mma_terms(precision), d_scores);
         double out[2];
         IQM_CHECK_CUDA(cudaMemcpyAsync(out, d_scores, sizeof(out), cudaMemcpyDeviceToHost, ctx->stream));
         IQM_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));

@@ -53,3 +53,14 @@ def test_flip_rejects_bad_params(rt):
     a = np.zeros((16, 16, 4), np.uint8)
     with pytest.raises(iqm_b200.IQMError):
         iqm_b200.FLIP(rt).compute_metric(a, a, iqm_b200.FLIPArguments(2560.0, 0.7, 0.0))
+
+
+@pytest.mark.parametrize("args", [ARGS_67, iqm_b200.FLIPArguments()])
+def test_flip_matches_independent_restatement(rt, args):
+    """Against the whole-plane numpy restatement (oracle/np_restatement.py), written from the
+    shaders independently of the C oracle."""
+    import np_restatement
+    a, b = synth.rgb_blockquant_pair(270, 480, config=2, pair=2)
+    f = iqm_b200.FLIP(rt)
+    want = np_restatement.flip(a, b, f.ppd(args))
+    assert abs(f.compute_metric(a, b, args).mean_flip - want) <= TOL

@@ -91,10 +91,71 @@ def test_fsim_errors(rt):
     assert e.value.code == iqm_b200.IQM_EINVAL
 
 
-def test_fsim_mixed_precision_is_reported_unsupported(rt):
+MIXED_TOL = 1e-4  # the mixed forms' bound against the FP64 oracle
+MIXED = [iqm_b200.IQM_MIXED, iqm_b200.IQM_MIXED_FAST]
+
+
+@pytest.mark.parametrize("precision", MIXED)
+@pytest.mark.parametrize("h,w,pair", [(1080, 1920, 0), (1080, 1920, 1), (2160, 3840, 0), (1920, 1080, 2)])
+def test_fsim_mixed_within_bound_of_fp64(rt, o64, precision, h, w, pair):
+    """Tensor-core inverse transforms (1080p and 4K pairs: 480x270 planes) and FP16 intermediate
+    planes: both scores within 1e-4 of the FP64 oracle.  The portrait pair has a 270x480 plane,
+    which has no tensor-core engines and runs the FP32 transforms."""
+    a, b = synth.rgb_gain_pair(h, w, config=1, pair=pair)
+    r = iqm_b200.FSIM(rt, precision=precision).compute_metric(a, b)
+    f64, fc64 = o64.fsim(a, b)
+    assert abs(r.fsim - f64) <= MIXED_TOL and abs(r.fsimc - fc64) <= MIXED_TOL, (r, f64, fc64)
+
+
+@pytest.mark.parametrize("precision", MIXED)
+def test_fsim_mixed_energy_mode_and_identity(rt, o64, precision):
+    a, b = synth.rgb_gain_pair(1080, 1920, config=1, pair=4)
+    r = iqm_b200.FSIM(rt, precision=precision, energy_mode=1).compute_metric(a, b)
+    f, fc = o64.fsim(a, b, energy_full=True)
+    assert abs(r.fsim - f) <= MIXED_TOL and abs(r.fsimc - fc) <= MIXED_TOL
+    same = iqm_b200.FSIM(rt, precision=precision).compute_metric(b, b)
+    assert same.fsim == pytest.approx(1.0, abs=1e-6) and same.fsimc == pytest.approx(1.0, abs=1e-6)
+
+
+@pytest.mark.parametrize("precision", MIXED)
+def test_fsim_mixed_batch_matches_single_and_oracle(rt, o64, precision):
+    """A batch mixing tensor-core (1080p) and FP32-transform plane sizes; several 1080p pairs so the
+    inverse passes run in more than one chunk."""
+    sizes = [(1080, 1920)] * 5 + [(130, 200), (600, 800), (1080, 1920)]
+    pairs = [synth.rgb_gain_pair(h, w, config=1, pair=i) for i, (h, w) in enumerate(sizes)]
+    f = iqm_b200.FSIM(rt, precision=precision)
+    got = f.compute_batch(pairs)
+    for (a, b), g in zip(pairs, got):
+        single = f.compute_metric(a, b)
+        assert g[0] == single.fsim and g[1] == single.fsimc
+        w64 = o64.fsim(a, b)
+        assert abs(g[0] - w64[0]) <= MIXED_TOL and abs(g[1] - w64[1]) <= MIXED_TOL
+
+
+def test_fsim_mixed_deterministic(rt):
+    a, b = synth.rgb_gain_pair(1080, 1920, config=1, pair=6)
+    f = iqm_b200.FSIM(rt, precision=iqm_b200.IQM_MIXED)
+    v = [f.compute_metric(a, b) for _ in range(3)]
+    assert v[0] == v[1] == v[2]
+
+
+def test_fsim_unknown_precision_rejected(rt):
     a, b = synth.rgb_gain_pair(64, 80, config=1, pair=1)
     with pytest.raises(iqm_b200.IQMError) as e:
-        iqm_b200.FSIM(rt, precision=iqm_b200.IQM_MIXED).compute_metric(a, b)
-    assert e.value.code == iqm_b200.IQM_EUNSUPPORTED
+        iqm_b200.FSIM(rt, precision=7).compute_metric(a, b)
+    assert e.value.code == iqm_b200.IQM_EINVAL
     # the context stays usable
     assert 0.0 < iqm_b200.FSIM(rt).compute_metric(a, b).fsim <= 1.0
+
+
+@pytest.mark.parametrize("h,w", [(1080, 1920), (131, 263), (300, 2048)])
+def test_fsim_matches_independent_restatement(rt, h, w):
+    """Against the whole-plane numpy restatement (oracle/np_restatement.py), written from the
+    shaders independently of the C oracle."""
+    import np_restatement
+    a, b = synth.rgb_gain_pair(h, w, config=1, pair=9)
+    want = np_restatement.fsim(a, b)
+    r = iqm_b200.FSIM(rt).compute_metric(a, b)
+    assert abs(r.fsim - want[0]) <= TOL and abs(r.fsimc - want[1]) <= TOL
+    m = iqm_b200.FSIM(rt, precision=iqm_b200.IQM_MIXED).compute_metric(a, b)
+    assert abs(m.fsim - want[0]) <= MIXED_TOL and abs(m.fsimc - want[1]) <= MIXED_TOL
