@@ -70,6 +70,12 @@ extern "C" __attribute__((visibility("default"))) int iqm_destroy(iqm_ctx *ctx) 
     for (auto ev : ctx->side_events) cudaEventDestroy(ev);
     for (auto ev : ctx->aux_events) cudaEventDestroy(ev);
     if (ctx->fork_event) cudaEventDestroy(ctx->fork_event);
+    if (ctx->copy_stream) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        cudaStreamDestroy(ctx->copy_stream);
+    }
+    for (auto ev : ctx->copy_events)
+        if (ev) cudaEventDestroy(ev);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return IQM_OK;
@@ -182,34 +188,91 @@ cudaEvent_t aux_event(iqm_ctx *ctx, int i) {
     return ctx->aux_events[i];
 }
 
-std::vector<iqm_pair> upload_pairs(iqm_ctx *ctx, const iqm_pair *pairs, int n) {
-    // Device copies use a 16-byte-aligned pitch so kernels can take their vector-load path.
+// Device layout of host pairs in ctx->images: a 16-byte-aligned pitch per image (so kernels can
+// take their vector-load path); returns the descriptors with device pointers.
+static std::vector<iqm_pair> device_layout(iqm_ctx *ctx, const iqm_pair *pairs, int n) {
     std::vector<iqm_pair> dev(pairs, pairs + n);
     std::vector<size_t> offs(n);
     size_t total = 0;
     for (int i = 0; i < n; i++) {
-        size_t pitch = (size_t(pairs[i].w) * 4 + 15) & ~size_t(15);
-        size_t bytes = (pitch * size_t(pairs[i].h) + 255) & ~size_t(255);
+        const size_t pitch = (size_t(pairs[i].w) * 4 + 15) & ~size_t(15);
+        const size_t bytes = (pitch * size_t(pairs[i].h) + 255) & ~size_t(255);
         offs[i] = total;
         total += 2 * bytes;
         dev[i].row_bytes = pitch;
     }
     auto *base = static_cast<uint8_t *>(ctx->images.get(total, ctx->stream));
     for (int i = 0; i < n; i++) {
-        size_t pitch = dev[i].row_bytes;
-        size_t bytes = (pitch * size_t(pairs[i].h) + 255) & ~size_t(255);
-        uint8_t *din = base + offs[i], *dref = base + offs[i] + bytes;
-        IQM_CHECK_CUDA(cudaMemcpy2DAsync(din, pitch, pairs[i].input, pairs[i].row_bytes,
-                                         size_t(pairs[i].w) * 4, pairs[i].h, cudaMemcpyHostToDevice,
-                                         ctx->stream));
-        IQM_CHECK_CUDA(cudaMemcpy2DAsync(dref, pitch, pairs[i].ref, pairs[i].row_bytes,
-                                         size_t(pairs[i].w) * 4, pairs[i].h, cudaMemcpyHostToDevice,
-                                         ctx->stream));
-        dev[i].input = din;
-        dev[i].ref = dref;
+        const size_t bytes = (dev[i].row_bytes * size_t(pairs[i].h) + 255) & ~size_t(255);
+        dev[i].input = base + offs[i];
+        dev[i].ref = base + offs[i] + bytes;
+    }
+    return dev;
+}
+
+// Copies one image: a single linear copy when both pitches equal the row, else a 2-D copy.
+static void copy_image(const uint8_t *dst, size_t dpitch, const uint8_t *src, size_t spitch, int w, int h,
+                       cudaStream_t st) {
+    const size_t row = size_t(w) * 4;
+    void *d = const_cast<uint8_t *>(dst);
+    if (spitch == row && dpitch == row) {
+        IQM_CHECK_CUDA(cudaMemcpyAsync(d, src, row * size_t(h), cudaMemcpyHostToDevice, st));
+    } else {
+        IQM_CHECK_CUDA(cudaMemcpy2DAsync(d, dpitch, src, spitch, row, h, cudaMemcpyHostToDevice, st));
+    }
+}
+
+std::vector<iqm_pair> upload_pairs(iqm_ctx *ctx, const iqm_pair *pairs, int n) {
+    std::vector<iqm_pair> dev = device_layout(ctx, pairs, n);
+    for (int i = 0; i < n; i++) {
+        copy_image(dev[i].input, dev[i].row_bytes, pairs[i].input, pairs[i].row_bytes, pairs[i].w, pairs[i].h,
+                   ctx->stream);
+        copy_image(dev[i].ref, dev[i].row_bytes, pairs[i].ref, pairs[i].row_bytes, pairs[i].w, pairs[i].h, ctx->stream);
     }
     timing_mark(ctx, nullptr);
     return dev;
+}
+
+void upload_pipelined(iqm_ctx *ctx, const iqm_pair *pairs, int n,
+                      const std::function<void(const iqm_pair *dev, int first, int count)> &run) {
+    std::vector<iqm_pair> dev = device_layout(ctx, pairs, n);
+    size_t total = 0;
+    for (int i = 0; i < n; i++) total += 2 * dev[i].row_bytes * size_t(pairs[i].h);
+    // about eight chunks of whole pairs, none below 32 MB of images (a chunk's kernels then run
+    // long enough to cover the start of the next copy)
+    constexpr size_t kMinChunk = size_t(32) << 20;
+    const size_t target = std::max(kMinChunk, total / 8);
+    const bool overlap = !ctx->timing && total > target;
+    cudaStream_t cs = ctx->stream;
+    if (overlap) {
+        if (!ctx->copy_stream) IQM_CHECK_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+        for (auto &ev : ctx->copy_events)
+            if (!ev) IQM_CHECK_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        cs = ctx->copy_stream;
+        // work already enqueued on the context stream may still read the image buffer
+        IQM_CHECK_CUDA(cudaEventRecord(ctx->copy_events[0], ctx->stream));
+        IQM_CHECK_CUDA(cudaStreamWaitEvent(cs, ctx->copy_events[0], 0));
+    }
+    for (int first = 0; first < n;) {
+        int last = first;
+        size_t bytes = 0;
+        do {
+            bytes += 2 * dev[last].row_bytes * size_t(pairs[last].h);
+            last++;
+        } while (last < n && bytes < target);
+        for (int i = first; i < last; i++) {
+            copy_image(dev[i].input, dev[i].row_bytes, pairs[i].input, pairs[i].row_bytes, pairs[i].w, pairs[i].h, cs);
+            copy_image(dev[i].ref, dev[i].row_bytes, pairs[i].ref, pairs[i].row_bytes, pairs[i].w, pairs[i].h, cs);
+        }
+        if (overlap) {
+            // a wait takes the event's state at the time of the call, so one event serves every chunk
+            IQM_CHECK_CUDA(cudaEventRecord(ctx->copy_events[1], cs));
+            IQM_CHECK_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->copy_events[1], 0));
+        }
+        timing_mark(ctx, nullptr);
+        run(dev.data() + first, first, last - first);
+        first = last;
+    }
 }
 
 // Charges every kernel mark the interval since the mark before it, then recycles the events.

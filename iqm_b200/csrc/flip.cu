@@ -724,9 +724,10 @@ IQM_API int iqm_flip_batch(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm
         check_params(p);
         iqm::check_pairs(pairs, n, 1, 1);
         IQM_REQUIRE(scores != nullptr, "scores is NULL");
-        auto dev = iqm::upload_pairs(ctx, pairs, n);
         auto *d_scores = static_cast<double *>(ctx->scores.get(sizeof(double) * n, ctx->stream));
-        flip_enqueue(ctx, dev, p, {}, d_scores);
+        iqm::upload_pipelined(ctx, pairs, n, [&](const iqm_pair *dev, int first, int count) {
+            flip_enqueue(ctx, std::vector<iqm_pair>(dev, dev + count), p, {}, d_scores + first);
+        });
         IQM_CHECK_CUDA(cudaMemcpyAsync(scores, d_scores, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
         IQM_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
     });

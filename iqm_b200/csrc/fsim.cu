@@ -1729,9 +1729,11 @@ IQM_API int iqm_fsim_batch(iqm_ctx *ctx, const iqm_pair *pairs, int n, iqm_preci
     return iqm::guarded(ctx, [&] {
         check_fsim_args(pairs, n, precision, energy_mode);
         IQM_REQUIRE(scores != nullptr, "scores is NULL");
-        auto dev = iqm::upload_pairs(ctx, pairs, n);
         auto *d_scores = static_cast<double *>(ctx->scores.get(sizeof(double) * 2 * n, ctx->stream));
-        fsim_enqueue(ctx, dev, energy_mode, mma_terms(precision), d_scores);
+        iqm::upload_pipelined(ctx, pairs, n, [&](const iqm_pair *dev, int first, int count) {
+            fsim_enqueue(ctx, std::vector<iqm_pair>(dev, dev + count), energy_mode, mma_terms(precision),
+                         d_scores + 2 * first);
+        });
         IQM_CHECK_CUDA(cudaMemcpyAsync(scores, d_scores, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, ctx->stream));
         IQM_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
     });

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <functional>
 #include <map>
 #include <memory>
 #include <string>
@@ -134,6 +135,10 @@ struct iqm_ctx {
     std::vector<cudaEvent_t> side_events;
     cudaEvent_t fork_event = nullptr;
     std::vector<cudaEvent_t> aux_events;  // further fork points (iqm::aux_event)
+    // host-image uploads of the batch entry points run on their own stream, chunk by chunk, so a
+    // chunk's copy overlaps the previous chunk's kernels (iqm::upload_pipelined)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copy_events[2] = {nullptr, nullptr};
 
     // named scratch areas (each grow-only)
     iqm::DevBuf desc;      // per-call pair descriptors
@@ -230,6 +235,13 @@ cudaEvent_t aux_event(iqm_ctx *ctx, int i);
 
 // Copies host pairs to device memory (inside ctx->images) and rewrites the pointers.
 std::vector<iqm_pair> upload_pairs(iqm_ctx *ctx, const iqm_pair *pairs, int n);
+
+// Copies host pairs to device memory in chunks of whole pairs on the context's copy stream and,
+// as each chunk lands, calls run(dev, first, count) to enqueue that chunk's work on the context
+// stream (dev: the chunk's device descriptors; first: its index in `pairs`): chunk k + 1's copy
+// overlaps chunk k's kernels.  Per-kernel timing keeps everything on the context stream.
+void upload_pipelined(iqm_ctx *ctx, const iqm_pair *pairs, int n,
+                      const std::function<void(const iqm_pair *dev, int first, int count)> &run);
 
 // Validate and enqueue one metric for device-resident pairs on the context stream (the bodies of
 // the iqm_*_dev entry points); batch plans call them directly.

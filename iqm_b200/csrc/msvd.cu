@@ -300,9 +300,10 @@ extern "C" __attribute__((visibility("default"))) int iqm_msvd_batch(iqm_ctx *ct
     return iqm::guarded(ctx, [&] {
         check_msvd_pairs(pairs, n);
         IQM_REQUIRE(scores != nullptr, "scores is NULL");
-        auto dev = iqm::upload_pairs(ctx, pairs, n);
         auto *d_scores = static_cast<double *>(ctx->scores.get(sizeof(double) * n, ctx->stream));
-        msvd_enqueue(ctx, dev, {}, d_scores);
+        iqm::upload_pipelined(ctx, pairs, n, [&](const iqm_pair *dev, int first, int count) {
+            msvd_enqueue(ctx, std::vector<iqm_pair>(dev, dev + count), {}, d_scores + first);
+        });
         IQM_CHECK_CUDA(cudaMemcpyAsync(scores, d_scores, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
         IQM_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
     });

@@ -219,18 +219,16 @@ IQM_API int iqm_batch(iqm_ctx *ctx, int metric_mask, const iqm_pair *pairs, int 
         IQM_REQUIRE(scores != nullptr, "scores is NULL");
         const BatchArgs a = resolve_args(metric_mask, ssim, flip, precision, energy_mode);
         const int k = scores_per_pair(metric_mask);
-        auto dev = iqm::upload_pairs(ctx, pairs, n);
         auto *d_scores = static_cast<double *>(ctx->scores.get(sizeof(double) * size_t(k) * n, ctx->stream));
-        double *out = d_scores;
-        int launches = 0;
-        for (int m = 0; m < 4; m++) {
-            if (!(metric_mask & kMetrics[m])) continue;
-            ctx->launches = 0;
-            enqueue_metric(ctx, m, a, dev.data(), n, out);
-            launches += ctx->launches;
-            out += size_t(kScores[m]) * n;
-        }
-        ctx->launches = launches;
+        // scores metric by metric (n per metric, 2n for FSIM); each chunk of pairs fills its slice
+        iqm::upload_pipelined(ctx, pairs, n, [&](const iqm_pair *dev, int first, int count) {
+            double *out = d_scores;
+            for (int m = 0; m < 4; m++) {
+                if (!(metric_mask & kMetrics[m])) continue;
+                enqueue_metric(ctx, m, a, dev, count, out + size_t(kScores[m]) * first);
+                out += size_t(kScores[m]) * n;
+            }
+        });
         IQM_CHECK_CUDA(cudaMemcpyAsync(scores, d_scores, sizeof(double) * size_t(k) * n, cudaMemcpyDeviceToHost,
                                        ctx->stream));
         IQM_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));

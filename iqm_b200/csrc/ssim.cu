@@ -440,9 +440,10 @@ extern "C" __attribute__((visibility("default"))) int iqm_ssim_batch(iqm_ctx *ct
         const int R = (p.kernel_size - 1) / 2;
         iqm::check_pairs(pairs, n, R, R);
         IQM_REQUIRE(scores != nullptr, "scores is NULL");
-        auto dev = iqm::upload_pairs(ctx, pairs, n);
         auto *d_scores = static_cast<double *>(ctx->scores.get(sizeof(double) * n, ctx->stream));
-        ssim_enqueue(ctx, dev, p, {}, d_scores);
+        iqm::upload_pipelined(ctx, pairs, n, [&](const iqm_pair *dev, int first, int count) {
+            ssim_enqueue(ctx, std::vector<iqm_pair>(dev, dev + count), p, {}, d_scores + first);
+        });
         IQM_CHECK_CUDA(cudaMemcpyAsync(scores, d_scores, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
         IQM_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
     });
