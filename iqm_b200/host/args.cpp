@@ -51,3 +51,21 @@ IQM::Args::Args(const unsigned argc, const char *argv[]) {
     if (!have_input && !batch) throw std::runtime_error("missing input");
     if (!have_ref && !batch) throw std::runtime_error("missing reference");
 }
+
+// --precision fp32 | mixed | mixed_fast (FSIM's forms; the other metrics compute in FP32).
+iqm_precision IQM::precision_option(const Args &args) {
+    auto it = args.options.find("--precision");
+    if (it == args.options.end() || it->second == "fp32") return IQM_FP32;
+    if (it->second == "mixed") return IQM_MIXED;
+    if (it->second == "mixed_fast") return IQM_MIXED_FAST;
+    throw std::runtime_error("--precision must be fp32, mixed or mixed_fast");
+}
+
+// FSIM_ENERGY_SUM reference | full: how FSIM pools its noise-energy estimates (the reference's
+// shader fills the first ceil(N/2) pixels only; "full" pools all N).
+int IQM::energy_option(const Args &args) {
+    auto it = args.options.find("FSIM_ENERGY_SUM");
+    if (it == args.options.end() || it->second == "reference") return 0;
+    if (it->second == "full") return 1;
+    throw std::runtime_error("FSIM_ENERGY_SUM must be reference or full");
+}

@@ -117,12 +117,12 @@ const char *label(IQM::Method m) {
 }
 
 // Evaluates n decoded pairs with one batch call; k scores per pair (k = 2 for FSIM).
-int evaluate(const IQM::CUDA::Runtime &rt, IQM::Method m, const iqm_flip_params &flip, const iqm_pair *pairs, int n,
-             double *scores) {
+int evaluate(const IQM::CUDA::Runtime &rt, IQM::Method m, const iqm_flip_params &flip, iqm_precision precision,
+             int energy_mode, const iqm_pair *pairs, int n, double *scores) {
     switch (m) {
         case IQM::Method::SSIM: return iqm_ssim_batch(rt.ctx, pairs, n, nullptr, scores);
         case IQM::Method::SVD: return iqm_msvd_batch(rt.ctx, pairs, n, scores);
-        case IQM::Method::FSIM: return iqm_fsim_batch(rt.ctx, pairs, n, IQM_FP32, 0, scores);
+        case IQM::Method::FSIM: return iqm_fsim_batch(rt.ctx, pairs, n, precision, energy_mode, scores);
         case IQM::Method::FLIP: return iqm_flip_batch(rt.ctx, pairs, n, &flip, scores);
         default: return IQM_OK;
     }
@@ -149,6 +149,8 @@ int IQM::run_batch(const Args &args) {
     if (args.options.count("FLIP_WIDTH")) flip.monitor_width = std::stof(args.options.at("FLIP_WIDTH"));
     if (args.options.count("FLIP_RES")) flip.monitor_resolution_x = std::stof(args.options.at("FLIP_RES"));
     if (args.options.count("FLIP_DISTANCE")) flip.monitor_distance = std::stof(args.options.at("FLIP_DISTANCE"));
+    const iqm_precision precision = precision_option(args);
+    const int energy_mode = energy_option(args);
     if (args.method == Method::CW_SSIM_CPU) return 0;  // the reference's CW-SSIM is an empty stub
     const CUDA::Runtime rt;
     const int k = args.method == Method::FSIM ? 2 : 1;
@@ -178,10 +180,10 @@ int IQM::run_batch(const Args &args) {
         for (size_t i = 0; i < cur.count; i++) err[i] = cur.error[i];
         if (!ok.empty()) {
             const auto g0 = clk::now();
-            int rc = evaluate(rt, args.method, flip, ok.data(), int(ok.size()), scores.data());
+            int rc = evaluate(rt, args.method, flip, precision, energy_mode, ok.data(), int(ok.size()), scores.data());
             if (rc != IQM_OK) {  // find the pairs the call rejects, evaluate the rest one by one
                 for (size_t q = 0; q < ok.size(); q++)
-                    if (evaluate(rt, args.method, flip, &ok[q], 1, &scores[k * q]) != IQM_OK)
+                    if (evaluate(rt, args.method, flip, precision, energy_mode, &ok[q], 1, &scores[k * q]) != IQM_OK)
                         err[where[q]] = iqm_last_error(rt.ctx);
             }
             gpu_s += std::chrono::duration<double>(clk::now() - g0).count();

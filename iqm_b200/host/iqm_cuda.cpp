@@ -62,9 +62,14 @@ FLIPResult FLIP::computeMetric(const Runtime &rt, const InputImage &image, const
     FLIPResult res{0.f, {}};
     const iqm_flip_params p{args.monitor_resolution_x, args.monitor_distance, args.monitor_width};
     double m = 0;
+    if (wantMap) {
+        res.imageData.resize(size_t(image.width) * image.height);
+        res.width = unsigned(image.width);
+        res.height = unsigned(image.height);
+    }
     res.timestamps.mark("start GPU pipeline");
     rt.check(iqm_flip(rt.ctx, image.data.data(), ref.data.data(), image.width, image.height, size_t(image.width) * 4,
-                      &p, nullptr, &m));
+                      &p, wantMap ? res.imageData.data() : nullptr, &m));
     res.mean_flip = float(m);
     res.timestamps.mark("FLIP computed");
     return res;

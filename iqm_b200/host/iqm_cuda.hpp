@@ -75,6 +75,10 @@ public:
 struct FLIPResult {  // src/gpu/flip/flip.h:16-19; mean_flip is assigned here
     float mean_flip;
     Timestamps timestamps;
+    // the per-pixel FLIP value (combine_error_maps.glsl:28), filled when FLIP::wantMap is set
+    std::vector<float> imageData;
+    unsigned int width = 0;
+    unsigned int height = 0;
 };
 
 struct FLIPArguments {  // src/gpu/flip/flip.h:21-25
@@ -88,6 +92,7 @@ public:
     explicit FLIP(const Runtime &) {}
     FLIPResult computeMetric(const Runtime &runtime, const InputImage &image, const InputImage &ref,
                              const FLIPArguments &args);
+    bool wantMap = false;
 };
 
 }  // namespace IQM::CUDA

@@ -16,11 +16,13 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <cmath>
 
 #include "args.h"
 #include "batch_pipeline.h"
 #include "iqm_cuda.hpp"
 #include "png_io.h"
+#include "viridis_table.h"
 
 namespace {
 
@@ -77,6 +79,23 @@ void save_map(const IQM::Args &args, unsigned w, unsigned h, const std::vector<f
         throw std::runtime_error("Failed to save output image");
 }
 
+// FLIP --output: each pixel's FLIP value v in [0, 1] shown as viridis entry floor(v * 255), as the
+// reference's combine pass colours its output image (shaders/flip/combine_error_maps.glsl:28-32);
+// written as RGBA8 (alpha 255, the map's 1.0).
+void save_flip_map(const IQM::Args &args, unsigned w, unsigned h, const std::vector<float> &map) {
+    if (!args.outputPath.has_value()) return;
+    std::vector<unsigned char> rgba(size_t(w) * h * 4);
+    for (size_t i = 0; i < map.size(); i++) {
+        const int idx = std::clamp(int(std::floor(map[i] * 255.0f)), 0, 255);
+        rgba[4 * i] = IQM::kViridisRGB[idx][0];
+        rgba[4 * i + 1] = IQM::kViridisRGB[idx][1];
+        rgba[4 * i + 2] = IQM::kViridisRGB[idx][2];
+        rgba[4 * i + 3] = 255;
+    }
+    if (!IQM::write_png(args.outputPath.value(), int(w), int(h), 4, rgba))
+        throw std::runtime_error("Failed to save output image");
+}
+
 void ssim(const IQM::Args &args) {
     InputImage input, ref;
     load_pair(args, input, ref);
@@ -110,6 +129,8 @@ void fsim(const IQM::Args &args) {
     load_pair(args, input, ref);
     const IQM::CUDA::Runtime rt;
     IQM::CUDA::FSIM metric(rt);
+    metric.precision = IQM::precision_option(args);
+    metric.energyMode = IQM::energy_option(args);
     if (args.verbose) std::cout << "Selected device: " << rt.selectedDevice << std::endl;
     const auto start = clk::now();
     auto result = repeated(args, [&] { return metric.computeMetric(rt, input, ref); });
@@ -123,6 +144,7 @@ void flip(const IQM::Args &args) {
     load_pair(args, input, ref);
     const IQM::CUDA::Runtime rt;
     IQM::CUDA::FLIP metric(rt);
+    metric.wantMap = args.outputPath.has_value();
     IQM::CUDA::FLIPArguments flip_args;
     if (args.options.count("FLIP_WIDTH")) flip_args.monitor_width = std::stof(args.options.at("FLIP_WIDTH"));
     if (args.options.count("FLIP_RES")) flip_args.monitor_resolution_x = std::stof(args.options.at("FLIP_RES"));
@@ -138,6 +160,7 @@ void flip(const IQM::Args &args) {
     const auto end = clk::now();
     std::cout << "FLIP: " << result.mean_flip << std::endl;
     if (args.verbose) result.timestamps.print(start, end);
+    save_flip_map(args, result.width, result.height, result.imageData);
 }
 
 }  // namespace
@@ -146,6 +169,8 @@ int main(int argc, const char **argv) {
     auto args = IQM::Args(argc, argv);
     if (args.verbose) std::cout << "Selected method: " << IQM::method_name(args.method) << std::endl;
     try {
+        IQM::precision_option(args);  // reject a bad value before any work
+        IQM::energy_option(args);
         if (args.options.count("--batch")) return IQM::run_batch(args);
         switch (args.method) {
             case IQM::Method::SSIM: ssim(args); break;

@@ -213,12 +213,15 @@ InputImage load_image(const std::string &path) {
     }
 }
 
-std::vector<unsigned char> encode_grey_png(int width, int height, const std::vector<unsigned char> &pixels) {
+std::vector<unsigned char> encode_png(int width, int height, int channels, const std::vector<unsigned char> &pixels) {
+    if (channels != 1 && channels != 3 && channels != 4) throw std::runtime_error("PNG: 1, 3 or 4 channels");
+    const size_t row = size_t(width) * channels;
+    if (pixels.size() < row * size_t(height)) throw std::runtime_error("PNG: pixel buffer too small");
     std::vector<unsigned char> raw;
-    raw.reserve(size_t(height) * (width + 1));
+    raw.reserve(size_t(height) * (row + 1));
     for (int y = 0; y < height; y++) {
         raw.push_back(0);
-        raw.insert(raw.end(), pixels.begin() + size_t(y) * width, pixels.begin() + size_t(y + 1) * width);
+        raw.insert(raw.end(), pixels.begin() + size_t(y) * row, pixels.begin() + size_t(y + 1) * row);
     }
     uLongf zlen = compressBound(uLong(raw.size()));
     std::vector<unsigned char> z(zlen);
@@ -235,22 +238,31 @@ std::vector<unsigned char> encode_grey_png(int width, int height, const std::vec
     std::vector<unsigned char> ihdr;
     put32(ihdr, uint32_t(width));
     put32(ihdr, uint32_t(height));
-    ihdr.insert(ihdr.end(), {8, 0, 0, 0, 0});
+    const unsigned char color_type = channels == 1 ? 0 : channels == 3 ? 2 : 6;
+    ihdr.insert(ihdr.end(), {8, color_type, 0, 0, 0});
     chunk("IHDR", ihdr);
     chunk("IDAT", z);
     chunk("IEND", {});
     return o;
 }
 
-bool write_grey_png(const std::string &path, int width, int height, const std::vector<unsigned char> &pixels) {
+std::vector<unsigned char> encode_grey_png(int width, int height, const std::vector<unsigned char> &pixels) {
+    return encode_png(width, height, 1, pixels);
+}
+
+bool write_png(const std::string &path, int width, int height, int channels, const std::vector<unsigned char> &pixels) {
     try {
-        const auto bytes = encode_grey_png(width, height, pixels);
+        const auto bytes = encode_png(width, height, channels, pixels);
         std::ofstream out(path, std::ios::binary);
         out.write(reinterpret_cast<const char *>(bytes.data()), std::streamsize(bytes.size()));
         return bool(out);
     } catch (...) {
         return false;
     }
+}
+
+bool write_grey_png(const std::string &path, int width, int height, const std::vector<unsigned char> &pixels) {
+    return write_png(path, width, height, 1, pixels);
 }
 
 }  // namespace IQM

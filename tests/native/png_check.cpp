@@ -1,6 +1,7 @@
 // Test harness: decodes an image file with the command line's decoder and writes the RGBA8 pixels
 // (width, height as two little-endian uint32 values, then the bytes) to stdout; with "--encode W H"
-// it reads W*H grey bytes from stdin and writes a PNG to stdout.
+// it reads W*H grey bytes from stdin and writes a PNG to stdout ("--encode W H C": W*H*C bytes of C
+// interleaved channels, C = 1, 3 or 4).
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -12,11 +13,11 @@
 
 int main(int argc, char **argv) {
     try {
-        if (argc == 4 && std::strcmp(argv[1], "--encode") == 0) {
-            const int w = std::atoi(argv[2]), h = std::atoi(argv[3]);
-            std::vector<unsigned char> px(size_t(w) * h);
+        if ((argc == 4 || argc == 5) && std::strcmp(argv[1], "--encode") == 0) {
+            const int w = std::atoi(argv[2]), h = std::atoi(argv[3]), c = argc == 5 ? std::atoi(argv[4]) : 1;
+            std::vector<unsigned char> px(size_t(w) * h * c);
             if (std::fread(px.data(), 1, px.size(), stdin) != px.size()) return 2;
-            const auto png = IQM::encode_grey_png(w, h, px);
+            const auto png = c == 1 ? IQM::encode_grey_png(w, h, px) : IQM::encode_png(w, h, c, px);
             std::fwrite(png.data(), 1, png.size(), stdout);
             return 0;
         }

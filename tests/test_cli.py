@@ -85,6 +85,37 @@ def test_grey_png_encoder_round_trip(png_check, tmp_path):
     assert np.array_equal(np.asarray(Image.open(path)), px)
 
 
+@pytest.mark.parametrize("channels", [3, 4])
+def test_colour_png_encoder_round_trip(png_check, tmp_path, channels):
+    from PIL import Image
+    rng = np.random.default_rng(7)
+    px = rng.integers(0, 256, (17, 29, channels), dtype=np.uint8)
+    png = subprocess.run([png_check, "--encode", "29", "17", str(channels)], input=px.tobytes(), capture_output=True,
+                         check=True).stdout
+    path = str(tmp_path / "c.png")
+    open(path, "wb").write(png)
+    img = Image.open(path)
+    assert img.mode == ("RGB" if channels == 3 else "RGBA")
+    assert np.array_equal(np.asarray(img), px)
+
+
+def test_viridis_table_matches_opencv():
+    """The FLIP --output colour map (iqm_b200/host/viridis_table.h, written by make_viridis.py)."""
+    import re
+    import cv2
+    text = open(os.path.join(ROOT, "iqm_b200", "host", "viridis_table.h")).read()
+    rgb = np.array([int(v) for v in re.findall(r"\d+", text.split("= {", 1)[1])[:768]]).reshape(256, 3)
+    want = cv2.applyColorMap(np.arange(256, dtype=np.uint8).reshape(-1, 1), cv2.COLORMAP_VIRIDIS).reshape(256, 3)
+    assert np.array_equal(rgb, want[:, ::-1])
+
+
+def test_cli_option_value_errors(cli, tmp_path):
+    for opt in (["--precision", "half"], ["FSIM_ENERGY_SUM", "most"]):
+        r = subprocess.run([cli, "--method", "FSIM", "--input", "a.png", "--ref", "b.png"] + opt,
+                           capture_output=True, text=True)
+        assert r.returncode != 0 and "must be" in r.stderr
+
+
 def test_cli_argument_errors(cli):
     # src/args.cpp:32-34 and :52-60: unknown or missing arguments throw outside main's try block
     r = subprocess.run([cli, "--method", "SSIM_CPU", "--input", "a", "--ref", "b"], capture_output=True, text=True)

@@ -101,3 +101,33 @@ def test_cli_repeat_loop(cli, rt, tmp_path):
     out = run(cli, "--method", "SSIM", "--input", pa, "--ref", pb, "--repeat", "4", "-v")
     assert "Iterations: 4" in out
     assert value(out, "MSSIM") == pytest.approx(iqm_b200.SSIM(rt).compute_metric(a, b).mssim, rel=2e-6)
+
+
+def test_cli_flip_output_is_viridis_of_the_flip_map(cli, rt, tmp_path):
+    """FLIP --output writes the per-pixel FLIP value as viridis colours (entry floor(v * 255)),
+    as the reference's combine pass colours its output image."""
+    from PIL import Image
+    import cv2
+    a, b = synth.rgb_blockquant_pair(90, 130, config=2, pair=4)
+    pa, pb = save(tmp_path, "a.png", a), save(tmp_path, "b.png", b)
+    out_png = str(tmp_path / "flip.png")
+    out = run(cli, "--method", "FLIP", "--input", pa, "--ref", pb, "--output", out_png)
+    res = iqm_b200.FLIP(rt).compute_metric(a, b, want_map=True)
+    assert value(out, "FLIP") == pytest.approx(res.mean_flip, rel=2e-6)
+    img = np.asarray(Image.open(out_png))
+    assert img.shape == (90, 130, 4) and np.all(img[..., 3] == 255)
+    lut = cv2.applyColorMap(np.arange(256, dtype=np.uint8).reshape(-1, 1), cv2.COLORMAP_VIRIDIS).reshape(256, 3)[:, ::-1]
+    idx = np.clip(np.floor(res.image_data.astype(np.float32) * np.float32(255.0)), 0, 255).astype(int)
+    assert np.array_equal(img[..., :3], lut[idx])
+
+
+def test_cli_fsim_precision_and_energy_options(cli, rt, o64, tmp_path):
+    a, b = synth.rgb_gain_pair(1080, 1920, config=1, pair=2)
+    pa, pb = save(tmp_path, "a.png", a), save(tmp_path, "b.png", b)
+    f, fc = o64.fsim(a, b)
+    for prec in ("mixed", "mixed_fast"):
+        out = run(cli, "--method", "FSIM", "--input", pa, "--ref", pb, "--precision", prec)
+        assert abs(value(out, "FSIM") - f) <= 1e-4 and abs(value(out, "FSIMc") - fc) <= 1e-4
+    out = run(cli, "--method", "FSIM", "--input", pa, "--ref", pb, "FSIM_ENERGY_SUM", "full")
+    ff, ffc = o64.fsim(a, b, energy_full=True)
+    assert abs(value(out, "FSIM") - ff) <= 2e-6 and abs(value(out, "FSIMc") - ffc) <= 2e-6
