@@ -149,3 +149,59 @@ def test_dev_entry_points_reject_misaligned_images(rt):
             with pytest.raises(iqm_b200.IQMError) as e:
                 m.compute_dev([item], d_scores.data_ptr())
             assert e.value.code == iqm_b200.IQM_EINVAL
+
+
+def _largest_prime_factor(n):
+    p, best = 2, 1
+    while p * p <= n:
+        while n % p == 0:
+            best, n = p, n // p
+        p += 1
+    return max(best, n) if n > 1 else best
+
+
+def test_uneven_256_batch_as_benchmarked_matches_oracle(rt, o64):
+    """The uneven batch exactly as `bench.py --batch` runs it: the same 256 seeded sizes and crops,
+    the SSIM plan without and the FSIM plan with autotuned launch shapes.  Every SSIM score is
+    checked against the FP64 oracle; FSIM on a seeded subset that holds every transform class the
+    batch reaches (the longest planes, which run CTA-wide, Bluestein lengths, lengths with direct
+    odd-prime butterflies, and others)."""
+    import torch
+    import bench
+    from oracle import fsim_plane_size
+    sizes, grey, rgb = bench.batch_pairs()
+    assert len(sizes) == 256
+    plane = []
+    for w, h in sizes:
+        F = max(1, int(np.floor(min(w, h) / 256.0 + 0.5)))
+        plane.append(fsim_plane_size(w, h, F))
+    lpf = [max(_largest_prime_factor(w2), _largest_prime_factor(h2)) for w2, h2 in plane]
+    order = np.argsort([-(w2 * h2) for w2, h2 in plane], kind="stable")
+    picks = list(order[:6])                                                  # longest planes
+    picks += [i for i in range(256) if lpf[i] > 61][:6]                      # Bluestein lengths
+    picks += [i for i in range(256) if 15 < lpf[i] <= 61][:6]                # direct odd primes
+    picks += list(np.random.default_rng(11).choice(256, 6, replace=False))   # anything else
+    picks = sorted(set(int(i) for i in picks))
+    results = {}
+    for name, mask, pairs, tune in (("ssim", iqm_b200.METRIC_SSIM, grey, False),
+                                    ("fsim", iqm_b200.METRIC_FSIM, rgb, True)):
+        bufs, items = _to_device(pairs)
+        d_scores = torch.zeros(iqm_b200.scores_per_pair(mask) * len(pairs), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        plan = iqm_b200.BatchPlan(rt, mask, items, d_scores.data_ptr(), autotune=tune)
+        try:
+            for _ in range(2):  # replays are identical
+                plan.run()
+                rt.synchronize()
+                got = d_scores.cpu().numpy()
+                if name in results:
+                    assert np.array_equal(results[name], got)
+                results[name] = got
+        finally:
+            plan.close()
+        del bufs
+    for i, (a, b) in enumerate(grey):
+        assert abs(results["ssim"][i] - o64.ssim(a, b)) <= TOL, (i, sizes[i])
+    for i in picks:
+        f, fc = o64.fsim(*rgb[i])
+        assert abs(results["fsim"][2 * i] - f) <= TOL and abs(results["fsim"][2 * i + 1] - fc) <= TOL, (i, sizes[i])
