@@ -14,7 +14,10 @@
 //            leaves registers between the stages -- and the DFT-N2 matrix in real form the B operand
 //            (columns 2 k2 + c: Re / Im of output k2).
 // Each lane (g = lane / 4, t = lane % 4) reads its share of the input (12 points at 270 = 15 x 18,
-// 16 at 480 = 16 x 30) and ends with its share of the output as complex pairs.
+// 16 at 480 = 16 x 30) and ends with its share of the output as complex pairs.  The stage-A matrix
+// stays in registers; the stage-C matrix and the twiddles, the same for every warp, live in one
+// lane-indexed shared-memory table per CTA (conflict-free 8-byte loads), which keeps the engine's
+// registers low enough for several CTAs per SM.
 //
 // SPLIT = 3 adds the split-precision products: operands as hi + lo FP16 pairs (hi = fp16(v),
 // lo = fp16(v - hi)) and A B ~ A_hi B_hi + A_hi B_lo + A_lo B_hi, about 21 significant bits per
@@ -65,13 +68,25 @@ struct MmaDft {
     static_assert(N1 >= 2 && N1 <= 16 && N2 >= 2 && N2 <= 32, "factor range of the MMA engine");
     static_assert(SPLIT == 1 || SPLIT == 3, "SPLIT is 1 or 3 products");
 
-    unsigned fa[P][2][2][4];      // stage A matrix: [part][m-tile: Re/Im out][k-tile][register]
-    unsigned fc[P][NT2][NTC][2];  // stage C matrix: [part][k-tile][n-tile][register]
-    float2 tw[2][NT2][2];         // twiddle of (k1 = g + 8 r, n2 = 8 j + 2 t + e): [r][j][e]
+    // shared tables: stage C matrix [part][k-tile][n-tile][lane] as register pairs, then the twiddle
+    // of (k1 = g + 8 r, n2 = 8 j + 2 t + e) as [r][j][e][lane]
+    static constexpr int FC_ENTRIES = P * NT2 * NTC * 32;
+    static constexpr int TW_ENTRIES = 2 * NT2 * 2 * 32;
+    static constexpr size_t smem_bytes = sizeof(uint2) * FC_ENTRIES + sizeof(float2) * TW_ENTRIES;
 
-    // Builds this lane's constant fragments for transforms of sign `sign` (+1 inverse, -1 forward).
-    __device__ __forceinline__ void init(float sign) {
+    unsigned fa[P][2][2][4];  // stage A matrix: [part][m-tile: Re/Im out][k-tile][register]
+    const uint2 *fcs;         // shared stage C table
+    const float2 *tws;        // shared twiddle table
+
+    // Builds this lane's stage-A fragments for transforms of sign `sign` (+1 inverse, -1 forward)
+    // and points the engine at `tables` (smem_bytes of shared memory, 8-byte aligned), which warp 0
+    // fills; the caller synchronises the CTA before the first run().
+    __device__ __forceinline__ void init(float sign, void *tables) {
         const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+        uint2 *fc_w = static_cast<uint2 *>(tables);
+        float2 *tw_w = reinterpret_cast<float2 *>(fc_w + FC_ENTRIES);
+        fcs = fc_w;
+        tws = tw_w;
         auto put = [&](unsigned *hi, unsigned *lo, float x, float y) {
             if constexpr (SPLIT == 1) {
                 *hi = pack_h2(x, y);
@@ -96,11 +111,10 @@ struct MmaDft {
                     }
                     put(&fa[0][mt][kt][q], &fa[P - 1][mt][kt][q], vr, vi);
                 }
-#pragma unroll
+        if (threadIdx.x >= 32) return;  // warp 0 writes the shared tables
         for (int kc = 0; kc < NT2; kc++)
-#pragma unroll
-            for (int nc = 0; nc < NTC; nc++)
-#pragma unroll
+            for (int nc = 0; nc < NTC; nc++) {
+                unsigned hi[2], lo[2];
                 for (int q = 0; q < 2; q++) {
                     // rows 16 kc + 8 q + 2 t + {0, 1} (half-tile h = 2 kc + q: Re / Im block c, n2),
                     // column 8 nc + g (output k2 = (8 nc + g) / 2, Re / Im part cc)
@@ -117,16 +131,16 @@ struct MmaDft {
                             v[e] = c == 0 ? (cc == 0 ? w.x : w.y) : (cc == 0 ? -w.y : w.x);
                         }
                     }
-                    put(&fc[0][kc][nc][q], &fc[P - 1][kc][nc][q], v[0], v[1]);
+                    put(&hi[q], &lo[q], v[0], v[1]);
                 }
-#pragma unroll
+                fc_w[(kc * NTC + nc) * 32 + lane] = make_uint2(hi[0], hi[1]);
+                if constexpr (P == 2) fc_w[((NT2 + kc) * NTC + nc) * 32 + lane] = make_uint2(lo[0], lo[1]);
+            }
         for (int r = 0; r < 2; r++)
-#pragma unroll
             for (int j = 0; j < NT2; j++)
-#pragma unroll
                 for (int e = 0; e < 2; e++) {
                     const int k1 = g + 8 * r, n2 = 8 * j + 2 * t + e;
-                    tw[r][j][e] = unit_root((k1 * n2) % N, N, sign);
+                    tw_w[((r * NT2 + j) * 2 + e) * 32 + lane] = unit_root((k1 * n2) % N, N, sign);
                 }
     }
 
@@ -174,7 +188,7 @@ struct MmaDft {
         for (int j = 0; j < NT2; j++)
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                const float2 w = tw[q >> 1][j][q & 1];
+                const float2 w = tws[(((q >> 1) * NT2 + j) * 2 + (q & 1)) * 32 + lane];
                 const float re = acc[0][j][q], im = acc[1][j][q];
                 acc[0][j][q] = re * w.x - im * w.y;
                 acc[1][j][q] = re * w.y + im * w.x;
@@ -195,7 +209,10 @@ struct MmaDft {
                 const unsigned a[4] = {pack_h2(c0[0], c0[1]), pack_h2(c0[2], c0[3]), pack_h2(c1[0], c1[1]),
                                        pack_h2(c1[2], c1[3])};
 #pragma unroll
-                for (int nc = 0; nc < NTC; nc++) mma_f16_16816(out[nc], a, fc[0][kc][nc][0], fc[0][kc][nc][1]);
+                for (int nc = 0; nc < NTC; nc++) {
+                    const uint2 b = fcs[(kc * NTC + nc) * 32 + lane];
+                    mma_f16_16816(out[nc], a, b.x, b.y);
+                }
             } else {
                 unsigned ah[4], al[4];
                 split_h2(c0[0], c0[1], ah[0], al[0]);
@@ -204,9 +221,11 @@ struct MmaDft {
                 split_h2(c1[2], c1[3], ah[3], al[3]);
 #pragma unroll
                 for (int nc = 0; nc < NTC; nc++) {
-                    mma_f16_16816(out[nc], ah, fc[0][kc][nc][0], fc[0][kc][nc][1]);
-                    mma_f16_16816(out[nc], al, fc[0][kc][nc][0], fc[0][kc][nc][1]);
-                    mma_f16_16816(out[nc], ah, fc[1][kc][nc][0], fc[1][kc][nc][1]);
+                    const uint2 bh = fcs[(kc * NTC + nc) * 32 + lane];
+                    const uint2 bl = fcs[((NT2 + kc) * NTC + nc) * 32 + lane];
+                    mma_f16_16816(out[nc], ah, bh.x, bh.y);
+                    mma_f16_16816(out[nc], al, bh.x, bh.y);
+                    mma_f16_16816(out[nc], ah, bl.x, bl.y);
                 }
             }
         }

@@ -764,19 +764,21 @@ struct MmaColGeom {
     static constexpr int SEG = Dft::N2 + ((4 - Dft::N2 % 16) + 16) % 16;  // N2 padded to 4 mod 16
     static constexpr int SLAB = Dft::N1 * SEG;                            // padded column, float2
     static constexpr int SP = MCW + 1;                                    // staging row stride, half2
-    static constexpr size_t smem = sizeof(float2) * MCW * SLAB + sizeof(__half2) * 4 * H * SP;
+    static constexpr size_t tables = (Dft::smem_bytes + 15) & ~size_t(15);
+    static constexpr size_t smem = tables + sizeof(float2) * MCW * SLAB + sizeof(__half2) * 4 * H * SP;
 };
 
 template <class Dft>
-__global__ void __launch_bounds__(32 * MCW, 2) fsim_inv_cols_mma_kernel(FsimGroup g, int items) {
+// Single-product engines fit 3 CTAs per SM without spills; split-precision ones 2.
+__global__ void __launch_bounds__(32 * MCW, Dft::P == 1 ? 3 : 2) fsim_inv_cols_mma_kernel(FsimGroup g, int items) {
     using Gm = MmaColGeom<Dft>;
     constexpr int H = Gm::H;
     extern __shared__ __align__(16) float2 sm[];
-    float2 *Sl = sm;
+    float2 *Sl = sm + Gm::tables / sizeof(float2);
     __half2 *stage = reinterpret_cast<__half2 *>(Sl + MCW * Gm::SLAB);
     const int warp = threadIdx.x >> 5;
     Dft dft;
-    dft.init(1.f);
+    dft.init(1.f, sm);  // tables complete at the item loop's first barrier
     const int ngroups = (g.w2 + MCW - 1) / MCW;
     const float invN = 1.0f / float(g.n);
     for (int item = blockIdx.x; item < items; item += gridDim.x) {
@@ -835,19 +837,22 @@ struct MmaRowGeom {
     static constexpr int W = Dft::N;
     static constexpr int RS = Dft::N1 + ((4 - Dft::N1 % 16) + 16) % 16;  // N1 padded to 4 mod 16
     static constexpr int RL = RS * Dft::N2;
-    static constexpr size_t smem = sizeof(float2) * MRR * 4 * RL;
+    static constexpr size_t tables = (Dft::smem_bytes + 15) & ~size_t(15);
+    static constexpr size_t smem = tables + sizeof(float2) * MRR * 4 * RL;
     static_assert(Dft::N1 % 4 == 0 && RL % 4 == 0, "4-pixel epilogue needs N1 % 4 == 0");
 };
 
 template <class Dft>
-__global__ void __launch_bounds__(32 * 4 * MRR, 1) fsim_inv_rows_mma_kernel(FsimGroup g, int items) {
+__global__ void __launch_bounds__(32 * 4 * MRR, Dft::P == 1 ? 3 : 2) fsim_inv_rows_mma_kernel(FsimGroup g, int items) {
     using Gm = MmaRowGeom<Dft>;
     constexpr int W = Gm::W;
-    extern __shared__ __align__(16) float2 sm[];
+    extern __shared__ __align__(16) float2 smraw[];
+    float2 *sm = smraw + Gm::tables / sizeof(float2);
     const int warp = threadIdx.x >> 5;
     const int r = warp >> 2, sc = warp & 3;
     Dft dft;
-    dft.init(1.f);
+    dft.init(1.f, smraw);
+    __syncthreads();
     const int nrg = (g.h2 + MRR - 1) / MRR;
     for (int item = blockIdx.x; item < items; item += gridDim.x) {
         const int yg = item % nrg;
