@@ -14,10 +14,10 @@
 //            leaves registers between the stages -- and the DFT-N2 matrix in real form the B operand
 //            (columns 2 k2 + c: Re / Im of output k2).
 // Each lane (g = lane / 4, t = lane % 4) reads its share of the input (12 points at 270 = 15 x 18,
-// 16 at 480 = 16 x 30) and ends with its share of the output as complex pairs.  The stage-A matrix
-// stays in registers; the stage-C matrix and the twiddles, the same for every warp, live in one
-// lane-indexed shared-memory table per CTA (conflict-free 8-byte loads), which keeps the engine's
-// registers low enough for several CTAs per SM.
+// 16 at 480 = 16 x 30) and ends with its share of the output as complex pairs.  The constants are
+// built once into a global table (build); each CTA copies the stage-C matrix and the twiddles, the
+// same for every warp, into one lane-indexed shared-memory table (conflict-free 8-byte loads) and
+// keeps only the stage-A matrix in registers, which leaves room for several CTAs per SM.
 //
 // SPLIT = 3 adds the split-precision products: operands as hi + lo FP16 pairs (hi = fp16(v),
 // lo = fp16(v - hi)) and A B ~ A_hi B_hi + A_hi B_lo + A_lo B_hi, about 21 significant bits per
@@ -68,25 +68,28 @@ struct MmaDft {
     static_assert(N1 >= 2 && N1 <= 16 && N2 >= 2 && N2 <= 32, "factor range of the MMA engine");
     static_assert(SPLIT == 1 || SPLIT == 3, "SPLIT is 1 or 3 products");
 
-    // shared tables: stage C matrix [part][k-tile][n-tile][lane] as register pairs, then the twiddle
-    // of (k1 = g + 8 r, n2 = 8 j + 2 t + e) as [r][j][e][lane]
+    // Tables: the stage-A fragments of every lane, [part][m-tile][k-tile][register][lane] as 32-bit
+    // words, then the stage-C matrix [part][k-tile][n-tile][lane] as register pairs, then the
+    // twiddle of (k1 = g + 8 r, n2 = 8 j + 2 t + e) as [r][j][e][lane].  build() writes the whole
+    // table to global memory once; load() copies the stage-C and twiddle parts into the CTA's shared
+    // memory and the lane's stage-A fragments into registers.
+    static constexpr int FA_WORDS = P * 2 * 2 * 4 * 32;
     static constexpr int FC_ENTRIES = P * NT2 * NTC * 32;
     static constexpr int TW_ENTRIES = 2 * NT2 * 2 * 32;
     static constexpr size_t smem_bytes = sizeof(uint2) * FC_ENTRIES + sizeof(float2) * TW_ENTRIES;
+    static constexpr size_t table_bytes = sizeof(unsigned) * FA_WORDS + smem_bytes;
+    static_assert(sizeof(unsigned) * FA_WORDS % 16 == 0 && smem_bytes % 16 == 0, "16-byte table parts");
 
     unsigned fa[P][2][2][4];  // stage A matrix: [part][m-tile: Re/Im out][k-tile][register]
     const uint2 *fcs;         // shared stage C table
     const float2 *tws;        // shared twiddle table
 
-    // Builds this lane's stage-A fragments for transforms of sign `sign` (+1 inverse, -1 forward)
-    // and points the engine at `tables` (smem_bytes of shared memory, 8-byte aligned), which warp 0
-    // fills; the caller synchronises the CTA before the first run().
-    __device__ __forceinline__ void init(float sign, void *tables) {
+    // Writes the table for transforms of sign `sign` (+1 inverse, -1 forward); run by one warp.
+    static __device__ void build(void *table, float sign) {
         const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-        uint2 *fc_w = static_cast<uint2 *>(tables);
+        unsigned *fa_w = static_cast<unsigned *>(table);
+        uint2 *fc_w = reinterpret_cast<uint2 *>(fa_w + FA_WORDS);
         float2 *tw_w = reinterpret_cast<float2 *>(fc_w + FC_ENTRIES);
-        fcs = fc_w;
-        tws = tw_w;
         auto put = [&](unsigned *hi, unsigned *lo, float x, float y) {
             if constexpr (SPLIT == 1) {
                 *hi = pack_h2(x, y);
@@ -94,11 +97,8 @@ struct MmaDft {
                 split_h2(x, y, *hi, *lo);
             }
         };
-#pragma unroll
         for (int mt = 0; mt < 2; mt++)
-#pragma unroll
             for (int kt = 0; kt < 2; kt++)
-#pragma unroll
                 for (int q = 0; q < 4; q++) {
                     // register q: rows g (q even) / g + 8 (q odd); columns 2 t, 2 t + 1 (+ 8 for q >= 2)
                     const int k1 = g + 8 * (q & 1);
@@ -109,9 +109,11 @@ struct MmaDft {
                         vr = mt == 0 ? w.x : w.y;
                         vi = mt == 0 ? -w.y : w.x;
                     }
-                    put(&fa[0][mt][kt][q], &fa[P - 1][mt][kt][q], vr, vi);
+                    unsigned hi, lo;
+                    put(&hi, &lo, vr, vi);
+                    fa_w[(((0 * 2 + mt) * 2 + kt) * 4 + q) * 32 + lane] = hi;
+                    if constexpr (P == 2) fa_w[(((1 * 2 + mt) * 2 + kt) * 4 + q) * 32 + lane] = lo;
                 }
-        if (threadIdx.x >= 32) return;  // warp 0 writes the shared tables
         for (int kc = 0; kc < NT2; kc++)
             for (int nc = 0; nc < NTC; nc++) {
                 unsigned hi[2], lo[2];
@@ -122,7 +124,6 @@ struct MmaDft {
                     const int c = h / NT2, n2 = 8 * (h % NT2) + 2 * t;
                     const int k2 = (8 * nc + g) >> 1, cc = g & 1;
                     float v[2];
-#pragma unroll
                     for (int e = 0; e < 2; e++) {
                         v[e] = 0.f;
                         if (n2 + e < N2 && k2 < N2) {
@@ -144,9 +145,35 @@ struct MmaDft {
                 }
     }
 
+    // Copies the shared part of `table` (global, from build) into `shared` (smem_bytes, 16-byte
+    // aligned) with every thread of the CTA, and this lane's stage-A fragments into registers.  The
+    // caller synchronises the CTA before the first run().
+    __device__ __forceinline__ void load(const void *table, void *shared) {
+        const int lane = threadIdx.x & 31;
+        const unsigned *fa_g = static_cast<const unsigned *>(table);
+#pragma unroll
+        for (int p = 0; p < P; p++)
+#pragma unroll
+            for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+                for (int kt = 0; kt < 2; kt++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++) fa[p][mt][kt][q] = __ldg(fa_g + (((p * 2 + mt) * 2 + kt) * 4 + q) * 32 + lane);
+        const uint4 *src = reinterpret_cast<const uint4 *>(fa_g + FA_WORDS);
+        uint4 *dst = static_cast<uint4 *>(shared);
+        for (int i = threadIdx.x; i < int(smem_bytes / 16); i += blockDim.x) dst[i] = __ldg(src + i);
+        fcs = static_cast<const uint2 *>(shared);
+        tws = reinterpret_cast<const float2 *>(fcs + FC_ENTRIES);
+    }
+
+    // Output slot s of a lane (0 <= s < 2 NTC) holds X[k1 + N1 k2] with k1 = g + 8 (s & 1),
+    // k2 = 4 (s >> 1) + t when both are in range.
+    static __device__ __forceinline__ int slot_k1(int s) { return ((threadIdx.x & 31) >> 2) + 8 * (s & 1); }
+    static __device__ __forceinline__ int slot_k2(int s) { return 4 * (s >> 1) + (threadIdx.x & 3); }
+
     // One transform.  ld(n1, n2) returns the (already scaled) input x[N2 n1 + n2] as float2 for
-    // n1 < N1, n2 < N2; st(k, v) receives output X[k] for every k < N exactly once across the warp.
-    // All 32 lanes must call it together (warp-synchronous MMAs).
+    // n1 < N1, n2 < N2; st(k, slot, v) receives output X[k] (in this lane's `slot`) for every k < N
+    // exactly once across the warp.  All 32 lanes must call it together (warp-synchronous MMAs).
     template <class Load, class Store>
     __device__ __forceinline__ void run(Load ld, Store st) const {
         const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -234,8 +261,8 @@ struct MmaDft {
         for (int nc = 0; nc < NTC; nc++) {
             const int k2 = 4 * nc + t;
             if (k2 < N2) {
-                if (g < N1) st(g + N1 * k2, make_float2(out[nc][0], out[nc][1]));
-                if (g + 8 < N1) st(g + 8 + N1 * k2, make_float2(out[nc][2], out[nc][3]));
+                if (g < N1) st(g + N1 * k2, 2 * nc, make_float2(out[nc][0], out[nc][1]));
+                if (g + 8 < N1) st(g + 8 + N1 * k2, 2 * nc + 1, make_float2(out[nc][2], out[nc][3]));
             }
         }
     }

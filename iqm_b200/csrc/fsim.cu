@@ -48,10 +48,12 @@ struct FsimPlan {
     FftLen row{}, col{};
     float *filters = nullptr;  // 16 planes of n (z = o*4 + s)
     double *consts = nullptr;  // device: em[4], an2[2][4], aiaj[2][4]
+    void *mma_tables = nullptr;  // tensor-core engines' constants (480 x 270 plans in a mixed form)
     double em[4], an2[2][4], aiaj[2][4];
     ~FsimPlan() {
         if (filters) cudaFree(filters);
         if (consts) cudaFree(consts);
+        if (mma_tables) cudaFree(mma_tables);
     }
 };
 
@@ -752,152 +754,161 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_seq_kernel(FsimGroup g, c
 // normalised responses directly.  Both kernels are persistent: each warp builds its transform's
 // constant fragments once and the CTAs stride over (columns or rows, orientation, plane) items.
 
-// Column pass: a work item is MCW adjacent columns of one (orientation, plane); warp c transforms
-// column c for the orientation's 4 scales.  The separated spectrum slab sits in shared memory with
-// each column stored as N1 segments of N2 points padded to a stride of SEG (conflict-free loads by
-// the engine's lane pattern); outputs are staged per scale as FP16 rows of MCW columns and written
-// row by row.
+// Column pass: a work item is MCW adjacent columns of one (orientation, pair); warp c transforms
+// column c of both images for the orientation's 4 scales.  The pair's packed spectrum is read once
+// per item and separated into both images' spectra in a shared slab, each column stored as N1
+// segments of N2 points padded to a stride of SEG (conflict-free loads by the engine's lane
+// pattern); each scale's outputs are staged as FP16 rows of MCW columns and written to the
+// intermediate planes as 16-byte row segments.
 constexpr int MCW = 8;
 template <class Dft>
 struct MmaColGeom {
     static constexpr int H = Dft::N;                                      // column length
     static constexpr int SEG = Dft::N2 + ((4 - Dft::N2 % 16) + 16) % 16;  // N2 padded to 4 mod 16
     static constexpr int SLAB = Dft::N1 * SEG;                            // padded column, float2
-    static constexpr int SP = MCW + 1;                                    // staging row stride, half2
-    static constexpr size_t tables = (Dft::smem_bytes + 15) & ~size_t(15);
-    static constexpr size_t smem = tables + sizeof(float2) * MCW * SLAB + sizeof(__half2) * 4 * H * SP;
+    static constexpr int SP = 12;  // staging row stride (half2): MCW columns, 16-byte aligned rows
+    static constexpr size_t tables = Dft::smem_bytes;
+    static constexpr size_t slab_bytes = sizeof(float2) * 2 * MCW * SLAB;
+    static constexpr size_t smem = tables + slab_bytes + sizeof(__half2) * 2 * H * SP;
+    static_assert(MCW == 8 && tables % 16 == 0 && slab_bytes % 16 == 0, "16-byte staging rows");
 };
 
 template <class Dft>
 // Single-product engines fit 3 CTAs per SM without spills; split-precision ones 2.
-__global__ void __launch_bounds__(32 * MCW, Dft::P == 1 ? 3 : 2) fsim_inv_cols_mma_kernel(FsimGroup g, int items) {
+__global__ void __launch_bounds__(32 * MCW, Dft::P == 1 ? 3 : 2)
+    fsim_inv_cols_mma_kernel(FsimGroup g, const void *__restrict__ table, int items) {
     using Gm = MmaColGeom<Dft>;
     constexpr int H = Gm::H;
     extern __shared__ __align__(16) float2 sm[];
-    float2 *Sl = sm + Gm::tables / sizeof(float2);
-    __half2 *stage = reinterpret_cast<__half2 *>(Sl + MCW * Gm::SLAB);
+    float2 *Sl = sm + Gm::tables / sizeof(float2);                          // [img][column][SLAB]
+    __half2 *stage = reinterpret_cast<__half2 *>(Sl + 2 * MCW * Gm::SLAB);  // [img][y][SP]
     const int warp = threadIdx.x >> 5;
     Dft dft;
-    dft.init(1.f, sm);  // tables complete at the item loop's first barrier
+    dft.load(table, sm);  // complete at the item loop's first barrier
     const int ngroups = (g.w2 + MCW - 1) / MCW;
-    const float invN = 1.0f / float(g.n);
+    const float hs = 0.5f / float(g.n);
     for (int item = blockIdx.x; item < items; item += gridDim.x) {
         const int cg = item % ngroups;
         const int o = (item / ngroups) & 3;
-        const int plane = item / (ngroups * 4);  // chunk-local pair*2 + img
-        const int x0 = cg * MCW, nc = min(MCW, g.w2 - x0), img = plane & 1;
-        const float2 *src = g.spec + size_t(g.pair0 + (plane >> 1)) * g.n;
+        const int pr = item / (ngroups * 4);  // chunk-local pair
+        const int x0 = cg * MCW, nc = min(MCW, g.w2 - x0);
+        const float2 *src = g.spec + size_t(g.pair0 + pr) * g.n;
         for (int idx = threadIdx.x; idx < MCW * H; idx += blockDim.x) {
             const int y = idx / MCW, c = idx - y * MCW;
-            float2 v = make_float2(0.f, 0.f);
+            float2 v0 = make_float2(0.f, 0.f), v1 = v0;
             if (c < nc) {
                 const int x = x0 + c;
                 // Z = F(Y_img + i Y_ref): F(Y_img) = (Z(k) + conj Z(-k)) / 2, F(Y_ref) = (Z(k) - conj Z(-k)) / 2i
                 const float2 z = src[size_t(y) * g.w2 + x];
                 const float2 m = src[size_t(y ? H - y : 0) * g.w2 + (x ? g.w2 - x : 0)];
-                const float hs = 0.5f * invN;
-                v = img == 0 ? make_float2(hs * (z.x + m.x), hs * (z.y - m.y)) : make_float2(hs * (z.y + m.y), hs * (m.x - z.x));
+                v0 = make_float2(hs * (z.x + m.x), hs * (z.y - m.y));
+                v1 = make_float2(hs * (z.y + m.y), hs * (m.x - z.x));
             }
-            Sl[c * Gm::SLAB + (y / Dft::N2) * Gm::SEG + y % Dft::N2] = v;
+            const int si = c * Gm::SLAB + (y / Dft::N2) * Gm::SEG + y % Dft::N2;
+            Sl[si] = v0;
+            Sl[MCW * Gm::SLAB + si] = v1;
         }
         __syncthreads();
-        if (warp < nc) {  // warp-uniform
-            const float2 *col = Sl + warp * Gm::SLAB;
 #pragma unroll 1
-            for (int s = 0; s < 4; s++) {
+        for (int s = 0; s < 4; s++) {
+            if (warp < nc) {  // warp-uniform
                 const float *Hz = g.filters + size_t(o * 4 + s) * g.n + size_t(x0 + warp) * H;
-                __half2 *st = stage + s * H * Gm::SP + warp;
-                dft.run(
-                    [&](int n1, int n2) {
-                        const float h = __ldg(Hz + Dft::N2 * n1 + n2);
-                        const float2 v = col[n1 * Gm::SEG + n2];
-                        return make_float2(h * v.x, h * v.y);
-                    },
-                    [&](int k, float2 v) { st[k * Gm::SP] = __floats2half2_rn(v.x, v.y); });
+#pragma unroll 1
+                for (int img = 0; img < 2; img++) {
+                    const float2 *col = Sl + (img * MCW + warp) * Gm::SLAB;
+                    __half2 *st = stage + img * H * Gm::SP + warp;
+                    dft.run(
+                        [&](int n1, int n2) {
+                            const float h = __ldg(Hz + Dft::N2 * n1 + n2);
+                            const float2 v = col[n1 * Gm::SEG + n2];
+                            return make_float2(h * v.x, h * v.y);
+                        },
+                        [&](int k, int, float2 v) { st[k * Gm::SP] = __floats2half2_rn(v.x, v.y); });
+                }
             }
+            __syncthreads();
+            const size_t zoff = size_t(o * 4 + s) * g.n + size_t(x0);
+            if (nc == MCW) {
+                for (int idx = threadIdx.x; idx < 2 * H * 2; idx += blockDim.x) {
+                    const int q = idx & 1, r = idx >> 1;  // r = img * H + y
+                    const int img = r / H, y = r - img * H;
+                    const uint4 v = *reinterpret_cast<const uint4 *>(stage + r * Gm::SP + 4 * q);
+                    *reinterpret_cast<uint4 *>(g.Th + size_t(2 * pr + img) * 16 * g.n + zoff + size_t(y) * g.w2 + 4 * q) = v;
+                }
+            } else {
+                for (int idx = threadIdx.x; idx < 2 * H * MCW; idx += blockDim.x) {
+                    const int c = idx % MCW, r = idx / MCW;
+                    const int img = r / H, y = r - img * H;
+                    if (c < nc) g.Th[size_t(2 * pr + img) * 16 * g.n + zoff + size_t(y) * g.w2 + c] = stage[r * Gm::SP + c];
+                }
+            }
+            __syncthreads();  // staging rows read before the next scale overwrites them
         }
-        __syncthreads();
-        for (int idx = threadIdx.x; idx < 4 * H * MCW; idx += blockDim.x) {
-            const int r = idx / MCW, c = idx - r * MCW;  // r = s * H + y
-            const int s = r / H, y = r - s * H;
-            if (c < nc)
-                g.Th[(size_t(plane) * 16 + o * 4 + s) * g.n + size_t(y) * g.w2 + x0 + c] = stage[r * Gm::SP + c];
-        }
-        // the next item's first barrier orders these staging reads before its staging writes
     }
 }
 
-// Row pass: a work item is MRR rows of one (orientation, plane); warp (r, s) transforms row r for
-// scale s, reading its FP16 inputs straight from the intermediate planes, and leaves the outputs
-// in shared memory (each group of N1 outputs padded to RS, conflict-free stores); then the CTA
-// forms the response sums of 4 consecutive pixels per thread, as fsim_inv_rows_kernel does.
-constexpr int MRR = 2;
+// Row pass: a work item is one row of one (orientation, plane), taken by one warp on its own: it
+// transforms the row for the 4 scales, reading its FP16 inputs straight from the intermediate
+// planes, parks the first 3 scales' outputs in its own shared slots and keeps the last in
+// registers, then forms the response sums of its outputs (as fsim_inv_rows_kernel does) and
+// stores them; no barrier after the tables are loaded.
+constexpr int MRW = 8;  // warps per CTA of the row pass
 template <class Dft>
 struct MmaRowGeom {
     static constexpr int W = Dft::N;
-    static constexpr int RS = Dft::N1 + ((4 - Dft::N1 % 16) + 16) % 16;  // N1 padded to 4 mod 16
-    static constexpr int RL = RS * Dft::N2;
-    static constexpr size_t tables = (Dft::smem_bytes + 15) & ~size_t(15);
-    static constexpr size_t smem = tables + sizeof(float2) * MRR * 4 * RL;
-    static_assert(Dft::N1 % 4 == 0 && RL % 4 == 0, "4-pixel epilogue needs N1 % 4 == 0");
+    static constexpr int SLOTS = 2 * Dft::NTC;  // output slots per lane
+    static constexpr size_t tables = Dft::smem_bytes;
+    static constexpr size_t smem = tables + sizeof(float2) * MRW * 3 * SLOTS * 32;
 };
 
 template <class Dft>
-__global__ void __launch_bounds__(32 * 4 * MRR, Dft::P == 1 ? 3 : 2) fsim_inv_rows_mma_kernel(FsimGroup g, int items) {
+__global__ void __launch_bounds__(32 * MRW, Dft::P == 1 ? 2 : 1)
+    fsim_inv_rows_mma_kernel(FsimGroup g, const void *__restrict__ table, int items) {
     using Gm = MmaRowGeom<Dft>;
-    constexpr int W = Gm::W;
-    extern __shared__ __align__(16) float2 smraw[];
-    float2 *sm = smraw + Gm::tables / sizeof(float2);
-    const int warp = threadIdx.x >> 5;
-    const int r = warp >> 2, sc = warp & 3;
+    constexpr int W = Gm::W, SL = Gm::SLOTS;
+    extern __shared__ __align__(16) float2 sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float2 *keep = sm + Gm::tables / sizeof(float2) + size_t(warp) * 3 * SL * 32;  // [scale][slot][lane]
     Dft dft;
-    dft.init(1.f, smraw);
+    dft.load(table, sm);
     __syncthreads();
-    const int nrg = (g.h2 + MRR - 1) / MRR;
-    for (int item = blockIdx.x; item < items; item += gridDim.x) {
-        const int yg = item % nrg;
-        const int o = (item / nrg) & 3;
-        const int plane = item / (nrg * 4);
-        const int y = yg * MRR + r;
-        if (y < g.h2) {  // warp-uniform
-            const __half2 *src = g.Th + (size_t(plane) * 16 + o * 4 + sc) * g.n + size_t(y) * W;
-            float2 *dst = sm + (r * 4 + sc) * Gm::RL;
+    for (int item = blockIdx.x * MRW + warp; item < items; item += gridDim.x * MRW) {  // warp-uniform
+        const int y = item % g.h2;
+        const int o = (item / g.h2) & 3;
+        const int plane = item / (g.h2 * 4);  // chunk-local pair*2 + img
+        float2 last[SL];
+#pragma unroll 1
+        for (int s = 0; s < 4; s++) {
+            const __half2 *src = g.Th + (size_t(plane) * 16 + o * 4 + s) * g.n + size_t(y) * W;
             dft.run([&](int n1, int n2) { return __half22float2(src[Dft::N2 * n1 + n2]); },
-                    [&](int k, float2 v) { dst[(k % Dft::N1) + Gm::RS * (k / Dft::N1)] = v; });
+                    [&](int, int slot, float2 v) {
+                        if (s < 3)
+                            keep[(s * SL + slot) * 32 + lane] = v;
+                        else
+                            last[slot] = v;
+                    });
         }
-        __syncthreads();
-        const int gp = g.pair0 * 2 + plane;
-        constexpr int QPR = W / 4;
-        for (int idx = threadIdx.x; idx < MRR * QPR; idx += blockDim.x) {
-            const int rl = idx / QPR;
-            const int x = (idx - rl * QPR) * 4;
-            const int yy = yg * MRR + rl;
-            if (yy >= g.h2) continue;
-            const int si = (x % Dft::N1) + Gm::RS * (x / Dft::N1);  // 4 consecutive outputs
-            float2 v[4][4];  // [scale][pixel]
+        const size_t row = (size_t(g.pair0 * 2 + plane) * 4 + o) * g.n + size_t(y) * W;
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const float4 *p = reinterpret_cast<const float4 *>(sm + (rl * 4 + q) * Gm::RL + si);
-                const float4 lo = p[0], hi = p[1];
-                v[q][0] = make_float2(lo.x, lo.y);
-                v[q][1] = make_float2(lo.z, lo.w);
-                v[q][2] = make_float2(hi.x, hi.y);
-                v[q][3] = make_float2(hi.z, hi.w);
-            }
-            float4 oa, oe, o0;
-            float *pa = &oa.x, *pe = &oe.x, *p0 = &o0.x;
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                const float2 w[4] = {v[0][i], v[1][i], v[2][i], v[3][i]};
-                response_sums(w, 1.0f, pa[i], pe[i], p0[i]);  // already normalised
-            }
-            const size_t off = (size_t(gp) * 4 + o) * g.n + size_t(yy) * W + x;
-            *reinterpret_cast<float4 *>(g.amp + off) = oa;
-            *reinterpret_cast<float4 *>(g.energy + off) = oe;
-            *reinterpret_cast<float4 *>(g.eo0 + off) = o0;
+        for (int slot = 0; slot < SL; slot++) {
+            const int k1 = Dft::slot_k1(slot), k2 = Dft::slot_k2(slot);
+            if (k1 >= Dft::N1 || k2 >= Dft::N2) continue;
+            const int x = k1 + Dft::N1 * k2;
+            const float2 v[4] = {keep[slot * 32 + lane], keep[(SL + slot) * 32 + lane], keep[(2 * SL + slot) * 32 + lane],
+                                 last[slot]};
+            float sA, en, e0;
+            response_sums(v, 1.0f, sA, en, e0);  // already normalised
+            g.amp[row + x] = sA;
+            g.energy[row + x] = en;
+            g.eo0[row + x] = e0;
         }
-        __syncthreads();  // staging reads done before the next item's transforms overwrite it
     }
+}
+
+// Builds an engine's constant table (one warp).
+template <class Dft>
+__global__ void mma_table_kernel(void *table) {
+    Dft::build(table, 1.f);
 }
 
 // Tensor-core transform engines of the mixed forms: 270 = 15 x 18 (columns), 480 = 16 x 30 (rows).
@@ -1468,20 +1479,52 @@ int persistent_grid(const void *fn, int threads, size_t smem, int items) {
     return std::max(1, std::min(items, sms * std::max(1, per_sm)));
 }
 
+// Offsets of the four engines' constant tables in FsimPlan::mma_tables.
+struct MmaTableLayout {
+    size_t col1, col3, row1, row3, total;
+};
+MmaTableLayout mma_table_layout() {
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    MmaTableLayout L{};
+    L.col1 = 0;
+    L.col3 = L.col1 + al(MmaCol270<1>::table_bytes);
+    L.row1 = L.col3 + al(MmaCol270<3>::table_bytes);
+    L.row3 = L.row1 + al(MmaRow480<1>::table_bytes);
+    L.total = L.row3 + al(MmaRow480<3>::table_bytes);
+    return L;
+}
+
+// pairs: pairs in the chunk (each item of the column pass covers both images of a pair).
 template <int SPLIT>
-void launch_inv_mma(const FsimGroup &g, int planes, cudaStream_t st, iqm_ctx *ctx) {
+void launch_inv_mma(const FsimGroup &g, const iqm::FsimPlan &P, int pairs, cudaStream_t st, iqm_ctx *ctx) {
     using C = MmaCol270<SPLIT>;
     using R = MmaRow480<SPLIT>;
-    const int citems = int(iqm::ceil_div(g.w2, MCW)) * 4 * planes;
+    const MmaTableLayout TL = mma_table_layout();
+    const uint8_t *tables = static_cast<const uint8_t *>(P.mma_tables);
+    const int citems = int(iqm::ceil_div(g.w2, MCW)) * 4 * pairs;
     const size_t csm = MmaColGeom<C>::smem;
     const int cgrid = persistent_grid((const void *)fsim_inv_cols_mma_kernel<C>, 32 * MCW, csm, citems);
-    fsim_inv_cols_mma_kernel<C><<<cgrid, 32 * MCW, csm, st>>>(g, citems);
+    fsim_inv_cols_mma_kernel<C><<<cgrid, 32 * MCW, csm, st>>>(g, tables + (SPLIT == 1 ? TL.col1 : TL.col3), citems);
     iqm::check_launch(ctx, "fsim_inv_cols_mma_kernel");
-    const int ritems = int(iqm::ceil_div(g.h2, MRR)) * 4 * planes;
+    const int ritems = g.h2 * 4 * 2 * pairs;
     const size_t rsm = MmaRowGeom<R>::smem;
-    const int rgrid = persistent_grid((const void *)fsim_inv_rows_mma_kernel<R>, 32 * 4 * MRR, rsm, ritems);
-    fsim_inv_rows_mma_kernel<R><<<rgrid, 32 * 4 * MRR, rsm, st>>>(g, ritems);
+    const int rgrid = persistent_grid((const void *)fsim_inv_rows_mma_kernel<R>, 32 * MRW, rsm,
+                                      int(iqm::ceil_div(ritems, MRW)));
+    fsim_inv_rows_mma_kernel<R><<<rgrid, 32 * MRW, rsm, st>>>(g, tables + (SPLIT == 1 ? TL.row1 : TL.row3), ritems);
     iqm::check_launch(ctx, "fsim_inv_rows_mma_kernel");
+}
+
+// The tensor-core engines' constant tables of a 480 x 270 plan, built once on the context stream.
+void ensure_mma_tables(iqm_ctx *ctx, iqm::FsimPlan *P) {
+    if (P->mma_tables) return;
+    const MmaTableLayout TL = mma_table_layout();
+    IQM_CHECK_CUDA(cudaMalloc(&P->mma_tables, TL.total));
+    uint8_t *t = static_cast<uint8_t *>(P->mma_tables);
+    mma_table_kernel<MmaCol270<1>><<<1, 32, 0, ctx->stream>>>(t + TL.col1);
+    mma_table_kernel<MmaCol270<3>><<<1, 32, 0, ctx->stream>>>(t + TL.col3);
+    mma_table_kernel<MmaRow480<1>><<<1, 32, 0, ctx->stream>>>(t + TL.row1);
+    mma_table_kernel<MmaRow480<3>><<<1, 32, 0, ctx->stream>>>(t + TL.row3);
+    IQM_CHECK_CUDA(cudaGetLastError());
 }
 
 void launch_ingest(const FsimGroup &g, int F_uniform, int tiles, cudaStream_t st) {
@@ -1541,6 +1584,7 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
             r.s = shapes_for(*r.P, ctx->fsim_tune);
             const int n = r.P->n;
             r.mma = mma_plane(r.w2, r.h2) ? mma : 0;
+            if (r.mma) ensure_mma_tables(ctx, r.P);
             const size_t tbytes = r.mma ? sizeof(__half2) : sizeof(float2);
             r.chunk = chunk_pairs(ctx->fsim_tune, r.G, n, tbytes);
             // More than one chunk: split the L2 budget over two buffers and let consecutive chunks run
@@ -1660,9 +1704,9 @@ void fsim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, int energy_m
                 gc.Th = reinterpret_cast<__half2 *>(g.T) + size_t(j) * chunk * 32 * n;
                 gc.T = nullptr;
                 if (r.mma == 3)
-                    launch_inv_mma<3>(gc, 2 * cg, cs, ctx);
+                    launch_inv_mma<3>(gc, *P, cg, cs, ctx);
                 else
-                    launch_inv_mma<1>(gc, 2 * cg, cs, ctx);
+                    launch_inv_mma<1>(gc, *P, cg, cs, ctx);
                 continue;
             }
             gc.T = g.T + size_t(j) * chunk * 32 * n;
