@@ -88,6 +88,8 @@ def parse():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed", "mixed_fast"],
                     help="FSIM form: FP32 transforms, or tensor-core transforms with FP16 planes "
                          "(split-precision hi + lo products, or single products)")
+    ap.add_argument("--flip-monitor", default="3840,0.7,0.7",
+                    help="FLIP viewing set-up RES,DISTANCE,WIDTH (default 67.02 pixels per degree)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     return ap.parse_args()
@@ -463,7 +465,8 @@ def main():
     if metric == "fsim":
         obj.precision = prec
     nscore = WORKLOADS[metric][2]
-    flip_args = iqm_b200.FLIPArguments(3840.0, 0.7, 0.7)  # 67.02 pixels per degree
+    res_x, dist_m, width_m = (float(v) for v in args.flip_monitor.split(","))
+    flip_args = iqm_b200.FLIPArguments(res_x, dist_m, width_m)  # default 67.02 pixels per degree
 
     # device-resident batch: B distinct buffers (replicas of the distinct synthetic pairs)
     img_bytes = H * W * 4
