@@ -32,8 +32,12 @@ SIZE = "1080p"
 
 
 def set_size(name):
+    """1080p, 4k, or WxH (a profiling case; its lines are named by the size)."""
     global W, H, SIZE
-    W, H = SIZES[name]
+    if name in SIZES:
+        W, H = SIZES[name]
+    else:
+        W, H = (int(v) for v in name.lower().split("x"))
     SIZE = name
 
 # metric -> (workload name, synthetic generator name, score count per pair)
@@ -69,7 +73,7 @@ def workload_name(metric):
 
 
 def metric_name(metric):
-    return "%s image pairs/sec (%s)" % ("1080p" if SIZE == "1080p" else "4K", metric.upper())
+    return "%s image pairs/sec (%s)" % ({"1080p": "1080p", "4k": "4K"}.get(SIZE, SIZE), metric.upper())
 
 
 def parse():
@@ -80,7 +84,7 @@ def parse():
     ap.add_argument("--metric", default=None)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--pairs", type=int, default=None, help="pairs per step (default 32 at 1080p, 16 at 4K)")
-    ap.add_argument("--size", default="1080p", choices=sorted(SIZES))
+    ap.add_argument("--size", default="1080p", help="1080p, 4k, or WxH (e.g. 1100x300, a profiling case)")
     ap.add_argument("--batch", action="store_true",
                     help="uneven-size batch: 256 pairs, sides uniform in [256, 2048], SSIM + FSIM through one "
                          "CUDA-graph batch plan")
