@@ -206,8 +206,15 @@ InputImage load_image(const std::string &path) {
     try {
         if (!in) throw std::runtime_error("can't fopen");
         std::vector<unsigned char> f((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+        if (f.size() >= 8 && f[0] == 137 && f[1] == 'P' && f[2] == 'N' && f[3] == 'G') return decode_png(f);
         if (f.size() >= 2 && f[0] == 'P' && (f[1] == '5' || f[1] == '6')) return decode_pnm(f);
-        return decode_png(f);
+        if (f.size() >= 2 && f[0] == 'B' && f[1] == 'M') return decode_bmp(f);
+        // TGA has no signature: like the reference's loader, try it when nothing else matched
+        try {
+            return decode_tga(f);
+        } catch (const std::exception &) {
+            throw std::runtime_error("unknown image type");
+        }
     } catch (const std::exception &e) {
         throw std::runtime_error("Failed to load image '" + path + "', reason: " + e.what());
     }

@@ -23,7 +23,8 @@ def cli():
 def png_check(tmp_path_factory):
     exe = str(tmp_path_factory.mktemp("native") / "png_check")
     subprocess.run(["/usr/bin/g++", "-O1", "-std=c++20", "-I", HOST, "-o", exe,
-                    os.path.join(ROOT, "tests", "native", "png_check.cpp"), os.path.join(HOST, "png_io.cpp"), "-lz"],
+                    os.path.join(ROOT, "tests", "native", "png_check.cpp"), os.path.join(HOST, "png_io.cpp"),
+                    os.path.join(HOST, "image_formats.cpp"), "-lz"],
                    check=True)
     return exe
 
@@ -73,6 +74,44 @@ def test_pnm_decoder(png_check, tmp_path):
     Image.fromarray(arr).save(path)
     got = decode(png_check, path)
     assert np.array_equal(got[..., :3], arr) and np.all(got[..., 3] == 255)
+
+
+@pytest.mark.parametrize("mode", ["RGB", "RGBA", "P", "L"])
+def test_bmp_decoder_matches_pil(png_check, tmp_path, mode):
+    from PIL import Image
+    rng = np.random.default_rng(8)
+    arr = rng.integers(0, 256, (23, 37, 3), dtype=np.uint8)
+    im = Image.fromarray(arr)
+    im = im.convert("P", palette=Image.ADAPTIVE, colors=64) if mode == "P" else im.convert(mode)
+    path = str(tmp_path / "t.bmp")
+    im.save(path)
+    got = decode(png_check, path)
+    want = np.asarray(Image.open(path).convert("RGBA"))
+    assert np.array_equal(got[..., :3], want[..., :3])
+
+
+@pytest.mark.parametrize("mode", ["RGB", "RGBA", "L", "P"])
+@pytest.mark.parametrize("rle", [False, True])
+@pytest.mark.parametrize("origin", ["bl", "tl"])
+def test_tga_decoder_matches_pil(png_check, tmp_path, mode, rle, origin):
+    from PIL import Image
+    rng = np.random.default_rng(9)
+    arr = rng.integers(0, 256, (19, 31, 3), dtype=np.uint8)
+    arr[5:9, :, :] = 77  # runs for the run-length form
+    im = Image.fromarray(arr)
+    im = im.convert("P", palette=Image.ADAPTIVE, colors=32) if mode == "P" else im.convert(mode)
+    path = str(tmp_path / "t.tga")
+    im.save(path, compression="tga_rle" if rle else None, orientation=1 if origin == "tl" else -1)
+    got = decode(png_check, path)
+    want = np.asarray(Image.open(path).convert("RGBA"))
+    assert np.array_equal(got[..., :3], want[..., :3])
+
+
+def test_unknown_image_type_is_rejected(png_check, tmp_path):
+    path = str(tmp_path / "x.bin")
+    open(path, "wb").write(b"\x00\x01not an image at all")
+    r = subprocess.run([png_check, path], capture_output=True, text=True)
+    assert r.returncode != 0 and "unknown image type" in r.stderr
 
 
 def test_grey_png_encoder_round_trip(png_check, tmp_path):
