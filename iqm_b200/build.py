@@ -35,8 +35,8 @@ def stale():
     return any(os.path.getmtime(f) > t for f in sources() + headers())
 
 
-HOST_SRC = ["methods.cpp", "args.cpp", "png_io.cpp", "image_formats.cpp", "iqm_cuda.cpp", "batch_pipeline.cpp",
-            "main.cpp"]
+HOST_SRC = ["methods.cpp", "args.cpp", "png_io.cpp", "image_formats.cpp", "jpeg_decode.cpp", "iqm_cuda.cpp",
+            "batch_pipeline.cpp", "main.cpp"]
 CUDA_INC = os.path.join(os.path.dirname(os.path.dirname(NVCC)), "include")  # NVTX3 (header-only)
 CLI = os.path.join(HERE, "bin", "IQM")
 CXX = os.environ.get("IQM_CXX", "/usr/bin/g++")

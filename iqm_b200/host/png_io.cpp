@@ -209,6 +209,7 @@ InputImage load_image(const std::string &path) {
         if (f.size() >= 8 && f[0] == 137 && f[1] == 'P' && f[2] == 'N' && f[3] == 'G') return decode_png(f);
         if (f.size() >= 2 && f[0] == 'P' && (f[1] == '5' || f[1] == '6')) return decode_pnm(f);
         if (f.size() >= 2 && f[0] == 'B' && f[1] == 'M') return decode_bmp(f);
+        if (f.size() >= 3 && f[0] == 0xFF && f[1] == 0xD8 && f[2] == 0xFF) return decode_jpeg(f);
         // TGA has no signature: like the reference's loader, try it when nothing else matched
         try {
             return decode_tga(f);

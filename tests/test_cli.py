@@ -24,7 +24,7 @@ def png_check(tmp_path_factory):
     exe = str(tmp_path_factory.mktemp("native") / "png_check")
     subprocess.run(["/usr/bin/g++", "-O1", "-std=c++20", "-I", HOST, "-o", exe,
                     os.path.join(ROOT, "tests", "native", "png_check.cpp"), os.path.join(HOST, "png_io.cpp"),
-                    os.path.join(HOST, "image_formats.cpp"), "-lz"],
+                    os.path.join(HOST, "image_formats.cpp"), os.path.join(HOST, "jpeg_decode.cpp"), "-lz"],
                    check=True)
     return exe
 
@@ -105,6 +105,44 @@ def test_tga_decoder_matches_pil(png_check, tmp_path, mode, rle, origin):
     got = decode(png_check, path)
     want = np.asarray(Image.open(path).convert("RGBA"))
     assert np.array_equal(got[..., :3], want[..., :3])
+
+
+@pytest.mark.parametrize("subsampling", [0, 1, 2])
+@pytest.mark.parametrize("size", [(48, 64), (37, 53)])
+def test_jpeg_decoder_close_to_pil(png_check, tmp_path, subsampling, size):
+    """Baseline JPEG (4:4:4, 4:2:2, 4:2:0; odd sizes): a lossy format decodes to slightly different
+    bytes in different decoders, so the bound is a few levels per channel."""
+    from PIL import Image
+    from iqm_b200 import synth
+    h, w = size
+    a, _ = synth.rgb_gain_pair(h, w, config=1, pair=1)
+    path = str(tmp_path / "t.jpg")
+    Image.fromarray(a[..., :3]).save(path, quality=90, subsampling=subsampling)
+    got = decode(png_check, path)[..., :3].astype(int)
+    want = np.asarray(Image.open(path).convert("RGB")).astype(int)
+    d = np.abs(got - want)
+    assert d.max() <= 4 and d.mean() <= 0.6, (d.max(), d.mean())
+
+
+def test_jpeg_grey_and_restart_intervals(png_check, tmp_path):
+    from PIL import Image
+    from iqm_b200 import synth
+    a, _ = synth.grey_pair(45, 70, config=0, pair=2)
+    for name, im, kw in (("g.jpg", Image.fromarray(a[..., 0]), {}),
+                         ("r.jpg", Image.fromarray(a[..., :3]), {"restart_marker_blocks": 3})):
+        path = str(tmp_path / name)
+        im.save(path, quality=85, **kw)
+        got = decode(png_check, path)[..., :3].astype(int)
+        want = np.asarray(Image.open(path).convert("RGB")).astype(int)
+        assert np.abs(got - want).max() <= 4
+
+
+def test_progressive_jpeg_is_refused(png_check, tmp_path):
+    from PIL import Image
+    path = str(tmp_path / "p.jpg")
+    Image.fromarray(np.zeros((16, 16, 3), np.uint8)).save(path, progressive=True)
+    r = subprocess.run([png_check, path], capture_output=True, text=True)
+    assert r.returncode != 0 and "progressive" in r.stderr
 
 
 def test_unknown_image_type_is_rejected(png_check, tmp_path):
