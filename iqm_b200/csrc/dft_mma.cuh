@@ -29,6 +29,8 @@
 
 #include <cuda_fp16.h>
 
+#include <type_traits>
+
 namespace iqm {
 
 __device__ __forceinline__ void mma_f16_16816(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
@@ -59,12 +61,15 @@ __device__ __forceinline__ float2 unit_root(int m, int L, float sign) {
     return make_float2(c, sign * s);
 }
 
-template <int N1_, int N2_, int SPLIT>
+// REGS: keep the stage-C matrix and the twiddles in registers instead of the shared table (fewer
+// shared-memory loads per transform, more registers).
+template <int N1_, int N2_, int SPLIT, bool REGS = false>
 struct MmaDft {
     static constexpr int N1 = N1_, N2 = N2_, N = N1 * N2;
     static constexpr int NT2 = (N2 + 7) / 8;      // stage A column tiles (n2); stage C k-tiles
     static constexpr int NTC = (2 * N2 + 7) / 8;  // stage C column tiles (2 k2 + c)
     static constexpr int P = SPLIT == 1 ? 1 : 2;  // parts of each constant (hi, lo)
+    static constexpr bool kRegs = REGS;
     static_assert(N1 >= 2 && N1 <= 16 && N2 >= 2 && N2 <= 32, "factor range of the MMA engine");
     static_assert(SPLIT == 1 || SPLIT == 3, "SPLIT is 1 or 3 products");
 
@@ -76,13 +81,31 @@ struct MmaDft {
     static constexpr int FA_WORDS = P * 2 * 2 * 4 * 32;
     static constexpr int FC_ENTRIES = P * NT2 * NTC * 32;
     static constexpr int TW_ENTRIES = 2 * NT2 * 2 * 32;
-    static constexpr size_t smem_bytes = sizeof(uint2) * FC_ENTRIES + sizeof(float2) * TW_ENTRIES;
-    static constexpr size_t table_bytes = sizeof(unsigned) * FA_WORDS + smem_bytes;
-    static_assert(sizeof(unsigned) * FA_WORDS % 16 == 0 && smem_bytes % 16 == 0, "16-byte table parts");
+    static constexpr size_t shared_part = sizeof(uint2) * FC_ENTRIES + sizeof(float2) * TW_ENTRIES;
+    static constexpr size_t smem_bytes = REGS ? 0 : shared_part;  // shared memory the engine needs
+    static constexpr size_t table_bytes = sizeof(unsigned) * FA_WORDS + shared_part;
+    static_assert(sizeof(unsigned) * FA_WORDS % 16 == 0 && shared_part % 16 == 0, "16-byte table parts");
 
     unsigned fa[P][2][2][4];  // stage A matrix: [part][m-tile: Re/Im out][k-tile][register]
     const uint2 *fcs;         // shared stage C table
     const float2 *tws;        // shared twiddle table
+    uint2 fcr[REGS ? P : 1][REGS ? NT2 : 1][REGS ? NTC : 1];  // the same in registers (REGS)
+    float2 twr[REGS ? 2 : 1][REGS ? NT2 : 1][REGS ? 2 : 1];
+
+    __device__ __forceinline__ uint2 fc_at(int p, int kc, int nc) const {
+        if constexpr (REGS) {
+            return fcr[p][kc][nc];
+        } else {
+            return fcs[((p * NT2 + kc) * NTC + nc) * 32 + (threadIdx.x & 31)];
+        }
+    }
+    __device__ __forceinline__ float2 tw_at(int r, int j, int e) const {
+        if constexpr (REGS) {
+            return twr[r][j][e];
+        } else {
+            return tws[((r * NT2 + j) * 2 + e) * 32 + (threadIdx.x & 31)];
+        }
+    }
 
     // Writes the table for transforms of sign `sign` (+1 inverse, -1 forward); run by one warp.
     static __device__ void build(void *table, float sign) {
@@ -159,11 +182,29 @@ struct MmaDft {
                 for (int kt = 0; kt < 2; kt++)
 #pragma unroll
                     for (int q = 0; q < 4; q++) fa[p][mt][kt][q] = __ldg(fa_g + (((p * 2 + mt) * 2 + kt) * 4 + q) * 32 + lane);
-        const uint4 *src = reinterpret_cast<const uint4 *>(fa_g + FA_WORDS);
-        uint4 *dst = static_cast<uint4 *>(shared);
-        for (int i = threadIdx.x; i < int(smem_bytes / 16); i += blockDim.x) dst[i] = __ldg(src + i);
-        fcs = static_cast<const uint2 *>(shared);
-        tws = reinterpret_cast<const float2 *>(fcs + FC_ENTRIES);
+        if constexpr (REGS) {
+            const uint2 *fc_g = reinterpret_cast<const uint2 *>(fa_g + FA_WORDS);
+            const float2 *tw_g = reinterpret_cast<const float2 *>(fc_g + FC_ENTRIES);
+#pragma unroll
+            for (int p = 0; p < P; p++)
+#pragma unroll
+                for (int kc = 0; kc < NT2; kc++)
+#pragma unroll
+                    for (int nc = 0; nc < NTC; nc++) fcr[p][kc][nc] = __ldg(fc_g + ((p * NT2 + kc) * NTC + nc) * 32 + lane);
+#pragma unroll
+            for (int r = 0; r < 2; r++)
+#pragma unroll
+                for (int j = 0; j < NT2; j++)
+#pragma unroll
+                    for (int e = 0; e < 2; e++) twr[r][j][e] = __ldg(tw_g + ((r * NT2 + j) * 2 + e) * 32 + lane);
+            (void)shared;
+        } else {
+            const uint4 *src = reinterpret_cast<const uint4 *>(fa_g + FA_WORDS);
+            uint4 *dst = static_cast<uint4 *>(shared);
+            for (int i = threadIdx.x; i < int(smem_bytes / 16); i += blockDim.x) dst[i] = __ldg(src + i);
+            fcs = static_cast<const uint2 *>(shared);
+            tws = reinterpret_cast<const float2 *>(fcs + FC_ENTRIES);
+        }
     }
 
     // Output slot s of a lane (0 <= s < 2 NTC) holds X[k1 + N1 k2] with k1 = g + 8 (s & 1),
@@ -171,9 +212,12 @@ struct MmaDft {
     static __device__ __forceinline__ int slot_k1(int s) { return ((threadIdx.x & 31) >> 2) + 8 * (s & 1); }
     static __device__ __forceinline__ int slot_k2(int s) { return 4 * (s >> 1) + (threadIdx.x & 3); }
 
-    // One transform.  ld(n1, n2) returns the (already scaled) input x[N2 n1 + n2] as float2 for
-    // n1 < N1, n2 < N2; st(k, slot, v) receives output X[k] (in this lane's `slot`) for every k < N
-    // exactly once across the warp.  All 32 lanes must call it together (warp-synchronous MMAs).
+    // One transform.  ld(n1, n2) returns the (already scaled) input x[N2 n1 + n2] for n1 < N1,
+    // n2 < N2, either as float2 or, for inputs that already are FP16, as the raw bits of a __half2
+    // (real part in the low half), which go into the MMA operand as they are (and, being exact,
+    // need no lo part in the split form); st(k, slot, v) receives output X[k] (in this lane's
+    // `slot`) for every k < N exactly once across the warp.  All 32 lanes must call it together
+    // (warp-synchronous MMAs).
     template <class Load, class Store>
     __device__ __forceinline__ void run(Load ld, Store st) const {
         const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -191,21 +235,31 @@ struct MmaDft {
 #pragma unroll
             for (int kt = 0; kt < 2; kt++) {
                 const int n1a = 8 * kt + t, n1b = n1a + 4;
-                const float2 xa = (n1a < N1 && n2 < N2) ? ld(n1a, n2) : make_float2(0.f, 0.f);
-                const float2 xb = (n1b < N1 && n2 < N2) ? ld(n1b, n2) : make_float2(0.f, 0.f);
-                if constexpr (SPLIT == 1) {
-                    const unsigned b0 = pack_h2(xa.x, xa.y), b1 = pack_h2(xb.x, xb.y);
-#pragma unroll
-                    for (int mt = 0; mt < 2; mt++) mma_f16_16816(acc[mt][j], fa[0][mt][kt], b0, b1);
-                } else {
-                    unsigned h0, l0, h1, l1;
-                    split_h2(xa.x, xa.y, h0, l0);
-                    split_h2(xb.x, xb.y, h1, l1);
+                if constexpr (std::is_same<decltype(ld(0, 0)), unsigned>::value) {
+                    const unsigned b0 = (n1a < N1 && n2 < N2) ? ld(n1a, n2) : 0u;
+                    const unsigned b1 = (n1b < N1 && n2 < N2) ? ld(n1b, n2) : 0u;
 #pragma unroll
                     for (int mt = 0; mt < 2; mt++) {
-                        mma_f16_16816(acc[mt][j], fa[0][mt][kt], h0, h1);
-                        mma_f16_16816(acc[mt][j], fa[0][mt][kt], l0, l1);
-                        mma_f16_16816(acc[mt][j], fa[1][mt][kt], h0, h1);
+                        mma_f16_16816(acc[mt][j], fa[0][mt][kt], b0, b1);
+                        if constexpr (SPLIT == 3) mma_f16_16816(acc[mt][j], fa[1][mt][kt], b0, b1);
+                    }
+                } else {
+                    const float2 xa = (n1a < N1 && n2 < N2) ? ld(n1a, n2) : make_float2(0.f, 0.f);
+                    const float2 xb = (n1b < N1 && n2 < N2) ? ld(n1b, n2) : make_float2(0.f, 0.f);
+                    if constexpr (SPLIT == 1) {
+                        const unsigned b0 = pack_h2(xa.x, xa.y), b1 = pack_h2(xb.x, xb.y);
+#pragma unroll
+                        for (int mt = 0; mt < 2; mt++) mma_f16_16816(acc[mt][j], fa[0][mt][kt], b0, b1);
+                    } else {
+                        unsigned h0, l0, h1, l1;
+                        split_h2(xa.x, xa.y, h0, l0);
+                        split_h2(xb.x, xb.y, h1, l1);
+#pragma unroll
+                        for (int mt = 0; mt < 2; mt++) {
+                            mma_f16_16816(acc[mt][j], fa[0][mt][kt], h0, h1);
+                            mma_f16_16816(acc[mt][j], fa[0][mt][kt], l0, l1);
+                            mma_f16_16816(acc[mt][j], fa[1][mt][kt], h0, h1);
+                        }
                     }
                 }
             }
@@ -215,7 +269,7 @@ struct MmaDft {
         for (int j = 0; j < NT2; j++)
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                const float2 w = tws[(((q >> 1) * NT2 + j) * 2 + (q & 1)) * 32 + lane];
+                const float2 w = tw_at(q >> 1, j, q & 1);
                 const float re = acc[0][j][q], im = acc[1][j][q];
                 acc[0][j][q] = re * w.x - im * w.y;
                 acc[1][j][q] = re * w.y + im * w.x;
@@ -237,7 +291,7 @@ struct MmaDft {
                                        pack_h2(c1[2], c1[3])};
 #pragma unroll
                 for (int nc = 0; nc < NTC; nc++) {
-                    const uint2 b = fcs[(kc * NTC + nc) * 32 + lane];
+                    const uint2 b = fc_at(0, kc, nc);
                     mma_f16_16816(out[nc], a, b.x, b.y);
                 }
             } else {
@@ -248,8 +302,8 @@ struct MmaDft {
                 split_h2(c1[2], c1[3], ah[3], al[3]);
 #pragma unroll
                 for (int nc = 0; nc < NTC; nc++) {
-                    const uint2 bh = fcs[(kc * NTC + nc) * 32 + lane];
-                    const uint2 bl = fcs[((NT2 + kc) * NTC + nc) * 32 + lane];
+                    const uint2 bh = fc_at(0, kc, nc);
+                    const uint2 bl = fc_at(1, kc, nc);
                     mma_f16_16816(out[nc], ah, bh.x, bh.y);
                     mma_f16_16816(out[nc], al, bh.x, bh.y);
                     mma_f16_16816(out[nc], ah, bl.x, bl.y);

@@ -774,8 +774,8 @@ struct MmaColGeom {
 };
 
 template <class Dft>
-// Single-product engines fit 3 CTAs per SM without spills; split-precision ones 2.
-__global__ void __launch_bounds__(32 * MCW, Dft::P == 1 ? 3 : 2)
+// Single-product engines with shared tables fit 3 CTAs per SM without spills; the others 2.
+__global__ void __launch_bounds__(32 * MCW, Dft::P == 1 && !Dft::kRegs ? 3 : 2)
     fsim_inv_cols_mma_kernel(FsimGroup g, const void *__restrict__ table, int items) {
     using Gm = MmaColGeom<Dft>;
     constexpr int H = Gm::H;
@@ -847,6 +847,9 @@ __global__ void __launch_bounds__(32 * MCW, Dft::P == 1 ? 3 : 2)
     }
 }
 
+// The 32 bits of an FP16 pair, to go into an MMA operand unchanged.
+__device__ __forceinline__ unsigned h2_word(__half2 h) { return *reinterpret_cast<unsigned *>(&h); }
+
 // Row pass: a work item is one row of one (orientation, plane), taken by one warp on its own: it
 // transforms the row for the 4 scales, reading its FP16 inputs straight from the intermediate
 // planes, parks the first 3 scales' outputs in its own shared slots and keeps the last in
@@ -880,7 +883,7 @@ __global__ void __launch_bounds__(32 * MRW, Dft::P == 1 ? 2 : 1)
 #pragma unroll 1
         for (int s = 0; s < 4; s++) {
             const __half2 *src = g.Th + (size_t(plane) * 16 + o * 4 + s) * g.n + size_t(y) * W;
-            dft.run([&](int n1, int n2) { return __half22float2(src[Dft::N2 * n1 + n2]); },
+            dft.run([&](int n1, int n2) { return h2_word(src[Dft::N2 * n1 + n2]); },
                     [&](int, int slot, float2 v) {
                         if (s < 3)
                             keep[(s * SL + slot) * 32 + lane] = v;
