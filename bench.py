@@ -183,6 +183,16 @@ def cpu_baseline(metric, pairs, seconds, one_pair_only=False):
                 done, workload_name(metric), W, H, el)}
 
 
+def oracle_errors(pairs, form_scores):
+    """Largest |score - FP64 oracle| over the pairs and both scores, per FSIM form (part of the CPU
+    baseline leg: the oracle is the checker here)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle
+    o64 = Oracle("f64")
+    want = np.array([o64.fsim(a, b) for a, b in pairs])
+    return {name: float(np.abs(s - want).max()) for name, s in form_scores.items()}
+
+
 def run_reference(args, metric, rank, world):
     """--impl reference: the reference's arithmetic on the host CPU (the oracle port)."""
     if rank != 0:
@@ -516,6 +526,36 @@ def main():
     ms_per_step = ms / args.steps
     value = world * B / (ms_per_step / 1e3)
 
+    # FSIM: the three forms (plain FP32, tensor-core split-precision, tensor-core single products) on
+    # the same device buffers, timed the same way, with their scores of the distinct pairs kept for
+    # the error against the FP64 oracle (reported with the CPU baseline)
+    forms, form_scores = None, {}
+    if metric == "fsim":
+        forms = {}
+        for fname, fprec in (("fp32", iqm_b200.IQM_FP32), ("mixed", iqm_b200.IQM_MIXED),
+                             ("mixed_fast", iqm_b200.IQM_MIXED_FAST)):
+            obj.precision = fprec
+            for _ in range(3):
+                step()
+            torch.cuda.synchronize()
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            for _ in range(args.steps):
+                step()
+            f1.record(stream)
+            torch.cuda.synchronize()
+            fms = f0.elapsed_time(f1)
+            if dist:
+                t = torch.tensor([fms], device="cuda")
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                fms = float(t.item())
+            form_scores[fname] = d_scores[:2 * len(host_pairs)].cpu().numpy().reshape(-1, 2)
+            forms[fname] = {"value": world * B / (fms / args.steps / 1e3), "ms_per_step": fms / args.steps}
+        for fname in forms:
+            forms[fname]["vs_fp32"] = forms[fname]["value"] / forms["fp32"]["value"]
+            forms[fname]["max_score_diff_vs_fp32"] = float(abs(form_scores[fname] - form_scores["fp32"]).max())
+        obj.precision = prec
+
     # per-kernel device time: the same K steps again with an event after every launch on the
     # library's stream (kept out of the throughput timing above)
     rt.set_kernel_timing(True)
@@ -616,8 +656,13 @@ def main():
                    "l2": "inputs larger than L2 (%.0f MB per step), no flush" % (alg_bytes / 1e6)},
         "roofline": roof, "kernels": kernels, "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "clocks": clk,
     }
+    if forms:
+        line["forms"] = forms
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(metric, host_pairs, args.cpu_seconds)
+        if form_scores:
+            # the checker: each FSIM form's scores of the distinct pairs against the FP64 oracle
+            line["forms_err_vs_fp64"] = oracle_errors(host_pairs, form_scores)
     if rank == 0:
         print(json.dumps(line), flush=True)
     rt.close()
