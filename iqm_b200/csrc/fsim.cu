@@ -915,8 +915,11 @@ __global__ void mma_table_kernel(void *table) {
 }
 
 // Tensor-core transform engines of the mixed forms: 270 = 15 x 18 (columns), 480 = 16 x 30 (rows).
+// Single products keep the column engine's stage-C matrix and twiddles in registers (measured 5%
+// faster than the shared table at 1080p); split products keep them in shared memory (registers
+// would spill).
 template <int SPLIT>
-using MmaCol270 = iqm::MmaDft<15, 18, SPLIT>;
+using MmaCol270 = iqm::MmaDft<15, 18, SPLIT, SPLIT == 1>;
 template <int SPLIT>
 using MmaRow480 = iqm::MmaDft<16, 30, SPLIT>;
 
