@@ -511,165 +511,6 @@ __global__ void __launch_bounds__(CW_T, 2) flip_vcols_kernel(FlipArgs args, cons
 }
 
 // ---------------------------------------------------------------------------------------------
-// Fused pass for compile-time radii: the column walkers above, fed from shared memory.  Before each
-// block of K output rows the CTA computes the horizontal pass (YCxCz of the strip's 32 columns plus
-// an R-column halo on each side, then the feature and CSF row taps) of the K image rows that block
-// needs, into a shared buffer of 12 planes x 32 columns per row; the walkers read their new rows
-// from there.  The 12 FP32 planes (96 MB per 1080p pair) never reach HBM: the kernel reads each
-// input pixel about (32 + 2R) / 32 times (halo columns) plus 2R / (10 K) for the halo rows.
-constexpr int FU_CPT = 2;  // output columns per row-tap task of the fused pass
-template <int RF, int RC>
-struct FuGeom {
-    static constexpr int R = RF > RC ? RF : RC, K = 2 * R + 1;
-    static constexpr int COLS = 32 + 2 * R;                           // staged YCxCz columns
-    static constexpr size_t ycc_floats = size_t(4) * K * 2 * COLS;    // [row][img][col] float4
-    static constexpr size_t h_floats = size_t(K) * NPLANE * 32;       // [row][plane][col]
-    static constexpr size_t px_floats = size_t(K) * CW_ROLES * 32;    // [row][role][col]
-    static constexpr size_t smem = sizeof(float) * (ycc_floats + h_floats + px_floats);
-};
-
-// Horizontal pass of image rows y_first .. y_first + nrows - 1 (each clamped into the image) for the
-// strip's columns x0 .. x0 + 31 into hb[row][plane][column], planes per image: dx, ddx, value (the
-// feature taps edge, point and g on (Y + 16) / 116) and the CSF-filtered Y, Cx, Cz, as
-// flip_hpass_kernel computes them.  Ends with a CTA barrier.
-template <int RF, int RC>
-__device__ __forceinline__ void fu_hpass(const FlipPairDev &P, const FlipTaps &T, const float *lin, int x0, int y_first,
-                                         int nrows, float4 *ycc, float *hb) {
-    using G = FuGeom<RF, RC>;
-    constexpr int R = G::R, COLS = G::COLS;
-    for (int q = threadIdx.x; q < nrows * 2 * COLS; q += blockDim.x) {
-        const int c = q % COLS, t = q / COLS;
-        const int img = t & 1, row = t >> 1;
-        const int y = min(max(y_first + row, 0), P.h - 1), x = min(max(x0 - R + c, 0), P.w - 1);
-        const uint32_t px = __ldg(reinterpret_cast<const uint32_t *>((img ? P.b : P.a) + (long long)y * P.pitch) + x);
-        const float r = lin[px & 0xffu], g = lin[(px >> 8) & 0xffu], b = lin[(px >> 16) & 0xffu];
-        const float X = fmaf(T.rgb2xyz[0], r, fmaf(T.rgb2xyz[1], g, T.rgb2xyz[2] * b)) * T.inv_white[0];
-        const float Y = fmaf(T.rgb2xyz[3], r, fmaf(T.rgb2xyz[4], g, T.rgb2xyz[5] * b)) * T.inv_white[1];
-        const float Z = fmaf(T.rgb2xyz[6], r, fmaf(T.rgb2xyz[7], g, T.rgb2xyz[8] * b)) * T.inv_white[2];
-        const float Yc = fmaf(116.0f, Y, -16.0f);
-        ycc[t * COLS + c] = make_float4(Yc, 500.0f * (X - Y), 200.0f * (Y - Z), (Yc + 16.0f) / 116.0f);
-    }
-    __syncthreads();
-    // one task = FU_CPT consecutive output columns of one (row, image): a register window slides
-    // along the taps (output column i, tap j reads staged column i + R - j)
-    constexpr int CPT = FU_CPT, GROUPS = 32 / FU_CPT;
-    for (int task = threadIdx.x; task < nrows * 2 * GROUPS; task += blockDim.x) {
-        const int cg = task % GROUPS, t = task / GROUPS;
-        const int img = t & 1, row = t >> 1;
-        const float4 *src = ycc + t * COLS + CPT * cg;
-        float fa[CPT][3] = {}, ca[CPT][3] = {};
-        float4 win[CPT];
-#pragma unroll
-        for (int i = 0; i < CPT - 1; i++) win[i + 1] = src[i];
-#pragma unroll
-        for (int u = 0; u <= 2 * R; u++) {
-#pragma unroll
-            for (int i = 0; i < CPT - 1; i++) win[i] = win[i + 1];
-            win[CPT - 1] = src[u + CPT - 1];
-            const int j = R - u;
-            if (j >= -RF && j <= RF) {
-                const float wg = T.feat[0][j + RF], we = T.feat[1][j + RF], wp = T.feat[2][j + RF];
-#pragma unroll
-                for (int i = 0; i < CPT; i++) {
-                    fa[i][0] = fmaf(we, win[i].w, fa[i][0]);  // dx   (edge)
-                    fa[i][1] = fmaf(wp, win[i].w, fa[i][1]);  // ddx  (point)
-                    fa[i][2] = fmaf(wg, win[i].w, fa[i][2]);  // value (gauss)
-                }
-            }
-            if (j >= -RC && j <= RC) {
-                const float w0 = T.csf[0][j + RC], w1 = T.csf[1][j + RC], w2 = T.csf[2][j + RC];
-#pragma unroll
-                for (int i = 0; i < CPT; i++) {
-                    ca[i][0] = fmaf(w0, win[i].x, ca[i][0]);
-                    ca[i][1] = fmaf(w1, win[i].y, ca[i][1]);
-                    ca[i][2] = fmaf(w2, win[i].z, ca[i][2]);
-                }
-            }
-        }
-        float *dst = hb + (size_t(row) * NPLANE + img * 6) * 32 + CPT * cg;
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-#pragma unroll
-            for (int i = 0; i < CPT; i++) {
-                dst[c * 32 + i] = fa[i][c];
-                dst[(3 + c) * 32 + i] = ca[i][c];
-            }
-    }
-    __syncthreads();
-}
-
-template <int RF, int RC>
-__global__ void __launch_bounds__(CW_T, 2) flip_fused_kernel(FlipArgs args, const __grid_constant__ FlipTaps T) {
-    using G = FuGeom<RF, RC>;
-    constexpr int R = G::R, K = G::K;
-    constexpr int SEG = cw_rows(RF, RC);
-    extern __shared__ __align__(16) float fu_buf[];
-    float4 *ycc = reinterpret_cast<float4 *>(fu_buf);
-    float *hb = fu_buf + G::ycc_floats;
-    float *pxb = hb + G::h_floats;
-    __shared__ float lin[256];
-    __shared__ double red[CW_T / 32];
-    __shared__ int is_last;
-    const int gt = blockIdx.x;
-    const int pi = find_tile(args.pairs, args.npairs, gt);
-    const FlipPairDev P = args.pairs[pi];
-    const int local = gt - P.tile_base;
-    const int x0 = (local % P.tiles_x) * 32, y0 = (local / P.tiles_x) * SEG;
-    const int lane = threadIdx.x & 31, role = threadIdx.x >> 5;
-    const int f = role % 7, m = role / 7;
-    // plane of each role within the image's six: dx, ddx, value, Y, Cx, Cz
-    const int pl = m * 6 + (f == 0 ? 0 : f == 1 ? 2 : f == 2 ? 1 : f == 3 ? 2 : f - 1);
-    // this role's taps: image row y - k weighs tap k + radius; feature roles use g, edge, g, point
-    const float *tap_src = f < 4 ? T.feat[f == 1 ? 1 : f == 3 ? 2 : 0] : T.csf[f - 4];
-    const int rad = f < 4 ? RF : RC;
-    for (int i = threadIdx.x; i < 256; i += CW_T) lin[i] = T.lin[i];
-    __syncthreads();
-    // the window's first K - 1 rows: image rows y0 - R .. y0 + R - 1
-    fu_hpass<RF, RC>(P, T, lin, x0, y0 - R, K - 1, ycc, hb);
-    float win[K];
-#pragma unroll
-    for (int t = 0; t < K - 1; t++) win[t] = hb[(t * NPLANE + pl) * 32 + lane];
-    double dsum = 0.0;
-    for (int b = 0; b < CW_BLOCKS; b++) {
-        const int yb = y0 + b * K;  // first output row of the block
-        if (yb >= P.h) break;       // uniform over the CTA
-        __syncthreads();            // the window's reads of hb are done before it is refilled
-        fu_hpass<RF, RC>(P, T, lin, x0, yb + R, K, ycc, hb);  // rows yb + R .. yb + R + K - 1
-        float taps[K];
-#pragma unroll
-        for (int u = 0; u < K; u++) {
-            const int k = R - u;
-            taps[u] = (k >= -rad && k <= rad) ? tap_src[k + rad] : 0.f;
-        }
-#pragma unroll
-        for (int j = 0; j < K; j++) {
-            // window slot (j + u) % K holds image row yb - R + j + u of output row yb + j
-            win[(j + K - 1) % K] = hb[(j * NPLANE + pl) * 32 + lane];
-            float acc = 0.f;
-#pragma unroll
-            for (int u = 0; u < K; u++) acc = fmaf(win[(j + u) % K], taps[u], acc);
-            pxb[(j * CW_ROLES + role) * 32 + lane] = acc;
-        }
-        __syncthreads();
-        for (int p = threadIdx.x; p < K * 32; p += CW_T) {
-            const int j = p >> 5, c = p & 31;
-            const int y = yb + j, x = x0 + c;
-            if (y >= P.h || x >= P.w) continue;
-            float v[2][7];
-            const float *px = pxb + j * CW_ROLES * 32 + c;
-#pragma unroll
-            for (int mm = 0; mm < 2; mm++)
-#pragma unroll
-                for (int q = 0; q < 7; q++) v[mm][q] = px[(mm * 7 + q) * 32];
-            const float val = flip_pixel(T, v);
-            if (P.map) P.map[size_t(y) * size_t(P.w) + x] = val;
-            dsum += double(val);
-        }
-    }
-    pool_tile<CW_T>(args, P, pi, gt, dsum, red, is_last);
-}
-
-// ---------------------------------------------------------------------------------------------
 // host side
 
 double ppd_of(const iqm_flip_params &p) {  // src/gpu/flip/flip.cpp:125 (float operands)
@@ -803,8 +644,7 @@ void flip_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_fl
     IQM_REQUIRE(segs < (1LL << 31) && tiles < (1 << 30), "batch too large");
     auto *d_desc = static_cast<FlipPairDev *>(iqm::upload_bytes(ctx, ctx->desc, hd.data(), sizeof(FlipPairDev) * n));
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
-    // only the two-kernel path for other radii keeps the 12 horizontal-pass planes in memory
-    const size_t pb = fixed ? 0 : al(sizeof(float) * size_t(plane_floats)), qb = al(sizeof(double) * tiles),
+    const size_t pb = al(sizeof(float) * size_t(plane_floats)), qb = al(sizeof(double) * tiles),
                  cb = al(sizeof(unsigned) * n);
     auto *base = static_cast<uint8_t *>(ctx->scratch.get(pb + qb + cb, ctx->stream));
     FlipArgs a{};
@@ -819,18 +659,24 @@ void flip_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_fl
     iqm::timing_mark(ctx, nullptr);
     const int R = std::max(T.rf, T.rc);
     const size_t smem = sizeof(float) * NPLANE * (VT_ROWS + 2 * R) * VT_COLS;
+    // dynamic shared memory of the column walkers: CW_GROUP blocks of K rows x 14 roles x 32 columns
+    auto cw_smem = [](int rf, int rc) { return sizeof(float) * CW_GROUP * (2 * std::max(rf, rc) + 1) * CW_ROLES * 32; };
     if (fixed == 1) {  // default monitor, 52.1 ppd
-        const size_t sm = FuGeom<7, 8>::smem;
-        IQM_CHECK_CUDA(cudaFuncSetAttribute((const void *)flip_fused_kernel<7, 8>,
+        flip_hpass_kernel<7, 8><<<unsigned(segs), HT, 0, ctx->stream>>>(a, T);
+        iqm::check_launch(ctx, "flip_hpass_kernel");
+        const size_t sm = cw_smem(7, 8);
+        IQM_CHECK_CUDA(cudaFuncSetAttribute((const void *)flip_vcols_kernel<7, 8>,
                                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-        flip_fused_kernel<7, 8><<<tiles, CW_T, sm, ctx->stream>>>(a, T);
-        iqm::check_launch(ctx, "flip_fused_kernel");
+        flip_vcols_kernel<7, 8><<<tiles, CW_T, sm, ctx->stream>>>(a, T);
+        iqm::check_launch(ctx, "flip_vcols_kernel");
     } else if (fixed == 2) {  // 67 ppd
-        const size_t sm = FuGeom<9, 10>::smem;
-        IQM_CHECK_CUDA(cudaFuncSetAttribute((const void *)flip_fused_kernel<9, 10>,
+        flip_hpass_kernel<9, 10><<<unsigned(segs), HT, 0, ctx->stream>>>(a, T);
+        iqm::check_launch(ctx, "flip_hpass_kernel");
+        const size_t sm = cw_smem(9, 10);
+        IQM_CHECK_CUDA(cudaFuncSetAttribute((const void *)flip_vcols_kernel<9, 10>,
                                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-        flip_fused_kernel<9, 10><<<tiles, CW_T, sm, ctx->stream>>>(a, T);
-        iqm::check_launch(ctx, "flip_fused_kernel");
+        flip_vcols_kernel<9, 10><<<tiles, CW_T, sm, ctx->stream>>>(a, T);
+        iqm::check_launch(ctx, "flip_vcols_kernel");
     } else {
         flip_hpass_kernel<0, 0><<<unsigned(segs), HT, 0, ctx->stream>>>(a, T);
         iqm::check_launch(ctx, "flip_hpass_kernel");
