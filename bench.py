@@ -312,7 +312,10 @@ def run_batch(args, rank, world, local):
     plans = []
     if n:
         plans.append(iqm_b200.BatchPlan(rt, iqm_b200.METRIC_SSIM, g_items, d_ssim.data_ptr(), autotune=False))
-        plans.append(iqm_b200.BatchPlan(rt, iqm_b200.METRIC_FSIM, c_items, d_fsim.data_ptr(), autotune=True))
+        prec = {"fp32": iqm_b200.IQM_FP32, "mixed": iqm_b200.IQM_MIXED,
+                "mixed_fast": iqm_b200.IQM_MIXED_FAST}[args.precision]
+        plans.append(iqm_b200.BatchPlan(rt, iqm_b200.METRIC_FSIM, c_items, d_fsim.data_ptr(), precision=prec,
+                                        autotune=True))
     launches = sum(p.info()[1] for p in plans)
 
     def step():
@@ -405,7 +408,7 @@ def run_batch(args, rank, world, local):
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded; crops of 2 distinct 2048x2048 pairs per metric)",
         "config": {"workload": "batch256_ssim_fsim", "pairs_per_step": N, "sizes": "w, h uniform in [256, 2048]",
-                   "precision": "fp32", "parallelism": "lpt shards" if world > 1 else "single",
+                   "precision": args.precision, "parallelism": "lpt shards" if world > 1 else "single",
                    "form": "one CUDA-graph batch plan per metric, FSIM shapes autotuned",
                    "l2": "inputs larger than L2 (%.0f MB per metric per step), no flush" % (total_bytes / 1e6)},
         "roofline": roof,
