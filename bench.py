@@ -647,6 +647,32 @@ def main():
     e2e = {"value": world * B / (ems / e2e_steps / 1e3), "unit": "pairs/s",
            "h2d_bytes_per_step": B * 2 * img_bytes, "d2h_bytes_per_step": B * nscore * 8}
 
+    # the host link's own ceiling: the same pinned buffers copied to the device with nothing else
+    # running (one plain copy per image, as the e2e step issues), timed like the e2e step
+    link = torch.empty(B * 2 * img_bytes, dtype=torch.uint8, device="cuda")
+
+    def link_step():
+        off = 0
+        for pa, pb in pin:
+            for t in (pa, pb):
+                n = t.numel() * t.element_size()
+                link[off:off + n].copy_(t.view(torch.uint8).reshape(-1), non_blocking=True)
+                off += n
+
+    with torch.cuda.stream(stream):
+        link_step()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            link_step()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    lms = e0.elapsed_time(e1) / e2e_steps
+    del link
+    e2e["h2d_gbs"] = B * 2 * img_bytes / (ems / e2e_steps) / 1e6
+    e2e["h2d_copy_only_gbs"] = B * 2 * img_bytes / lms / 1e6
+    e2e["link_frac"] = e2e["h2d_gbs"] / e2e["h2d_copy_only_gbs"]
+
     line = {
         "metric": metric_name(metric), "value": value, "unit": "pairs/s",
         "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_per_step,
