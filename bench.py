@@ -64,8 +64,19 @@ TRAFFIC = {
 # 32 inverse transforms of each of the 480 columns (270 = 15 x 18: 27 m16n8k16 tiles) and of each
 # of the 270 rows (480 = 16 x 30: 48 tiles), 2 * 16 * 8 * 16 = 4096 flops a tile, times the products
 # per tile (3 with split-precision operands, 1 with single FP16 operands).
-MMA_TILES_PER_PAIR = {"fsim_inv_cols_mma_kernel": 32 * 480 * 27, "fsim_inv_rows_mma_kernel": 32 * 270 * 48}
+# The mixed SSIM forms run one CTA per 64x32 output tile: 4 warps, each with 3 x 16 horizontal and
+# 2 x 16 vertical m16n8k16 tiles (4 moments x 2 n-tiles x 2 k-steps per 16-row block).
 MMA_PRODUCTS = {"mixed": 3, "mixed_fast": 1}
+
+
+def mma_tiles_per_pair(kernel, w, h):
+    if kernel == "fsim_inv_cols_mma_kernel":
+        return 32 * 480 * 27
+    if kernel == "fsim_inv_rows_mma_kernel":
+        return 32 * 270 * 48
+    if kernel == "ssim_mma_kernel":
+        return -(-w // 64) * -(-h // 32) * 4 * (48 + 32)
+    return 0
 
 
 def workload_name(metric):
@@ -90,7 +101,7 @@ def parse():
                          "CUDA-graph batch plan")
     ap.add_argument("--distinct", type=int, default=4, help="distinct synthetic pairs (replicated to --pairs)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed", "mixed_fast"],
-                    help="FSIM form: FP32 transforms, or tensor-core transforms with FP16 planes "
+                    help="FSIM and SSIM form: FP32, or the tensor-core forms with FP16 operands "
                          "(split-precision hi + lo products, or single products)")
     ap.add_argument("--flip-monitor", default="3840,0.7,0.7",
                     help="FLIP viewing set-up RES,DISTANCE,WIDTH (default 67.02 pixels per degree)")
@@ -183,13 +194,14 @@ def cpu_baseline(metric, pairs, seconds, one_pair_only=False):
                 done, workload_name(metric), W, H, el)}
 
 
-def oracle_errors(pairs, form_scores):
-    """Largest |score - FP64 oracle| over the pairs and both scores, per FSIM form (part of the CPU
+def oracle_errors(metric, pairs, form_scores):
+    """Largest |score - FP64 oracle| over the pairs and their scores, per form (part of the CPU
     baseline leg: the oracle is the checker here)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import Oracle
     o64 = Oracle("f64")
-    want = np.array([o64.fsim(a, b) for a, b in pairs])
+    fn = o64.fsim if metric == "fsim" else o64.ssim
+    want = np.array([fn(a, b) for a, b in pairs]).reshape(len(pairs), -1)
     return {name: float(np.abs(s - want).max()) for name, s in form_scores.items()}
 
 
@@ -311,9 +323,12 @@ def run_batch(args, rank, world, local):
     torch.cuda.synchronize()
     plans = []
     if n:
-        plans.append(iqm_b200.BatchPlan(rt, iqm_b200.METRIC_SSIM, g_items, d_ssim.data_ptr(), autotune=False))
         prec = {"fp32": iqm_b200.IQM_FP32, "mixed": iqm_b200.IQM_MIXED,
                 "mixed_fast": iqm_b200.IQM_MIXED_FAST}[args.precision]
+        sp = iqm_b200.SSIM(rt)
+        sp.precision = prec
+        plans.append(iqm_b200.BatchPlan(rt, iqm_b200.METRIC_SSIM, g_items, d_ssim.data_ptr(), ssim=sp.params(),
+                                        autotune=False))
         plans.append(iqm_b200.BatchPlan(rt, iqm_b200.METRIC_FSIM, c_items, d_fsim.data_ptr(), precision=prec,
                                         autotune=True))
     launches = sum(p.info()[1] for p in plans)
@@ -349,9 +364,11 @@ def run_batch(args, rank, world, local):
     ktimes = {}
     if n:
         rt.set_kernel_timing(True)
+        fs = iqm_b200.FSIM(rt)
+        fs.precision = prec
         for _ in range(2):
-            iqm_b200.SSIM(rt).compute_dev(g_items, d_ssim.data_ptr())
-            iqm_b200.FSIM(rt).compute_dev(c_items, d_fsim.data_ptr())
+            sp.compute_dev(g_items, d_ssim.data_ptr())
+            fs.compute_dev(c_items, d_fsim.data_ptr())
         ktimes = rt.kernel_times()
         rt.set_kernel_timing(False)
     ktotal = sum(t for _, t in ktimes.values()) or 1.0
@@ -479,7 +496,7 @@ def main():
     rt.set_stream(stream.cuda_stream)
     obj = {"fsim": iqm_b200.FSIM, "ssim": iqm_b200.SSIM, "flip": iqm_b200.FLIP, "msvd": iqm_b200.SVD}[metric](rt)
     prec = {"fp32": iqm_b200.IQM_FP32, "mixed": iqm_b200.IQM_MIXED, "mixed_fast": iqm_b200.IQM_MIXED_FAST}[args.precision]
-    if metric == "fsim":
+    if metric in ("fsim", "ssim"):
         obj.precision = prec
     nscore = WORKLOADS[metric][2]
     res_x, dist_m, width_m = (float(v) for v in args.flip_monitor.split(","))
@@ -529,11 +546,11 @@ def main():
     ms_per_step = ms / args.steps
     value = world * B / (ms_per_step / 1e3)
 
-    # FSIM: the three forms (plain FP32, tensor-core split-precision, tensor-core single products) on
-    # the same device buffers, timed the same way, with their scores of the distinct pairs kept for
-    # the error against the FP64 oracle (reported with the CPU baseline)
+    # FSIM and SSIM: the three forms (plain FP32, tensor-core split-precision, tensor-core single
+    # products) on the same device buffers, timed the same way, with their scores of the distinct
+    # pairs kept for the error against the FP64 oracle (reported with the CPU baseline)
     forms, form_scores = None, {}
-    if metric == "fsim":
+    if metric in ("fsim", "ssim"):
         forms = {}
         for fname, fprec in (("fp32", iqm_b200.IQM_FP32), ("mixed", iqm_b200.IQM_MIXED),
                              ("mixed_fast", iqm_b200.IQM_MIXED_FAST)):
@@ -552,7 +569,7 @@ def main():
                 t = torch.tensor([fms], device="cuda")
                 dist.all_reduce(t, op=dist.ReduceOp.MAX)
                 fms = float(t.item())
-            form_scores[fname] = d_scores[:2 * len(host_pairs)].cpu().numpy().reshape(-1, 2)
+            form_scores[fname] = d_scores[:nscore * len(host_pairs)].cpu().numpy().reshape(-1, nscore)
             forms[fname] = {"value": world * B / (fms / args.steps / 1e3), "ms_per_step": fms / args.steps}
         for fname in forms:
             forms[fname]["vs_fp32"] = forms[fname]["value"] / forms["fp32"]["value"]
@@ -587,10 +604,11 @@ def main():
             "avg_launch_us": avg_s * 1e6, "kernel_share": ktimes[kname][1] / ktotal,
             "pipeline_frac": alg_bytes / (ms_per_step / 1e3) / 1e9 / hbm_peak,
             "timing": "CUDA events on the library stream around every launch, second pass of the K steps"}
-    if metric == "fsim" and args.precision in MMA_PRODUCTS:
+    if metric in ("fsim", "ssim") and args.precision in MMA_PRODUCTS:
         # tensor pipe of the tensor-core kernels: executed MMA flops per launch / average launch time
         tens = {}
-        for k, tiles in MMA_TILES_PER_PAIR.items():
+        for k in ("fsim_inv_cols_mma_kernel", "fsim_inv_rows_mma_kernel", "ssim_mma_kernel"):
+            tiles = mma_tiles_per_pair(k, W, H)
             if k not in ktimes:
                 continue
             n_l, t_ms = ktimes[k]
@@ -680,7 +698,7 @@ def main():
         "data": "synthetic (seeded 1/f^2 noise pairs, %d distinct replicated to %d device buffers)" % (
             len(host_pairs), B),
         "config": {"workload": workload_name(metric), "pairs_per_step": B, "width": W, "height": H,
-                   "precision": args.precision if metric == "fsim" else "fp32",
+                   "precision": args.precision if metric in ("fsim", "ssim") else "fp32",
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (%.0f MB per step), no flush" % (alg_bytes / 1e6)},
         "roofline": roof, "kernels": kernels, "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "clocks": clk,
@@ -691,7 +709,7 @@ def main():
         line["cpu_baseline"] = cpu_baseline(metric, host_pairs, args.cpu_seconds)
         if form_scores:
             # the checker: each FSIM form's scores of the distinct pairs against the FP64 oracle
-            line["forms_err_vs_fp64"] = oracle_errors(host_pairs, form_scores)
+            line["forms_err_vs_fp64"] = oracle_errors(metric, host_pairs, form_scores)
     if rank == 0:
         print(json.dumps(line), flush=True)
     rt.close()

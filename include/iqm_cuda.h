@@ -48,10 +48,13 @@ typedef enum {
     IQM_MIXED = 1,      /* FSIM: inverse transforms on the tensor cores as FP16 tiles with
                            split-precision (hi + lo) products and FP32 accumulation, FP16
                            intermediate planes; FP64 noise threshold and pooling as in IQM_FP32.
-                           Scores within 1e-4 of the FP64 oracle.  Plane sizes without tensor-core
-                           engines (all but 480x270, the plane of 1080p and 4K pairs) run the FP32
-                           transforms.  Other metrics compute in FP32 whatever is asked.           */
-    IQM_MIXED_FAST = 2  /* as IQM_MIXED with single FP16 products (hi parts only)               */
+                           Plane sizes without tensor-core engines (all but 480x270, the plane of
+                           1080p and 4K pairs) run the FP32 transforms.
+                           SSIM: the Gaussian window sums on the tensor cores, moments staged as
+                           FP16 hi + lo pairs, split-precision products, FP32 accumulation.
+                           Scores within 1e-4 of the FP64 oracle.  FLIP and M-SVD compute in FP32
+                           whatever is asked.                                                      */
+    IQM_MIXED_FAST = 2  /* as IQM_MIXED with single FP16 operands and products (hi parts only)  */
 } iqm_precision;
 
 /* ---- context --------------------------------------------------------------------------- */
@@ -73,6 +76,7 @@ typedef struct {
     float k1;        /* default 0.01 */
     float k2;        /* default 0.03 */
     float sigma;     /* default 1.5  */
+    int precision;   /* iqm_precision; default IQM_FP32 (a zeroed struct asks for FP32)         */
 } iqm_ssim_params;
 void iqm_ssim_default_params(iqm_ssim_params *p);
 
@@ -96,8 +100,8 @@ int iqm_ssim(iqm_ctx *ctx, const uint8_t *rgba_in, const uint8_t *rgba_ref, int 
  * contexts, or after cudaDeviceReset, are not supported.  All calls share the one array: calls
  * that overlap on the GPU (other streams, other threads) race -- serialise them.  `d_in`, `d_ref`,
  * `row_bytes` and `d_map` must be multiples of 4 and `d_mssim` of 8 (else IQM_EINVAL, before any
- * launch).  Returns IQM_OK, IQM_EINVAL (null or misaligned pointer, size or parameter out of
- * range) or IQM_ECUDA (a launch of this call failed; errors pending from the caller's earlier work
+ * launch).  Only IQM_FP32 is served here: another `params->precision` returns IQM_EINVAL.
+ * Returns IQM_OK, IQM_EINVAL (null or misaligned pointer, size or parameter out of range) or IQM_ECUDA (a launch of this call failed; errors pending from the caller's earlier work
  * are left pending, not reported or cleared). */
 #define IQM_SSIM_NOALLOC_MAX_TILES 4096
 int iqm_ssim_noalloc(const uint8_t *d_in, const uint8_t *d_ref, int w, int h, size_t row_bytes,
@@ -197,7 +201,8 @@ int iqm_host_free(void *p);
 #define IQM_METRIC_MSVD 8
 
 /* Host pairs (sizes may differ): upload, evaluate every metric of the mask, copy the scores to the
- * host and return.  ssim/flip may be NULL for the defaults. */
+ * host and return.  ssim/flip may be NULL for the defaults.  `precision` is FSIM's; SSIM takes its
+ * own from ssim->precision (the defaults: IQM_FP32). */
 int iqm_batch(iqm_ctx *ctx, int metric_mask, const iqm_pair *pairs, int n, const iqm_ssim_params *ssim,
               const iqm_flip_params *flip, iqm_precision precision, int energy_mode, double *scores);
 

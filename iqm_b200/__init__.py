@@ -51,7 +51,7 @@ class IQMError(RuntimeError):
 
 class SSIMParams(ctypes.Structure):
     _fields_ = [("kernel_size", ctypes.c_int), ("k1", ctypes.c_float), ("k2", ctypes.c_float),
-                ("sigma", ctypes.c_float)]
+                ("sigma", ctypes.c_float), ("precision", ctypes.c_int)]
 
 
 class FLIPParams(ctypes.Structure):
@@ -263,9 +263,10 @@ class SSIM:
         self.k_1 = 0.01
         self.k_2 = 0.03
         self.sigma = 1.5
+        self.precision = IQM_FP32  # IQM_MIXED / IQM_MIXED_FAST: tensor-core window sums
 
     def params(self):
-        return SSIMParams(self.kernel_size, self.k_1, self.k_2, self.sigma)
+        return SSIMParams(self.kernel_size, self.k_1, self.k_2, self.sigma, self.precision)
 
     def compute_metric(self, image, ref, want_map=True):
         image, ref = _img(image), _img(ref)

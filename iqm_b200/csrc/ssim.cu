@@ -23,6 +23,7 @@
 //   * (u, v) pairs are processed with packed FP32x2 instructions (__ffma2_rn and friends);
 //   * MSSIM partials go to per-tile FP64 slots; the last CTA of a pair sums them in a fixed order
 //     (deterministic, no second launch).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -141,6 +142,47 @@ __device__ __forceinline__ void convert_row(Smem &sm, const SsimPairDev &P, int 
             o = make_float2((la + lb) - cu, (la - lb) - cv);
         }
         dst[q] = o;
+    }
+}
+
+// Deterministic pooling, shared by the SSIM kernels: the CTA's partial (FP64, fixed order) goes to
+// its tile slot; the last CTA of the pair to finish sums the pair's slots in a fixed order and
+// writes the mean (`count` pooled pixels).  `red` holds NTH/32 doubles of shared memory.
+template <int NTH>
+__device__ __forceinline__ void pool_tiles(float acc, double *red, int *is_last, double *partials,
+                                           unsigned *counters, double *scores, int pi, const SsimPairDev &P,
+                                           int gt, double count) {
+    const int tid = threadIdx.x;
+    double d = double(acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
+    if ((tid & 31) == 0) red[tid >> 5] = d;
+    __syncthreads();
+    if (tid == 0) {
+        double s = 0.0;
+#pragma unroll
+        for (int i = 0; i < NTH / 32; i++) s += red[i];
+        partials[gt] = s;
+        __threadfence();
+        const unsigned prev = atomicAdd(&counters[pi], 1u);
+        *is_last = (prev == unsigned(P.ntiles - 1));
+    }
+    __syncthreads();
+    if (!*is_last) return;
+    __threadfence();
+    double s = 0.0;
+    for (int i = tid; i < P.ntiles; i += NTH) s += __ldcg(&partials[P.tile_base + i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    __syncthreads();
+    if ((tid & 31) == 0) red[tid >> 5] = s;
+    __syncthreads();
+    if (tid == 0) {
+        double tot = 0.0;
+#pragma unroll
+        for (int i = 0; i < NTH / 32; i++) tot += red[i];
+        scores[pi] = tot / count;
+        counters[pi] = 0u;  // ready for the next launch
     }
 }
 
@@ -286,41 +328,15 @@ __global__ void __launch_bounds__(NT, 8) ssim_kernel(SsimArgs args) {
         }
     }
     cp_async_wait<0>();
-
-    // ---- deterministic pooling: CTA partial -> per-tile slot -> last CTA of the pair ----
-    double d = double(acc);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
-    if ((tid & 31) == 0) red[tid >> 5] = d;
-    __syncthreads();
-    if (tid == 0) {
-        double s = 0.0;
-#pragma unroll
-        for (int i = 0; i < NT / 32; i++) s += red[i];
-        args.partials[gt] = s;
-        __threadfence();
-        const unsigned prev = atomicAdd(&args.counters[pi], 1u);
-        is_last = (prev == unsigned(P.ntiles - 1));
-    }
-    __syncthreads();
-    if (!is_last) return;
-    __threadfence();
-    double s = 0.0;
-    for (int i = tid; i < P.ntiles; i += NT) s += __ldcg(&args.partials[P.tile_base + i]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    __syncthreads();
-    if ((tid & 31) == 0) red[tid >> 5] = s;
-    __syncthreads();
-    if (tid == 0) {
-        double tot = 0.0;
-#pragma unroll
-        for (int i = 0; i < NT / 32; i++) tot += red[i];
-        const double cnt = double(W - 2 * R + 1) * double(H - 2 * R + 1);
-        args.scores[pi] = tot / cnt;
-        args.counters[pi] = 0u;  // ready for the next launch
-    }
+    pool_tiles<NT>(acc, red, &is_last, args.partials, args.counters, args.scores, pi, P, gt,
+                   double(W - 2 * R + 1) * double(H - 2 * R + 1));
 }
+
+}  // namespace
+
+#include "ssim_mma.cuh"
+
+namespace {
 
 template <int R>
 void launch_ssim(const SsimArgs &a, int total_tiles, cudaStream_t s) {
@@ -344,6 +360,22 @@ void check_params(const iqm_ssim_params &p) {
     IQM_REQUIRE(R >= 1 && R <= 7, "kernel_size must give a radius (kernel_size-1)/2 in [1, 7]");
     IQM_REQUIRE(p.sigma > 0.f && std::isfinite(p.sigma), "sigma must be positive");
     IQM_REQUIRE(std::isfinite(p.k1) && std::isfinite(p.k2), "k1/k2 must be finite");
+    IQM_REQUIRE(p.precision == IQM_FP32 || p.precision == IQM_MIXED || p.precision == IQM_MIXED_FAST,
+                "unknown precision " + std::to_string(p.precision));
+}
+
+// The tensor-core kernel (one 64x32 tile per CTA) for IQM_MIXED (split products) and
+// IQM_MIXED_FAST (single products).
+// Persistent launch: as many CTAs as fit on the device at once (at most one per tile).
+template <int SPLIT>
+void launch_ssim_mma(const SsimMmaArgs &a, int total_tiles, int device, cudaStream_t s) {
+    const size_t smem = SsimMmaGeom<SPLIT>::smem_bytes;
+    IQM_CHECK_CUDA(cudaFuncSetAttribute(ssim_mma_kernel<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int sms = 0, per_sm = 0;
+    IQM_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    IQM_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ssim_mma_kernel<SPLIT>, MT_THREADS, smem));
+    const int grid = std::max(1, std::min(total_tiles, sms * std::max(1, per_sm)));
+    ssim_mma_kernel<SPLIT><<<grid, MT_THREADS, smem, s>>>(a, total_tiles);
 }
 
 // Enqueue SSIM for device-resident pairs; `maps[i]` (device, nullable) receive the SSIM maps.
@@ -351,7 +383,8 @@ void ssim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_ss
                   const std::vector<float *> &maps, double *d_scores) {
     const int n = int(pairs.size());
     const int R = (p.kernel_size - 1) / 2;
-    const int S = strip_rows(R);
+    const bool mma = p.precision != IQM_FP32;
+    const int tw = mma ? MT_W : TW, th = mma ? MT_H : strip_rows(R);
     std::vector<SsimPairDev> hd(n);
     int total = 0;
     for (int i = 0; i < n; i++) {
@@ -363,8 +396,8 @@ void ssim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_ss
         d.pitch = (long long)q.row_bytes;
         d.w = q.w;
         d.h = q.h;
-        d.tiles_x = int(iqm::ceil_div(q.w, TW));
-        d.ntiles = d.tiles_x * int(iqm::ceil_div(q.h, S));
+        d.tiles_x = int(iqm::ceil_div(q.w, tw));
+        d.ntiles = d.tiles_x * int(iqm::ceil_div(q.h, th));
         d.tile_base = total;
         d.vec_ok = ((reinterpret_cast<uintptr_t>(q.input) | reinterpret_cast<uintptr_t>(q.ref) |
                      uintptr_t(q.row_bytes)) & 15u) == 0;
@@ -375,18 +408,36 @@ void ssim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_ss
     const size_t part_bytes = (sizeof(double) * total + 255) & ~size_t(255);
     const size_t cnt_bytes = (sizeof(unsigned) * n + 255) & ~size_t(255);
     auto *scr = static_cast<uint8_t *>(ctx->scratch.get(part_bytes + cnt_bytes, ctx->stream));
+    double g64[15] = {}, gsum = 0.0;
+    for (int k = -R; k <= R; k++) gsum += (g64[k + R] = std::exp(-double(k * k) / (2.0 * double(p.sigma) * p.sigma)));
+    auto *counters = reinterpret_cast<unsigned *>(scr + part_bytes);
+    IQM_CHECK_CUDA(cudaMemsetAsync(counters, 0, sizeof(unsigned) * n, ctx->stream));
+    iqm::timing_mark(ctx, nullptr);
+    if (mma) {
+        SsimMmaArgs a{};
+        a.pairs = d_desc;
+        a.npairs = n;
+        a.R = R;
+        a.partials = reinterpret_cast<double *>(scr);
+        a.counters = counters;
+        a.scores = d_scores;
+        for (int k = 0; k < 15; k++) a.gn[k] = float(g64[k] / gsum);
+        a.c1 = p.k1 * p.k1;
+        a.c2 = p.k2 * p.k2;
+        if (p.precision == IQM_MIXED) launch_ssim_mma<3>(a, total, ctx->device, ctx->stream);
+        else launch_ssim_mma<1>(a, total, ctx->device, ctx->stream);
+        iqm::check_launch(ctx, "ssim_mma_kernel");
+        return;
+    }
     SsimArgs a{};
     a.pairs = d_desc;
     a.npairs = n;
     a.partials = reinterpret_cast<double *>(scr);
-    a.counters = reinterpret_cast<unsigned *>(scr + part_bytes);
+    a.counters = counters;
     a.scores = d_scores;
-    for (int k = 0; k < 15; k++) a.g[k] = 0.f;
-    for (int k = -R; k <= R; k++) a.g[k + R] = float(std::exp(-double(k * k) / (2.0 * double(p.sigma) * p.sigma)));
+    for (int k = 0; k < 15; k++) a.g[k] = float(g64[k]);
     a.c1 = p.k1 * p.k1;
     a.c2 = p.k2 * p.k2;
-    IQM_CHECK_CUDA(cudaMemsetAsync(a.counters, 0, sizeof(unsigned) * n, ctx->stream));
-    iqm::timing_mark(ctx, nullptr);
     switch (R) {
         case 1: launch_ssim<1>(a, total, ctx->stream); break;
         case 2: launch_ssim<2>(a, total, ctx->stream); break;
@@ -414,6 +465,7 @@ extern "C" __attribute__((visibility("default"))) void iqm_ssim_default_params(i
     p->k1 = 0.01f;
     p->k2 = 0.03f;
     p->sigma = 1.5f;
+    p->precision = IQM_FP32;
 }
 
 void iqm::enqueue_ssim_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, const iqm_ssim_params *params,
@@ -531,6 +583,7 @@ extern "C" __attribute__((visibility("default"))) int iqm_ssim_noalloc(
     } catch (const iqm::Error &e) {
         return e.code;
     }
+    if (p.precision != IQM_FP32) return IQM_EINVAL;  // the fixed scratch is sized for the FP32 tiles
     const int R = (p.kernel_size - 1) / 2;
     if (w < 2 * R || h < 2 * R || w > 65536 || h > 65536 || row_bytes < size_t(w) * 4) return IQM_EINVAL;
     const int tiles_x = int(iqm::ceil_div(w, TW));

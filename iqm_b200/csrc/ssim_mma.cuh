@@ -1,0 +1,400 @@
+// SSIM with the Gaussian window sums on the tensor cores (IQM_MIXED, IQM_MIXED_FAST).
+//
+// Included by ssim.cu (it uses SsimPairDev, find_pair and pool_tiles from there).  The quantities
+// are those of the FP32 kernel -- the four moments of u = a + b and v = a - b about a per-tile
+// shift, the in-image truncated window renormalised per pixel, MSSIM over x, y in [R, dim - R] --
+// with the two 1-D window passes run as banded matrix products (mma.sync m16n8k16, FP16 operands,
+// FP32 accumulation):
+//
+//   horizontal  Ht[c][y] = sum_j Gb[c][j] M[y][x0 - 8 + j]   (c: 16 output columns, j: 32 inputs)
+//   vertical    S[r][c]  = sum_k Gb[r][k] H[y0 - 8 + k][c]   (r: 16 output rows,    k: 32 H rows)
+//
+// with Gb[m][j] = g(j - 8 - m) (the normalised 1-D Gaussian, zero beyond its radius R <= 7, so
+// 16 + 2R <= 32 inputs cover 16 outputs).  The same band matrix is the A operand of both passes.
+// The horizontal pass is computed transposed (output columns as rows of the product), so its
+// accumulators -- m16n8 C fragments of (column, row) -- are, packed to FP16 pairs, exactly the
+// B fragments of the vertical product (k = image row, n = column): the horizontal results never
+// leave registers.  The moments enter the horizontal pass from shared memory through ldmatrix.
+//
+// CTA tile: 64 output columns (4 warps x 16) x 32 output rows (two 16-row blocks); the CTA works
+// from image rows y0-8 .. y0+39 and columns x0-8 .. x0+71.  The kernel is persistent: each CTA walks
+// the tiles blockIdx.x, blockIdx.x + gridDim.x, ...  Per tile: load the RGBA8 rows and stage them
+// as FP16 moment planes (one barrier), then each warp runs
+// its three 16-row horizontal blocks and two vertical blocks (a rolled loop, so the code stays in
+// the instruction cache).  The moments are taken about the tile's centre pixel (u, v) and scaled
+// by 2^12 (largest staged magnitude 4 * 2^12, well inside FP16's range, and small values stay clear
+// of FP16's subnormals).
+//
+// IQM_MIXED stages every moment as an FP16 hi + lo pair and forms each product as
+// A_hi B_hi + A_hi B_lo + A_lo B_hi (about 21 significant bits, MSSIM within ~1e-6 of FP64);
+// IQM_MIXED_FAST uses the hi parts alone (11-bit moments and taps: MSSIM within ~5e-5 of FP64 on
+// large natural and ramp images, up to ~1.1e-4 on small ones where fewer pixels average the
+// rounding; the 32-row shift tile keeps the second moments' cancellation small).  The per-pixel weight
+// normalisation uses the window as the tensor cores see it (FP16-rounded taps in the fast form).
+#pragma once
+
+#include "dft_mma.cuh"
+
+namespace {
+
+constexpr int MT_W = 64;              // output columns per CTA tile
+constexpr int MT_H = 32;              // output rows per CTA tile
+constexpr int MT_THREADS = 128;       // 4 warps, 16 output columns each
+constexpr int MT_ROWS = MT_H + 16;    // staged rows y0-8 .. y0+39 (three 16-row horizontal blocks)
+constexpr int MT_SCOLS = MT_W + 16;   // staged columns x0-8 .. x0+71
+constexpr int MT_LD = 88;             // FP16 row stride of a staged plane: 176 bytes, so the 8 rows
+                                      // of one ldmatrix 8x8 load fall in distinct 16-byte bank groups
+constexpr float MT_SCALE = 4096.f;    // staged moments are scaled by 2^12
+
+struct SsimMmaArgs {
+    const SsimPairDev *pairs;
+    int npairs;
+    int R;               // window radius, 1..7
+    double *partials;    // one per tile
+    unsigned *counters;  // one per pair, zero on entry
+    double *scores;      // one per pair
+    float gn[15];        // g(-R..R) / sum g, zero beyond 2R
+    float c1, c2;
+};
+
+template <int SPLIT>
+struct SsimMmaGeom {
+    static constexpr int PLANES = SPLIT == 1 ? 4 : 8;  // su, sv, su^2, sv^2 (hi), then their lo parts
+    static constexpr int PLANE = MT_ROWS * MT_LD;      // halves per plane
+    static constexpr size_t smem_bytes = size_t(PLANES) * PLANE * 2;
+};
+
+__device__ __forceinline__ void ldmatrix_x4(unsigned (&r)[4], const void *p) {
+    const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(p));
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+
+// Byte k of two RGBA8 words as exact floats: each byte placed under the exponent of 2^23 (an
+// integer-pipe byte permute), then 2^23 subtracted from both at once (instead of the quarter-rate
+// integer-to-float conversion).
+template <int K>
+__device__ __forceinline__ float2 bytes_f2(uint32_t pa, uint32_t pb) {
+    const float2 f = make_float2(__uint_as_float(__byte_perm(pa, 0x4B000000u, 0x7540 + K)),
+                                 __uint_as_float(__byte_perm(pb, 0x4B000000u, 0x7540 + K)));
+    return __fadd2_rn(f, make_float2(-8388608.0f, -8388608.0f));
+}
+
+// The two lumas of a pixel pair, shaders/ssim/ssim_lumapack.glsl:19-21 on unorm bytes.
+__device__ __forceinline__ float2 luma2(uint32_t pa, uint32_t pb) {
+    const float2 r = bytes_f2<0>(pa, pb);
+    const float2 g = bytes_f2<1>(pa, pb);
+    const float2 b = bytes_f2<2>(pa, pb);
+    const float s = 1.0f / 255.0f;
+    float2 l = __fmul2_rn(make_float2(0.114f * s, 0.114f * s), b);
+    l = __ffma2_rn(make_float2(0.581f * s, 0.581f * s), g, l);
+    return __ffma2_rn(make_float2(0.299f * s, 0.299f * s), r, l);
+}
+
+// Stage the tile's moment planes: staged row r = image row y0 - 8 + r, staged column q = image column
+// x0 - 8 + q; positions outside the image hold zero in every plane (they drop out of the sums).
+// The thread's loads are issued in two rounds of four 4-pixel chunks (eight 16-byte loads in
+// flight per thread) ahead of their conversion: two memory round trips per tile, with the code of
+// one round only.  (Prefetching the next tile into shared memory instead hides the round trips but
+// costs a CTA per SM, which measured slower.)
+template <int SPLIT>
+__device__ __forceinline__ void stage_moments(__half *pl, const SsimPairDev &P, int x0, int y0, float cu, float cv) {
+    using G = SsimMmaGeom<SPLIT>;
+    constexpr int CH = MT_SCOLS / 4;  // 4-pixel chunks per staged row
+    constexpr int CHUNKS = MT_ROWS * CH;
+    constexpr int PER_T = (CHUNKS + MT_THREADS - 1) / MT_THREADS;
+    constexpr int HALF = (PER_T + 1) / 2;
+#pragma unroll 1
+    for (int k0 = 0; k0 < PER_T; k0 += HALF) {
+        uint4 ra[HALF], rb[HALF];
+#pragma unroll
+        for (int kk = 0; kk < HALF; kk++) {
+            const int c = threadIdx.x + (k0 + kk) * MT_THREADS;
+            const int r = c / CH, q = c - r * CH;
+            const int y = y0 - 8 + r, x = x0 - 8 + 4 * q;  // x is a multiple of 4: a chunk is all in or all left of 0
+            ra[kk] = make_uint4(0u, 0u, 0u, 0u);
+            rb[kk] = make_uint4(0u, 0u, 0u, 0u);
+            if (c < CHUNKS && y >= 0 && y < P.h && x >= 0 && x < P.w) {
+                const int nv = min(4, P.w - x);
+                const uint8_t *pa = P.a + (long long)y * P.pitch + 4LL * x;
+                const uint8_t *pb = P.b + (long long)y * P.pitch + 4LL * x;
+                if (P.vec_ok && nv == 4) {
+                    ra[kk] = __ldg(reinterpret_cast<const uint4 *>(pa));
+                    rb[kk] = __ldg(reinterpret_cast<const uint4 *>(pb));
+                } else {
+                    const uint32_t *wa = reinterpret_cast<const uint32_t *>(pa);
+                    const uint32_t *wb = reinterpret_cast<const uint32_t *>(pb);
+                    ra[kk].x = __ldg(wa);
+                    rb[kk].x = __ldg(wb);
+                    if (nv > 1) ra[kk].y = __ldg(wa + 1), rb[kk].y = __ldg(wb + 1);
+                    if (nv > 2) ra[kk].z = __ldg(wa + 2), rb[kk].z = __ldg(wb + 2);
+                    if (nv > 3) ra[kk].w = __ldg(wa + 3), rb[kk].w = __ldg(wb + 3);
+                }
+            }
+        }
+#pragma unroll
+        for (int kk = 0; kk < HALF; kk++) {
+            const int c = threadIdx.x + (k0 + kk) * MT_THREADS;
+            if (c >= CHUNKS) break;
+            const int r = c / CH, q = c - r * CH;
+            const int y = y0 - 8 + r, x = x0 - 8 + 4 * q;
+            const int nv = (y >= 0 && y < P.h && x >= 0) ? min(4, P.w - x) : 0;
+            const uint32_t a[4] = {ra[kk].x, ra[kk].y, ra[kk].z, ra[kk].w};
+            const uint32_t b[4] = {rb[kk].x, rb[kk].y, rb[kk].z, rb[kk].w};
+            float m[4][4];  // [moment][pixel]: su, sv, su^2, sv^2 (scaled)
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const float2 l = luma2(a[i], b[i]);
+                // (du, dv) = (la + lb - cu, la - lb - cv); sm = (du, dv) * 2^12; sq = (du, dv) * sm
+                const float2 d = __ffma2_rn(make_float2(l.y, l.y), make_float2(1.f, -1.f),
+                                            __fadd2_rn(make_float2(l.x, l.x), make_float2(-cu, -cv)));
+                float2 sm = __fmul2_rn(d, make_float2(MT_SCALE, MT_SCALE));
+                if (i >= nv) sm = make_float2(0.f, 0.f);  // outside the image
+                const float2 sq = __fmul2_rn(d, sm);
+                m[0][i] = sm.x;
+                m[1][i] = sm.y;
+                m[2][i] = sq.x;
+                m[3][i] = sq.y;
+            }
+            const int off = r * MT_LD + 4 * q;
+#pragma unroll
+            for (int p = 0; p < 4; p++) {
+                if (SPLIT == 1) {
+                    *reinterpret_cast<uint2 *>(pl + p * G::PLANE + off) =
+                        make_uint2(iqm::pack_h2(m[p][0], m[p][1]), iqm::pack_h2(m[p][2], m[p][3]));
+                } else {
+                    unsigned h0, l0, h1, l1;
+                    iqm::split_h2(m[p][0], m[p][1], h0, l0);
+                    iqm::split_h2(m[p][2], m[p][3], h1, l1);
+                    *reinterpret_cast<uint2 *>(pl + p * G::PLANE + off) = make_uint2(h0, h1);
+                    *reinterpret_cast<uint2 *>(pl + (p + 4) * G::PLANE + off) = make_uint2(l0, l1);
+                }
+            }
+        }
+    }
+}
+
+// One 16-row horizontal block (staged rows 16 hb .. 16 hb + 15) of this warp's 16 columns, as the
+// vertical pass's B fragments: hh[p][v][kb] (moment p, output columns 8v..8v+7, block rows
+// 8kb..8kb+7 as the fragment's k rows 2t, 2t+1 (+8)); hl the lo parts (split form).
+template <int SPLIT>
+__device__ __forceinline__ void hpass(const __half *pl, int hb, int warp, const unsigned (&ah)[2][4],
+                                      const unsigned (&al)[2][4], unsigned (&hh)[4][2][2], unsigned (&hl)[4][2][2]) {
+    using G = SsimMmaGeom<SPLIT>;
+    const int lane = threadIdx.x & 31;
+    const int off = (16 * hb + (lane & 7)) * MT_LD + 16 * warp + 8 * (lane >> 3);
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++) {
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            unsigned b[4];
+            ldmatrix_x4(b, pl + p * G::PLANE + off + 8 * nt * MT_LD);
+            if (SPLIT != 1) {
+                unsigned bl[4];
+                ldmatrix_x4(bl, pl + (p + 4) * G::PLANE + off + 8 * nt * MT_LD);
+                // small products first
+                iqm::mma_f16_16816(acc, al[0], b[0], b[1]);
+                iqm::mma_f16_16816(acc, al[1], b[2], b[3]);
+                iqm::mma_f16_16816(acc, ah[0], bl[0], bl[1]);
+                iqm::mma_f16_16816(acc, ah[1], bl[2], bl[3]);
+            }
+            iqm::mma_f16_16816(acc, ah[0], b[0], b[1]);
+            iqm::mma_f16_16816(acc, ah[1], b[2], b[3]);
+            // acc: (output column g / g + 8, block rows 8 nt + 2t, 2t + 1)
+            if (SPLIT == 1) {
+                hh[p][0][nt] = iqm::pack_h2(acc[0], acc[1]);
+                hh[p][1][nt] = iqm::pack_h2(acc[2], acc[3]);
+            } else {
+                iqm::split_h2(acc[0], acc[1], hh[p][0][nt], hl[p][0][nt]);
+                iqm::split_h2(acc[2], acc[3], hh[p][1][nt], hl[p][1][nt]);
+            }
+        }
+    }
+}
+
+// Vertical block: out[p][v][i] for output rows g (i < 2) / g + 8 (i >= 2), columns 8v + 2t + (i & 1),
+// from the horizontal blocks above (h0: k rows 0-15 of the window) and below (h1: k rows 16-31).
+template <int SPLIT>
+__device__ __forceinline__ void vpass(const unsigned (&ah)[2][4], const unsigned (&al)[2][4],
+                                      const unsigned (&h0h)[4][2][2], const unsigned (&h0l)[4][2][2],
+                                      const unsigned (&h1h)[4][2][2], const unsigned (&h1l)[4][2][2],
+                                      float (&out)[4][2][4]) {
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+#pragma unroll
+        for (int v = 0; v < 2; v++) {
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            if (SPLIT != 1) {
+                iqm::mma_f16_16816(acc, al[0], h0h[p][v][0], h0h[p][v][1]);
+                iqm::mma_f16_16816(acc, al[1], h1h[p][v][0], h1h[p][v][1]);
+                iqm::mma_f16_16816(acc, ah[0], h0l[p][v][0], h0l[p][v][1]);
+                iqm::mma_f16_16816(acc, ah[1], h1l[p][v][0], h1l[p][v][1]);
+            }
+            iqm::mma_f16_16816(acc, ah[0], h0h[p][v][0], h0h[p][v][1]);
+            iqm::mma_f16_16816(acc, ah[1], h1h[p][v][0], h1h[p][v][1]);
+#pragma unroll
+            for (int i = 0; i < 4; i++) out[p][v][i] = acc[i];
+        }
+    }
+}
+
+// In-image sum of the effective window taps around position x of a line of length n.
+__device__ __forceinline__ float window_sum(const float *w, int R, int x, int n) {
+    float s = 0.f;
+    for (int k = 0; k <= 2 * R; k++) {
+        const int xx = x + k - R;
+        s += (xx >= 0 && xx < n) ? w[k] : 0.f;
+    }
+    return s;
+}
+
+// SSIM of one output pixel from its four window sums (m1: shifted first moments of u, v; m2: second
+// moments), `inv` the normalisation (1 / (window weight * 2^12)), (cu, cv) the tile's shift.
+__device__ __forceinline__ float ssim_px(float2 m1, float2 m2, float inv, float cu, float cv, float c1, float c2) {
+    const float2 iv = make_float2(inv, inv);
+    const float2 sm = __fmul2_rn(m1, iv);                                     // shifted means
+    const float2 var = __ffma2_rn(m2, iv, __fmul2_rn(sm, make_float2(-sm.x, -sm.y)));
+    const float2 mu = __fadd2_rn(sm, make_float2(cu, cv));
+    const float2 mu2 = __fmul2_rn(mu, mu);
+    // (mean term, variance term) of u and of v; SSIM = prod(0.5 (X - Y) + C) / prod(0.5 (X + Y) + C)
+    const float2 X = make_float2(mu2.x, var.x), Y = make_float2(mu2.y, var.y), C = make_float2(c1, c2);
+    const float2 plus = __ffma2_rn(__fadd2_rn(X, Y), make_float2(0.5f, 0.5f), C);
+    const float2 minus = __ffma2_rn(__ffma2_rn(Y, make_float2(-1.f, -1.f), X), make_float2(0.5f, 0.5f), C);
+    return __fdividef(minus.x * minus.y, plus.x * plus.y);
+}
+
+// Persistent: each CTA walks tiles blockIdx.x, blockIdx.x + gridDim.x, ... (neighbouring tiles run
+// at the same time, so the rows they share meet in L2), keeping the band fragments and a warm
+// instruction cache across tiles.
+template <int SPLIT>
+__global__ void __launch_bounds__(MT_THREADS, SPLIT == 1 ? 4 : 3) ssim_mma_kernel(SsimMmaArgs args, int total_tiles) {
+    extern __shared__ __align__(16) unsigned char ssim_mma_smem[];
+    __half *pl = reinterpret_cast<__half *>(ssim_mma_smem);
+    __shared__ double red[MT_THREADS / 32];
+    __shared__ int is_last;
+    __shared__ float gsh[16];   // the normalised taps g(-R..R), zero beyond
+    __shared__ float weff[16];  // the taps as the tensor cores apply them
+
+    const int R = args.R;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+
+    // the taps into shared memory (a kernel-parameter array indexed at run time would be copied
+    // to local memory whole): gsh as given, weff as the tensor cores apply them
+    if (threadIdx.x < 16) {
+        float v = 0.f;
+#pragma unroll
+        for (int k = 0; k < 15; k++)
+            if (int(threadIdx.x) == k) v = args.gn[k];
+        float w = __half2float(__float2half_rn(v));
+        if (SPLIT != 1) w += __half2float(__float2half_rn(v - w));
+        gsh[threadIdx.x] = v;
+        weff[threadIdx.x] = w;
+    }
+    __syncthreads();
+
+    // band fragments: Gb[m][j] = gn[j - 8 - m + R] where that index lies in 0..2R
+    unsigned ah[2][4], al[2][4];
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int m = g + 8 * (i & 1);
+            const int j = 16 * s + 2 * t + 8 * (i >> 1);
+            const int k0 = j - 8 - m + R, k1 = k0 + 1;
+            const float v0 = (k0 >= 0 && k0 <= 2 * R) ? gsh[k0] : 0.f;
+            const float v1 = (k1 >= 0 && k1 <= 2 * R) ? gsh[k1] : 0.f;
+            if (SPLIT == 1) {
+                ah[s][i] = iqm::pack_h2(v0, v1);
+                al[s][i] = 0u;
+            } else {
+                iqm::split_h2(v0, v1, ah[s][i], al[s][i]);
+            }
+        }
+    float wsum = 0.f;  // interior window sum (1 up to the taps' rounding)
+    for (int k = 0; k <= 2 * R; k++) wsum += weff[k];
+    const float inv_in = 1.0f / (wsum * wsum * MT_SCALE);
+
+    for (int gt = blockIdx.x; gt < total_tiles; gt += gridDim.x) {
+        const int pi = find_pair(args.pairs, args.npairs, gt);
+        const SsimPairDev P = args.pairs[pi];
+        const int local = gt - P.tile_base;
+        const int x0 = (local % P.tiles_x) * MT_W;
+        const int y0 = (local / P.tiles_x) * MT_H;
+        const int W = P.w, H = P.h;
+
+        // shift constants: u, v of the tile's centre pixel
+        float cu, cv;
+        {
+            const int cx = min(x0 + MT_W / 2, W - 1), cy = min(y0 + MT_H / 2, H - 1);
+            const uint32_t pa = __ldg(reinterpret_cast<const uint32_t *>(P.a + (long long)cy * P.pitch) + cx);
+            const uint32_t pb = __ldg(reinterpret_cast<const uint32_t *>(P.b + (long long)cy * P.pitch) + cx);
+            const float2 l = luma2(pa, pb);
+            cu = l.x + l.y;
+            cv = l.x - l.y;
+        }
+
+        // the previous tile's ldmatrix reads ended before the barriers of its pooling
+        stage_moments<SPLIT>(pl, P, x0, y0, cu, cv);
+        __syncthreads();
+
+        // every output pixel in the image, under the full window and pooled
+        const bool interior = x0 >= R && x0 + MT_W - 1 + R <= W - 1 && y0 >= R && y0 + MT_H - 1 + R <= H - 1;
+
+        // normalisation of the lane's rows (g, g + 8 of each output block) and columns (2t, 2t + 1 of
+        // each 8-column half): 1 / (window weight * 2^12), the weight cut at the image border
+        float rx[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int x = x0 + 16 * warp + 8 * (j >> 1) + 2 * t + (j & 1);
+            rx[j] = interior ? 1.f : wsum / window_sum(weff, R, x, W);
+        }
+
+        float acc = 0.f;
+        unsigned hph[4][2][2], hpl[4][2][2], hnh[4][2][2], hnl[4][2][2];
+#pragma unroll 1
+        for (int hb = 0; hb < 3; hb++) {
+            hpass<SPLIT>(pl, hb, warp, ah, al, hnh, hnl);
+            if (hb > 0) {
+                // output rows y0 + 16 (hb - 1) + 0..15 from the window of blocks hb - 1 and hb
+                float out[4][2][4];
+                vpass<SPLIT>(ah, al, hph, hpl, hnh, hnl, out);
+                const int yb = y0 + 16 * (hb - 1) + g;
+                float ry[2];
+#pragma unroll
+                for (int e = 0; e < 2; e++)
+                    ry[e] = interior ? inv_in : inv_in * wsum / window_sum(weff, R, yb + 8 * e, H);
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int v = 0; v < 2; v++) {
+                        const int y = yb + 8 * (i >> 1);
+                        const int x = x0 + 16 * warp + 8 * v + 2 * t + (i & 1);
+                        const float ssim = ssim_px(make_float2(out[0][v][i], out[1][v][i]),
+                                                   make_float2(out[2][v][i], out[3][v][i]),
+                                                   ry[i >> 1] * rx[2 * v + (i & 1)], cu, cv, args.c1, args.c2);
+                        const bool valid = interior || (x < W && y < H);
+                        if (valid && P.map) P.map[(long long)y * W + x] = ssim;
+                        const bool pool = interior || (valid && x >= R && x <= W - R && y >= R && y <= H - R);
+                        acc += pool ? ssim : 0.f;
+                    }
+            }
+#pragma unroll
+            for (int p = 0; p < 4; p++)
+#pragma unroll
+                for (int v = 0; v < 2; v++)
+#pragma unroll
+                    for (int kb = 0; kb < 2; kb++) {
+                        hph[p][v][kb] = hnh[p][v][kb];
+                        hpl[p][v][kb] = hnl[p][v][kb];
+                    }
+        }
+
+        pool_tiles<MT_THREADS>(acc, red, &is_last, args.partials, args.counters, args.scores, pi, P, gt,
+                               double(W - 2 * R + 1) * double(H - 2 * R + 1));
+    }
+}
+
+}  // namespace

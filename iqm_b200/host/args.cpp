@@ -52,7 +52,7 @@ IQM::Args::Args(const unsigned argc, const char *argv[]) {
     if (!have_ref && !batch) throw std::runtime_error("missing reference");
 }
 
-// --precision fp32 | mixed | mixed_fast (FSIM's forms; the other metrics compute in FP32).
+// --precision fp32 | mixed | mixed_fast (the forms of FSIM and SSIM; FLIP and M-SVD compute in FP32).
 iqm_precision IQM::precision_option(const Args &args) {
     auto it = args.options.find("--precision");
     if (it == args.options.end() || it->second == "fp32") return IQM_FP32;

@@ -120,7 +120,12 @@ const char *label(IQM::Method m) {
 int evaluate(const IQM::CUDA::Runtime &rt, IQM::Method m, const iqm_flip_params &flip, iqm_precision precision,
              int energy_mode, const iqm_pair *pairs, int n, double *scores) {
     switch (m) {
-        case IQM::Method::SSIM: return iqm_ssim_batch(rt.ctx, pairs, n, nullptr, scores);
+        case IQM::Method::SSIM: {
+            iqm_ssim_params p;
+            iqm_ssim_default_params(&p);
+            p.precision = int(precision);
+            return iqm_ssim_batch(rt.ctx, pairs, n, &p, scores);
+        }
         case IQM::Method::SVD: return iqm_msvd_batch(rt.ctx, pairs, n, scores);
         case IQM::Method::FSIM: return iqm_fsim_batch(rt.ctx, pairs, n, precision, energy_mode, scores);
         case IQM::Method::FLIP: return iqm_flip_batch(rt.ctx, pairs, n, &flip, scores);

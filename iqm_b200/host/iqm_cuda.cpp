@@ -23,7 +23,7 @@ void Runtime::check(int rc) const {
 SSIMResult SSIM::computeMetric(const Runtime &rt, const InputImage &image, const InputImage &ref) {
     SSIMResult res{std::vector<float>(size_t(image.width) * image.height), unsigned(image.width),
                    unsigned(image.height), 0.f, {}};
-    const iqm_ssim_params p{kernelSize, k_1, k_2, sigma};
+    const iqm_ssim_params p{kernelSize, k_1, k_2, sigma, int(precision)};
     double mssim = 0;
     res.timestamps.mark("start GPU pipeline");
     rt.check(iqm_ssim(rt.ctx, image.data.data(), ref.data.data(), image.width, image.height,

@@ -42,6 +42,7 @@ public:
     float k_1 = 0.01;
     float k_2 = 0.03;
     float sigma = 1.5;
+    iqm_precision precision = IQM_FP32;  // IQM_MIXED / IQM_MIXED_FAST: tensor-core window sums
 };
 
 struct SVDResult {  // src/gpu/svd/svd.h:17-23

@@ -102,6 +102,7 @@ void ssim(const IQM::Args &args) {
     const IQM::CUDA::Runtime rt;
     if (args.verbose) std::cout << "Selected device: " << rt.selectedDevice << std::endl;
     IQM::CUDA::SSIM metric(rt);
+    metric.precision = IQM::precision_option(args);
     const auto start = clk::now();
     auto result = repeated(args, [&] { return metric.computeMetric(rt, input, ref); });
     const auto end = clk::now();

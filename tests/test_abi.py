@@ -32,8 +32,10 @@ def test_library_exports_every_declared_symbol():
 def test_default_params_without_device():
     L = iqm_b200.load_library()
     p = iqm_b200.SSIMParams()
+    p.precision = 7
     L.iqm_ssim_default_params(ctypes.byref(p))
     assert (p.kernel_size, round(p.k1, 6), round(p.k2, 6), p.sigma) == (11, 0.01, 0.03, 1.5)
+    assert p.precision == iqm_b200.IQM_FP32
     f = iqm_b200.FLIPParams()
     L.iqm_flip_default_params(ctypes.byref(f))
     assert (f.monitor_resolution_x, round(f.monitor_distance, 6), round(f.monitor_width, 6)) == (2560.0, 0.7, 0.6)
