@@ -766,11 +766,13 @@ struct MmaColGeom {
     static constexpr int H = Dft::N;                                      // column length
     static constexpr int SEG = Dft::N2 + ((4 - Dft::N2 % 16) + 16) % 16;  // N2 padded to 4 mod 16
     static constexpr int SLAB = Dft::N1 * SEG;                            // padded column, float2
-    static constexpr int SP = 12;  // staging row stride (half2): MCW columns, 16-byte aligned rows
+    // staging row stride (half2): MCW columns; odd, so the 32 lanes' scattered output rows
+    // k = g + 15 t (+ const) fall at most 2 to a bank (a multiple of 4 puts them 4 to a bank)
+    static constexpr int SP = 13;
     static constexpr size_t tables = Dft::smem_bytes;
     static constexpr size_t slab_bytes = sizeof(float2) * 2 * MCW * SLAB;
     static constexpr size_t smem = tables + slab_bytes + sizeof(__half2) * 2 * H * SP;
-    static_assert(MCW == 8 && tables % 16 == 0 && slab_bytes % 16 == 0, "16-byte staging rows");
+    static_assert(MCW == 8 && tables % 16 == 0 && slab_bytes % 16 == 0, "16-byte aligned slab and staging");
 };
 
 template <class Dft>
@@ -832,7 +834,8 @@ __global__ void __launch_bounds__(32 * MCW, Dft::P == 1 && !Dft::kRegs ? 3 : 2)
                 for (int idx = threadIdx.x; idx < 2 * H * 2; idx += blockDim.x) {
                     const int q = idx & 1, r = idx >> 1;  // r = img * H + y
                     const int img = r / H, y = r - img * H;
-                    const uint4 v = *reinterpret_cast<const uint4 *>(stage + r * Gm::SP + 4 * q);
+                    const unsigned *row = reinterpret_cast<const unsigned *>(stage + r * Gm::SP + 4 * q);
+                    const uint4 v = make_uint4(row[0], row[1], row[2], row[3]);
                     *reinterpret_cast<uint4 *>(g.Th + size_t(2 * pr + img) * 16 * g.n + zoff + size_t(y) * g.w2 + 4 * q) = v;
                 }
             } else {
