@@ -1,12 +1,17 @@
-// BMP and TGA input for the command line, written from the formats' specifications (Microsoft's
-// BITMAPINFOHEADER family; Truevision TGA 2.0).  Output is RGBA8 like the reference's
-// stbi_load(..., 4) (src/main.cpp:37-57): grey expands to R = G = B, a missing alpha becomes 255.
-// The metrics ignore alpha, so only the colour bytes matter; for the lossless layouts read here
-// they are the file's bytes.  Covered: BMP with 8-bit palettes, 24-bit and 32-bit pixels
-// (BI_RGB, or BI_BITFIELDS with byte-aligned 8-bit masks), bottom-up or top-down rows; TGA types
-// 1, 2, 3 and their run-length forms 9, 10, 11 with 8-, 24- or 32-bit pixels and 24- or 32-bit
-// colour maps, either origin.  Other layouts are refused with a reason.
+// BMP, TGA, GIF, Radiance HDR and Photoshop PSD input for the command line, written from the
+// formats' specifications (Microsoft's BITMAPINFOHEADER family; Truevision TGA 2.0; GIF89a; the
+// Radiance RGBE picture format; Adobe's PSD file format).  Output is RGBA8 like the reference's
+// stbi_load(..., 4) (src/main.cpp:37-57), including that loader's conversions where a format
+// needs one (see each decoder).  Grey expands to R = G = B, a missing alpha becomes 255.
+// Covered: BMP with 8-bit palettes, 24-bit and 32-bit pixels (BI_RGB, or BI_BITFIELDS with
+// byte-aligned 8-bit masks), bottom-up or top-down rows; TGA types 1, 2, 3 and their run-length
+// forms 9, 10, 11 with 8-, 24- or 32-bit pixels and 24- or 32-bit colour maps, either origin; the
+// first frame of a GIF; HDR with run-length or flat RGBE scanlines; RGB PSD, 8 or 16 bits, raw or
+// PackBits.  Other layouts are refused with a reason.
+#include <cmath>
 #include <cstdint>
+#include <cstdlib>
+#include <cstring>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -23,6 +28,14 @@ uint32_t le16(const std::vector<unsigned char> &f, size_t o) {
 uint32_t le32(const std::vector<unsigned char> &f, size_t o) {
     if (o + 4 > f.size()) throw std::runtime_error("truncated");
     return le16(f, o) | le16(f, o + 2) << 16;
+}
+uint32_t be16(const std::vector<unsigned char> &f, size_t o) {
+    if (o + 2 > f.size()) throw std::runtime_error("truncated");
+    return uint32_t(f[o]) << 8 | uint32_t(f[o + 1]);
+}
+uint32_t be32(const std::vector<unsigned char> &f, size_t o) {
+    if (o + 4 > f.size()) throw std::runtime_error("truncated");
+    return be16(f, o) << 16 | be16(f, o + 2);
 }
 
 // Position (0-7, 8-bit lanes) of an 8-bit channel mask, -1 for an absent channel.
@@ -161,6 +174,318 @@ InputImage decode_tga(const std::vector<unsigned char> &f) {
         for (int32_t x = 0; x < w; x++) {
             const size_t src = size_t(top_left ? y : h - 1 - y) * w + (right_left ? w - 1 - x : x);
             for (int c = 0; c < 4; c++) img.data[(size_t(y) * w + x) * 4 + c] = px[src * 4 + c];
+        }
+    return img;
+}
+
+// First frame of a GIF, as stbi_load composes it: the canvas starts transparent black, the frame's
+// pixels are drawn unless their palette entry is the transparent one, and when the screen's
+// background index is not 0, every canvas pixel the frame's raster did not reach takes the global
+// palette's background entry with alpha 255 -- copied in the loader's internal palette order
+// (B, G, R), which the output keeps.  The LZW stream must start with a clear code.
+InputImage decode_gif(const std::vector<unsigned char> &f) {
+    if (f.size() < 13 || std::memcmp(f.data(), "GIF8", 4) != 0 || (f[4] != '7' && f[4] != '9') || f[5] != 'a')
+        throw std::runtime_error("not a GIF file");
+    const int w = int(le16(f, 6)), h = int(le16(f, 8));
+    const unsigned flags = f[10], bgindex = f[11];
+    check_size(w, h);
+    size_t pos = 13;
+    auto byte = [&]() -> unsigned {
+        if (pos >= f.size()) throw std::runtime_error("truncated");
+        return f[pos++];
+    };
+    unsigned char gpal[256][4] = {}, lpal[256][4] = {};  // r, g, b, a
+    auto read_palette = [&](unsigned char (*pal)[4], int n, int transparent) {
+        for (int i = 0; i < n; i++) {
+            pal[i][0] = byte(), pal[i][1] = byte(), pal[i][2] = byte();
+            pal[i][3] = i == transparent ? 0 : 255;
+        }
+    };
+    if (flags & 0x80) read_palette(gpal, 2 << (flags & 7), -1);
+    int transparent = -1;
+    unsigned eflags = 0;
+    for (;;) {
+        const unsigned tag = byte();
+        if (tag == 0x21) {  // extension
+            const unsigned ext = byte();
+            if (ext == 0xF9) {  // graphic control: disposal, delay, transparent index
+                const unsigned len = byte();
+                if (len == 4) {
+                    eflags = byte();
+                    byte(), byte();
+                    const unsigned t = byte();
+                    if (transparent >= 0) gpal[transparent][3] = 255;
+                    transparent = (eflags & 1) ? int(t) : -1;
+                    if (transparent >= 0) gpal[transparent][3] = 0;
+                } else {
+                    pos += len;
+                }
+            }
+            for (unsigned len; (len = byte()) != 0;) pos += len;  // remaining sub-blocks
+            continue;
+        }
+        if (tag == 0x3B) throw std::runtime_error("GIF has no image");
+        if (tag != 0x2C) throw std::runtime_error("corrupt GIF");
+        // image descriptor
+        const int x0 = int(le16(f, pos)), y0 = int(le16(f, pos + 2));
+        const int fw = int(le16(f, pos + 4)), fh = int(le16(f, pos + 6));
+        pos += 8;
+        if (x0 + fw > w || y0 + fh > h) throw std::runtime_error("GIF frame outside the screen");
+        const unsigned lflags = byte();
+        const unsigned char (*pal)[4] = gpal;
+        if (lflags & 0x80) {
+            read_palette(lpal, 2 << (lflags & 7), (eflags & 1) ? transparent : -1);
+            pal = lpal;
+        } else if (!(flags & 0x80)) {
+            throw std::runtime_error("GIF without colour table");
+        }
+        std::vector<unsigned char> out(size_t(w) * h * 4, 0);
+        std::vector<unsigned char> reached(size_t(w) * h, 0);
+        // raster order, with the 4 passes of an interlaced frame
+        const bool interlaced = lflags & 0x40;
+        int pass = 0, cx = 0, cy = 0, step = interlaced ? 8 : 1;
+        auto put = [&](unsigned idx) {
+            if (cy >= fh) return;
+            const size_t pi = size_t(y0 + cy) * w + (x0 + cx);
+            reached[pi] = 1;
+            if (pal[idx][3] > 128)
+                for (int c = 0; c < 4; c++) out[4 * pi + c] = pal[idx][c];
+            if (++cx >= fw) {
+                cx = 0;
+                cy += step;
+                while (interlaced && cy >= fh && pass < 3) {
+                    static const int start[4] = {0, 4, 2, 1}, steps[4] = {8, 8, 4, 2};
+                    pass++;
+                    cy = start[pass];
+                    step = steps[pass];
+                }
+            }
+        };
+        if (fw == 0) cy = fh;
+        // LZW over the data sub-blocks
+        const unsigned min_size = byte();
+        if (min_size > 12) throw std::runtime_error("corrupt GIF");
+        const int clear = 1 << min_size;
+        std::vector<int> prefix(4096, -1);
+        std::vector<unsigned char> first(4096), suffix(4096), stack(4097);
+        for (int c = 0; c < clear; c++) first[c] = suffix[c] = (unsigned char)c;
+        int size = int(min_size) + 1, avail = clear + 2, old = -1;
+        bool started = false;
+        uint32_t bits = 0;
+        int nbits = 0;
+        size_t block = 0;  // bytes left in the current sub-block
+        for (;;) {
+            if (nbits < size) {
+                if (block == 0) {
+                    block = byte();
+                    if (block == 0) break;  // data ended without an end code
+                }
+                block--;
+                bits |= uint32_t(byte()) << nbits;
+                nbits += 8;
+                continue;
+            }
+            const int code = int(bits & ((1u << size) - 1));
+            bits >>= size;
+            nbits -= size;
+            if (code == clear) {
+                size = int(min_size) + 1;
+                avail = clear + 2;
+                old = -1;
+                started = true;
+                continue;
+            }
+            if (code == clear + 1) {  // end code: skip what is left of the data
+                pos += block;
+                for (unsigned len; (len = byte()) != 0;) pos += len;
+                break;
+            }
+            if (code > avail) throw std::runtime_error("corrupt GIF raster");
+            if (!started) throw std::runtime_error("GIF raster without a clear code");
+            if (old >= 0 && avail < 4096) {  // a full table stays as it is until the next clear code
+                prefix[avail] = old;
+                first[avail] = first[old];
+                suffix[avail] = code == avail ? first[old] : first[code];
+                avail++;
+            } else if (old < 0 && code == avail) {
+                throw std::runtime_error("corrupt GIF raster");
+            }
+            int n = 0;
+            for (int c = code; c >= 0; c = prefix[c]) stack[n++] = suffix[c];
+            while (n) put(stack[--n]);
+            if ((avail & ((1 << size) - 1)) == 0 && avail <= 0x0FFF) size++;
+            old = code;
+        }
+        if (bgindex > 0)
+            for (size_t pi = 0; pi < size_t(w) * h; pi++)
+                if (!reached[pi]) {
+                    out[4 * pi + 0] = gpal[bgindex][2];
+                    out[4 * pi + 1] = gpal[bgindex][1];
+                    out[4 * pi + 2] = gpal[bgindex][0];
+                    out[4 * pi + 3] = 255;
+                }
+        InputImage img;
+        img.width = w;
+        img.height = h;
+        img.data = std::move(out);
+        return img;
+    }
+}
+
+// Radiance HDR converted to 8 bits as stbi_load does: each colour channel is m * 2^(e - 136) (0 when
+// e = 0), then (uint8) clamp(float(pow(v, 1 / 2.2f)) * 255 + 0.5f, 0, 255) with pow in double;
+// alpha is 255.  Header: "#?RADIANCE" or "#?RGBE", a FORMAT=32-bit_rle_rgbe line, a blank line,
+// then "-Y h +X w".  Scanlines of 8 to 32767 pixels may be run-length coded (2, 2, width, then
+// each component's runs); a scanline that does not start that way switches the loader to flat
+// RGBE quadruples from the first pixel on, the quadruple just read being pixel 0.
+InputImage decode_hdr(const std::vector<unsigned char> &f) {
+    size_t pos = 0;
+    auto line = [&]() {
+        std::string t;
+        while (pos < f.size() && f[pos] != '\n' && t.size() < 1023) t += char(f[pos++]);
+        while (pos < f.size() && f[pos] != '\n') pos++;  // an over-long line is cut, as the loader does
+        if (pos < f.size()) pos++;
+        return t;
+    };
+    const std::string magic = line();
+    if (magic != "#?RADIANCE" && magic != "#?RGBE") throw std::runtime_error("not an HDR file");
+    bool valid = false;
+    for (std::string t; !(t = line()).empty();)
+        if (t == "FORMAT=32-bit_rle_rgbe") valid = true;
+    if (!valid) throw std::runtime_error("unsupported HDR format");
+    const std::string res = line();
+    if (res.compare(0, 3, "-Y ") != 0) throw std::runtime_error("unsupported HDR data layout");
+    char *end = nullptr;
+    const long h = std::strtol(res.c_str() + 3, &end, 10);
+    while (*end == ' ') end++;
+    if (std::strncmp(end, "+X ", 3) != 0) throw std::runtime_error("unsupported HDR data layout");
+    const long w = std::strtol(end + 3, nullptr, 10);
+    check_size(w, h);
+    const size_t n = size_t(w) * h;
+    std::vector<unsigned char> rgbe(n * 4);
+    auto byte = [&]() -> unsigned {
+        if (pos >= f.size()) throw std::runtime_error("truncated");
+        return f[pos++];
+    };
+    auto flat_from = [&](size_t first) {
+        for (size_t i = first; i < n; i++)
+            for (int c = 0; c < 4; c++) rgbe[4 * i + c] = (unsigned char)byte();
+    };
+    if (w < 8 || w >= 32768) {
+        flat_from(0);
+    } else {
+        std::vector<unsigned char> sl(size_t(w) * 4);
+        for (long y = 0; y < h; y++) {
+            const unsigned c1 = byte(), c2 = byte(), len = byte();
+            if (c1 != 2 || c2 != 2 || (len & 0x80)) {
+                rgbe[0] = (unsigned char)c1, rgbe[1] = (unsigned char)c2, rgbe[2] = (unsigned char)len;
+                rgbe[3] = (unsigned char)byte();
+                flat_from(1);
+                break;
+            }
+            if (long((len << 8) | byte()) != w) throw std::runtime_error("corrupt HDR scanline");
+            for (int k = 0; k < 4; k++)
+                for (long i = 0; i < w;) {
+                    unsigned count = byte();
+                    if (count > 128) {
+                        const unsigned char v = (unsigned char)byte();
+                        count -= 128;
+                        if (long(count) > w - i) throw std::runtime_error("corrupt HDR run");
+                        while (count--) sl[4 * i++ + k] = v;
+                    } else {
+                        if (count == 0 || long(count) > w - i) throw std::runtime_error("corrupt HDR run");
+                        while (count--) sl[4 * i++ + k] = (unsigned char)byte();
+                    }
+                }
+            std::memcpy(&rgbe[size_t(y) * w * 4], sl.data(), sl.size());
+        }
+    }
+    InputImage img;
+    img.width = int(w);
+    img.height = int(h);
+    img.data.resize(n * 4);
+    const float gamma = 1.0f / 2.2f;
+    for (size_t i = 0; i < n; i++) {
+        const unsigned char *q = &rgbe[4 * i];
+        const float scale = q[3] ? std::ldexp(1.0f, int(q[3]) - 136) : 0.f;
+        for (int c = 0; c < 3; c++) {
+            const float v = q[3] ? float(q[c]) * scale : 0.f;
+            float z = float(std::pow(double(v), double(gamma))) * 255 + 0.5f;
+            z = z < 0 ? 0 : (z > 255 ? 255 : z);
+            img.data[4 * i + c] = (unsigned char)int(z);
+        }
+        img.data[4 * i + 3] = 255;
+    }
+    return img;
+}
+
+// RGB Photoshop files as stbi_load reads them: the composite image after the header sections, 8-bit
+// samples or the high byte of 16-bit ones; with PackBits compression every channel is one run of
+// w * h bytes (the loader does this whatever the depth); missing channels are 0 (alpha 255); with 4
+// or more channels, colours are un-premultiplied from the white matte in float, v * (1 / a) +
+// 255 (1 - 1 / a) with a = alpha / 255, truncated to an integer and kept modulo 256 as the loader's
+// float-to-byte conversion does on x86-64.
+InputImage decode_psd(const std::vector<unsigned char> &f) {
+    if (f.size() < 26 || be32(f, 0) != 0x38425053u) throw std::runtime_error("not a PSD file");
+    if (be16(f, 4) != 1) throw std::runtime_error("unsupported PSD version");
+    const int channels = int(be16(f, 12));
+    if (channels > 16) throw std::runtime_error("unsupported PSD channel count");
+    const int64_t h = be32(f, 14), w = be32(f, 18);
+    const unsigned depth = be16(f, 22);
+    if (depth != 8 && depth != 16) throw std::runtime_error("PSD bit depth is not 8 or 16");
+    if (be16(f, 24) != 3) throw std::runtime_error("PSD is not in RGB colour mode");
+    check_size(w, h);
+    size_t pos = 26;
+    for (int section = 0; section < 3; section++) pos += 4 + size_t(be32(f, pos));  // mode data, resources, layers
+    const unsigned compression = be16(f, pos);
+    pos += 2;
+    if (compression > 1) throw std::runtime_error("unknown PSD compression");
+    const size_t n = size_t(w) * size_t(h);
+    auto byte = [&]() -> unsigned {
+        if (pos >= f.size()) throw std::runtime_error("truncated");
+        return f[pos++];
+    };
+    InputImage img;
+    img.width = int(w);
+    img.height = int(h);
+    img.data.assign(n * 4, 0);
+    unsigned char *out = img.data.data();
+    if (compression) pos += size_t(h) * channels * 2;  // per-row byte counts, not needed
+    for (int c = 0; c < 4; c++) {
+        unsigned char *p = out + c;
+        if (c >= channels) {
+            for (size_t i = 0; i < n; i++, p += 4) *p = c == 3 ? 255 : 0;
+        } else if (compression) {
+            for (size_t i = 0; i < n;) {
+                const unsigned len = byte();
+                if (len == 128) continue;
+                if (len < 128) {
+                    if (len + 1 > n - i) throw std::runtime_error("corrupt PSD run");
+                    for (unsigned k = 0; k <= len; k++, i++, p += 4) *p = (unsigned char)byte();
+                } else {
+                    const unsigned cnt = 257 - len;
+                    if (cnt > n - i) throw std::runtime_error("corrupt PSD run");
+                    const unsigned char v = (unsigned char)byte();
+                    for (unsigned k = 0; k < cnt; k++, i++, p += 4) *p = v;
+                }
+            }
+        } else if (depth == 16) {
+            for (size_t i = 0; i < n; i++, p += 4) {
+                const unsigned hi = byte();
+                byte();
+                *p = (unsigned char)hi;
+            }
+        } else {
+            for (size_t i = 0; i < n; i++, p += 4) *p = (unsigned char)byte();
+        }
+    }
+    if (channels >= 4)
+        for (size_t i = 0; i < n; i++) {
+            unsigned char *px = out + 4 * i;
+            if (px[3] != 0 && px[3] != 255) {
+                const float a = px[3] / 255.0f, ra = 1.0f / a, inv_a = 255.0f * (1 - ra);
+                for (int c = 0; c < 3; c++) px[c] = (unsigned char)int(px[c] * ra + inv_a);
+            }
         }
     return img;
 }

@@ -4,8 +4,10 @@
 // bytes in different decoders (IDCT arithmetic, chroma upsampling, colour rounding): this one uses a
 // separable floating-point IDCT, the triangle ("fancy") filter for 2x horizontal and vertical
 // chroma upsampling (replication for other factors) and the JFIF YCbCr->RGB equations, which keeps
-// it within a few levels of other decoders.  Progressive and arithmetic-coded files, 12-bit
-// samples and 4-component (CMYK) images are refused with a reason.
+// it within a few levels of other decoders.  Progressive files (T.81 Annex G: spectral selection
+// and successive approximation, Huffman coded) keep every block's coefficients across their scans
+// and are transformed after the last one.  Arithmetic-coded and lossless files, 12-bit samples and
+// 4-component (CMYK) images are refused with a reason.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -47,6 +49,7 @@ struct Component {
     int id, h, v, tq, td = 0, ta = 0;
     int bw, bh;  // blocks per line / column (covering whole MCUs)
     std::vector<unsigned char> plane;  // bw*8 x bh*8 samples
+    std::vector<int> coef;             // progressive: bw*bh blocks of 64 coefficients, zig-zag order
     int pred = 0;
 };
 
@@ -144,13 +147,116 @@ void idct8x8(const float *coef, unsigned char *out, int stride) {
 
 }  // namespace
 
+// One progressive scan (T.81 G.1.2): spectral band ss..se, successive approximation ah -> al.  DC
+// scans may interleave components (MCU order); AC scans hold one component and walk its blocks.
+void progressive_scan(BitReader &br, const std::vector<Component *> &sc, const Huffman *dc, const Huffman *ac, int ss,
+                      int se, int ah, int al, int restart, int width, int height, int hmax, int vmax) {
+    if (ss > se || se > 63 || (ss == 0 && se != 0) || (ss > 0 && sc.size() != 1) || al > 13)
+        throw std::runtime_error("corrupt JPEG progressive scan");
+    int eobrun = 0;
+    const int p1 = 1 << al, m1 = -(1 << al);
+    auto refine = [&](int &z) {  // one correction bit of an already non-zero coefficient
+        if (br.bit() && (z & p1) == 0) z += z >= 0 ? p1 : m1;
+    };
+    auto block = [&](Component &c, int bx, int by) {
+        int *z = &c.coef[(size_t(by) * c.bw + bx) * 64];
+        if (ss == 0) {  // DC
+            if (ah == 0) {
+                c.pred += receive_extend(br, decode_symbol(br, dc[c.td]));
+                z[0] = c.pred * (1 << al);
+            } else if (br.bit()) {
+                z[0] |= p1;
+            }
+            return;
+        }
+        if (ah == 0) {  // AC, first pass of the band
+            if (eobrun > 0) {
+                eobrun--;
+                return;
+            }
+            for (int k = ss; k <= se; k++) {
+                const int rs = decode_symbol(br, ac[c.ta]), r = rs >> 4, s = rs & 15;
+                if (s == 0) {
+                    if (r < 15) {
+                        eobrun = (1 << r) - 1 + (r ? br.bits(r) : 0);
+                        break;
+                    }
+                    k += 15;
+                    continue;
+                }
+                k += r;
+                if (k > se) throw std::runtime_error("corrupt JPEG block");
+                z[k] = receive_extend(br, s) * (1 << al);
+            }
+            return;
+        }
+        int k = ss;  // AC refinement
+        if (eobrun == 0) {
+            for (; k <= se; k++) {
+                const int rs = decode_symbol(br, ac[c.ta]);
+                int r = rs >> 4, value = 0;
+                const int s = rs & 15;
+                if (s) {
+                    if (s != 1) throw std::runtime_error("corrupt JPEG refinement");
+                    value = br.bit() ? p1 : m1;
+                } else if (r != 15) {
+                    eobrun = (1 << r) + (r ? br.bits(r) : 0);
+                    break;
+                }
+                for (; k <= se; k++) {  // pass r zero-history coefficients, refining the others
+                    if (z[k] != 0) {
+                        refine(z[k]);
+                    } else {
+                        if (r == 0) {
+                            if (value) z[k] = value;
+                            break;
+                        }
+                        r--;
+                    }
+                }
+            }
+        }
+        if (eobrun > 0) {
+            for (; k <= se; k++)
+                if (z[k] != 0) refine(z[k]);
+            eobrun--;
+        }
+    };
+    int mcux, mcus;
+    if (sc.size() == 1) {  // non-interleaved: blocks of the component's own (unpadded) extent
+        const Component &c = *sc[0];
+        const int cw = (width * c.h + hmax - 1) / hmax, ch = (height * c.v + vmax - 1) / vmax;
+        mcux = (cw + 7) / 8;
+        mcus = mcux * ((ch + 7) / 8);
+    } else {
+        mcux = (width + 8 * hmax - 1) / (8 * hmax);
+        mcus = mcux * ((height + 8 * vmax - 1) / (8 * vmax));
+    }
+    for (auto *c : sc) c->pred = 0;
+    for (int n = 0; n < mcus; n++) {
+        if (restart && n && n % restart == 0) {
+            br.restart();
+            for (auto *c : sc) c->pred = 0;
+            eobrun = 0;
+        }
+        const int mx = n % mcux, my = n / mcux;
+        if (sc.size() == 1) {
+            block(*sc[0], mx, my);
+        } else {
+            for (auto *c : sc)
+                for (int v = 0; v < c->v; v++)
+                    for (int h = 0; h < c->h; h++) block(*c, mx * c->h + h, my * c->v + v);
+        }
+    }
+}
+
 InputImage decode_jpeg(const std::vector<unsigned char> &f) {
     if (f.size() < 4 || f[0] != 0xFF || f[1] != 0xD8) throw std::runtime_error("not a JPEG file");
     uint16_t qt[4][64] = {};
     Huffman dc[4], ac[4];
     std::vector<Component> comps;
     int width = 0, height = 0, restart = 0, hmax = 1, vmax = 1;
-    bool have_frame = false, done = false;
+    bool have_frame = false, done = false, progressive = false;
     size_t pos = 2;
     auto seg_len = [&](size_t p) -> size_t {
         if (p + 2 > f.size()) throw std::runtime_error("truncated JPEG");
@@ -187,7 +293,8 @@ InputImage decode_jpeg(const std::vector<unsigned char> &f) {
                 (tc ? ac : dc)[th].build(&f[p + 1], &f[p + 17], n);
                 p += 17 + n;
             }
-        } else if (m == 0xC0 || m == 0xC1) {  // baseline / extended sequential, Huffman
+        } else if (m == 0xC0 || m == 0xC1 || m == 0xC2) {  // baseline / extended sequential / progressive, Huffman
+            progressive = m == 0xC2;
             if (len < 8 || f[p0] != 8) throw std::runtime_error("only 8-bit JPEG samples are supported");
             height = f[p0 + 1] << 8 | f[p0 + 2];
             width = f[p0 + 3] << 8 | f[p0 + 4];
@@ -210,10 +317,11 @@ InputImage decode_jpeg(const std::vector<unsigned char> &f) {
                 c.bw = mcux * c.h;
                 c.bh = mcuy * c.v;
                 c.plane.assign(size_t(c.bw) * 8 * c.bh * 8, 0);
+                if (progressive) c.coef.assign(size_t(c.bw) * c.bh * 64, 0);
             }
             have_frame = true;
-        } else if (m >= 0xC2 && m <= 0xCF && m != 0xC4 && m != 0xC8 && m != 0xCC) {
-            throw std::runtime_error("progressive, lossless or arithmetic-coded JPEG is not supported");
+        } else if (m >= 0xC3 && m <= 0xCF && m != 0xC4 && m != 0xC8 && m != 0xCC) {
+            throw std::runtime_error("lossless or arithmetic-coded JPEG is not supported");
         } else if (m == 0xDD) {
             restart = f[p0] << 8 | f[p0 + 1];
         } else if (m == 0xDA) {  // start of scan: entropy-coded data follows the header
@@ -232,6 +340,14 @@ InputImage decode_jpeg(const std::vector<unsigned char> &f) {
                 sc.push_back(c);
             }
             BitReader br(f, end);
+            if (progressive) {
+                const size_t q = p0 + 1 + 2 * size_t(ns);
+                if (q + 3 > end) throw std::runtime_error("truncated JPEG");
+                progressive_scan(br, sc, dc, ac, f[q], f[q + 1], f[q + 2] >> 4, f[q + 2] & 15, restart, width,
+                                 height, hmax, vmax);
+                pos = br.pos();
+                continue;
+            }
             float coef[64];
             auto block = [&](Component &c, int bx, int by) {
                 std::fill(coef, coef + 64, 0.f);
@@ -284,6 +400,17 @@ InputImage decode_jpeg(const std::vector<unsigned char> &f) {
         pos = end;
     }
     if (!have_frame) throw std::runtime_error("JPEG has no frame");
+    if (progressive)  // dequantise with the tables in force at the end, transform every block
+        for (auto &c : comps) {
+            float coef[64];
+            const int stride = c.bw * 8;
+            for (int by = 0; by < c.bh; by++)
+                for (int bx = 0; bx < c.bw; bx++) {
+                    const int *z = &c.coef[(size_t(by) * c.bw + bx) * 64];
+                    for (int k = 0; k < 64; k++) coef[kZigzag[k]] = float(z[k] * qt[c.tq][k]);
+                    idct8x8(coef, &c.plane[size_t(by) * 8 * stride + size_t(bx) * 8], stride);
+                }
+        }
     InputImage img;
     img.width = width;
     img.height = height;

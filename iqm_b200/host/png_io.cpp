@@ -210,6 +210,13 @@ InputImage load_image(const std::string &path) {
         if (f.size() >= 2 && f[0] == 'P' && (f[1] == '5' || f[1] == '6')) return decode_pnm(f);
         if (f.size() >= 2 && f[0] == 'B' && f[1] == 'M') return decode_bmp(f);
         if (f.size() >= 3 && f[0] == 0xFF && f[1] == 0xD8 && f[2] == 0xFF) return decode_jpeg(f);
+        auto starts = [&](const char *sig) {
+            const size_t k = std::strlen(sig);
+            return f.size() >= k && std::memcmp(f.data(), sig, k) == 0;
+        };
+        if (starts("GIF87a") || starts("GIF89a")) return decode_gif(f);
+        if (starts("8BPS")) return decode_psd(f);
+        if (starts("#?RADIANCE\n") || starts("#?RGBE\n")) return decode_hdr(f);
         // TGA has no signature: like the reference's loader, try it when nothing else matched
         try {
             return decode_tga(f);

@@ -137,12 +137,36 @@ def test_jpeg_grey_and_restart_intervals(png_check, tmp_path):
         assert np.abs(got - want).max() <= 4
 
 
-def test_progressive_jpeg_is_refused(png_check, tmp_path):
+@pytest.mark.parametrize("subsampling", [0, 2])
+@pytest.mark.parametrize("size", [(48, 64), (37, 53), (130, 97)])
+def test_progressive_jpeg_close_to_baseline_decode(png_check, tmp_path, subsampling, size):
+    """Progressive JPEG (spectral selection and successive approximation scans): the coefficients
+    of all scans are the baseline file's, so the decode matches PIL's within the same few levels,
+    and the progressive and baseline encodings of one image decode to the same bytes here."""
     from PIL import Image
-    path = str(tmp_path / "p.jpg")
-    Image.fromarray(np.zeros((16, 16, 3), np.uint8)).save(path, progressive=True)
-    r = subprocess.run([png_check, path], capture_output=True, text=True)
-    assert r.returncode != 0 and "progressive" in r.stderr
+    from iqm_b200 import synth
+    h, w = size
+    a, _ = synth.rgb_gain_pair(h, w, config=1, pair=3)
+    prog, base = str(tmp_path / "p.jpg"), str(tmp_path / "b.jpg")
+    Image.fromarray(a[..., :3]).save(prog, quality=88, subsampling=subsampling, progressive=True)
+    Image.fromarray(a[..., :3]).save(base, quality=88, subsampling=subsampling, optimize=True)
+    assert open(prog, "rb").read().find(b"\xff\xc2") > 0
+    got = decode(png_check, prog)
+    want = np.asarray(Image.open(prog).convert("RGB")).astype(int)
+    d = np.abs(got[..., :3].astype(int) - want)
+    assert d.max() <= 4 and d.mean() <= 0.6, (d.max(), d.mean())
+    assert np.array_equal(got, decode(png_check, base))
+
+
+def test_progressive_grey_jpeg_with_restarts(png_check, tmp_path):
+    from PIL import Image
+    from iqm_b200 import synth
+    a, _ = synth.grey_pair(61, 90, config=0, pair=4)
+    path = str(tmp_path / "pg.jpg")
+    Image.fromarray(a[..., 0]).save(path, quality=80, progressive=True, restart_marker_blocks=2)
+    got = decode(png_check, path)[..., :3].astype(int)
+    want = np.asarray(Image.open(path).convert("RGB")).astype(int)
+    assert np.abs(got - want).max() <= 4
 
 
 def test_unknown_image_type_is_rejected(png_check, tmp_path):
@@ -238,3 +262,213 @@ def test_cli_batch_list_errors(cli, tmp_path):
     # CW-SSIM stays a no-op in batch mode (no device needed)
     r = subprocess.run([cli, "--method", "CW_SSIM_CPU", "--batch", str(ok)], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout == ""
+
+
+# ---- GIF, Radiance HDR and PSD, decoded as stbi_load(..., 4) decodes them ----------------------------
+
+def _lzw_literal_stream(indices, min_size):
+    """GIF LZW data that codes every pixel as a literal, with a clear code before the table would
+    widen the codes (a valid stream any decoder must read)."""
+    clear, end, size = 1 << min_size, (1 << min_size) + 1, min_size + 1
+    codes, since = [clear], 0
+    for v in indices:
+        if since == (1 << size) - (clear + 2) - 1:
+            codes.append(clear)
+            since = 0
+        codes.append(int(v))
+        since += 1
+    codes.append(end)
+    acc, nbits, out = 0, 0, bytearray()
+    for c in codes:
+        acc |= c << nbits
+        nbits += size
+        while nbits >= 8:
+            out.append(acc & 255)
+            acc >>= 8
+            nbits -= 8
+    if nbits:
+        out.append(acc & 255)
+    blocks = bytearray([min_size])
+    for i in range(0, len(out), 255):
+        chunk = out[i:i + 255]
+        blocks += bytes([len(chunk)]) + chunk
+    return bytes(blocks + b"\x00")
+
+
+def _gif(screen_w, screen_h, palette, bg, frame, x0=0, y0=0, transparent=None):
+    import struct as st
+    n = len(palette)
+    bits = max(1, (n - 1).bit_length())
+    pal = bytes(c for rgb in palette for c in rgb) + bytes(3 * ((1 << bits) - n))
+    out = b"GIF89a" + st.pack("<HHBBB", screen_w, screen_h, 0x80 | (bits - 1), bg, 0) + pal
+    if transparent is not None:
+        out += b"\x21\xf9\x04" + bytes([1, 0, 0, transparent, 0])
+    fh, fw = frame.shape
+    out += b"\x2c" + st.pack("<HHHHB", x0, y0, fw, fh, 0)
+    out += _lzw_literal_stream(frame.ravel(), max(2, bits)) + b"\x3b"
+    return out
+
+
+def test_gif_decoder_matches_palette(png_check, tmp_path):
+    from PIL import Image
+    rng = np.random.default_rng(4)
+    idx = rng.integers(0, 16, (23, 37)).astype(np.uint8)
+    pal = rng.integers(0, 256, (16, 3)).astype(np.uint8)
+    want = np.concatenate([pal[idx], np.full(idx.shape + (1,), 255, np.uint8)], -1)
+    for name, kw in (("flat", {"interlace": False}), ("interlaced", {"interlace": True})):
+        im = Image.fromarray(idx, "P")
+        im.putpalette(pal.ravel().tolist())
+        path = str(tmp_path / (name + ".gif"))
+        im.save(path, **kw)
+        assert np.array_equal(decode(png_check, path), want), name
+
+
+def test_gif_transparency_and_background(png_check, tmp_path):
+    rng = np.random.default_rng(5)
+    pal = [tuple(int(v) for v in rng.integers(0, 256, 3)) for _ in range(8)]
+    frame = rng.integers(0, 8, (5, 6)).astype(np.uint8)
+    frame[0, 0] = frame[2, 3] = 6
+    path = str(tmp_path / "t.gif")
+    open(path, "wb").write(_gif(11, 9, pal, 2, frame, x0=3, y0=2, transparent=6))
+    got = decode(png_check, path)
+    want = np.zeros((9, 11, 4), np.uint8)
+    r, g, b = pal[2]
+    want[...] = (b, g, r, 255)  # pixels outside the frame: the background entry in B, G, R order
+    for y in range(5):
+        for x in range(6):
+            v = frame[y, x]
+            want[2 + y, 3 + x] = (0, 0, 0, 0) if v == 6 else pal[v] + (255,)
+    assert np.array_equal(got, want)
+
+
+def _hdr_expected(rgbe):
+    m = rgbe[..., :3].astype(np.float32)
+    e = rgbe[..., 3].astype(np.int32)
+    scale = np.where(e > 0, np.ldexp(np.float32(1), e - 136).astype(np.float32), np.float32(0))
+    v = (m * scale[..., None]).astype(np.float32)
+    p = np.power(v.astype(np.float64), np.float64(np.float32(1) / np.float32(2.2))).astype(np.float32)
+    z = p * np.float32(255) + np.float32(0.5)
+    z = np.clip(z, 0, 255)
+    out = np.empty(rgbe.shape[:2] + (4,), np.uint8)
+    out[..., :3] = z.astype(np.int32).astype(np.uint8)
+    out[..., 3] = 255
+    return out
+
+
+def _hdr_rle_scanline(sl):
+    out = bytearray([2, 2, sl.shape[0] >> 8, sl.shape[0] & 255])
+    for k in range(4):
+        comp = sl[:, k].tolist()
+        i = 0
+        while i < len(comp):
+            j = i
+            while j < len(comp) and j - i < 127 and comp[j] == comp[i]:
+                j += 1
+            if j - i >= 3:
+                out += bytes([128 + j - i, comp[i]])
+                i = j
+            else:
+                lit = comp[i:i + min(128, len(comp) - i)]
+                out += bytes([len(lit)]) + bytes(lit)
+                i += len(lit)
+    return bytes(out)
+
+
+@pytest.mark.parametrize("w,rle", [(5, False), (40, True), (40, False)])
+def test_hdr_decoder(png_check, tmp_path, w, rle):
+    rng = np.random.default_rng(6)
+    h = 7
+    rgbe = rng.integers(0, 256, (h, w, 4)).astype(np.uint8)
+    rgbe[..., 0] |= 0x80  # a valid pixel has one mantissa >= 128, so a flat scanline never looks run-length coded
+    rgbe[:, :w // 3, :] = rgbe[:, :1, :]  # runs
+    rgbe[1, 2, 3] = 0  # zero exponent
+    body = b"".join(_hdr_rle_scanline(rgbe[y]) for y in range(h)) if rle else rgbe.tobytes()
+    path = str(tmp_path / "x.hdr")
+    open(path, "wb").write(b"#?RADIANCE\n# made by a test\nFORMAT=32-bit_rle_rgbe\n\n-Y %d +X %d\n" % (h, w) + body)
+    assert np.array_equal(decode(png_check, path), _hdr_expected(rgbe))
+
+
+def test_hdr_written_by_opencv(png_check, tmp_path):
+    import cv2
+    rng = np.random.default_rng(7)
+    img = (rng.random((12, 33, 3)) * 4).astype(np.float32)
+    path = str(tmp_path / "cv.hdr")
+    assert cv2.imwrite(path, img)
+    got = decode(png_check, path)
+    back = cv2.imread(path, cv2.IMREAD_UNCHANGED)[..., ::-1].astype(np.float32)  # OpenCV's RGBE decode
+    p = np.power(back.astype(np.float64), np.float64(np.float32(1) / np.float32(2.2))).astype(np.float32)
+    want = np.clip(p * np.float32(255) + np.float32(0.5), 0, 255).astype(np.int32)
+    assert got.shape == (12, 33, 4) and (got[..., 3] == 255).all()
+    assert np.abs(got[..., :3].astype(int) - want).max() <= 1
+
+
+def _packbits(row):
+    out, i = bytearray(), 0
+    while i < len(row):
+        j = i
+        while j < len(row) and j - i < 128 and row[j] == row[i]:
+            j += 1
+        if j - i >= 2:
+            out += bytes([257 - (j - i), row[i]])
+            i = j
+        else:
+            lit = row[i:i + min(128, len(row) - i)]
+            out += bytes([len(lit) - 1]) + bytes(lit)
+            i += len(lit)
+    return bytes(out)
+
+
+def _psd(planes, depth, rle):
+    import struct as st
+    c, h, w = planes.shape
+    out = b"8BPS" + st.pack(">H6xHIIHH", 1, c, h, w, depth, 3) + st.pack(">III", 0, 0, 0)  # empty sections
+    if not rle:
+        data = planes.astype(">u2").tobytes() if depth == 16 else planes.astype(np.uint8).tobytes()
+        return out + st.pack(">H", 0) + data
+    chunks = [_packbits(planes[k].ravel().tolist()) for k in range(c)]
+    counts = st.pack(">%dH" % (c * h), *([0] * (c * h)))
+    return out + st.pack(">H", 1) + counts + b"".join(chunks)
+
+
+def _unpremultiply(px):
+    out = px.copy()
+    a = px[..., 3]
+    m = (a != 0) & (a != 255)
+    af = a.astype(np.float32) / np.float32(255)
+    ra = np.float32(1) / np.where(m, af, np.float32(1))
+    inv = np.float32(255) * (np.float32(1) - ra)
+    for c in range(3):
+        v = px[..., c].astype(np.float32) * ra + inv
+        out[..., c] = np.where(m, (np.trunc(v).astype(np.int64) & 255).astype(np.uint8), px[..., c])
+    return out
+
+
+@pytest.mark.parametrize("channels,depth,rle", [(3, 8, False), (3, 8, True), (4, 8, False), (4, 8, True),
+                                                (3, 16, False), (5, 16, False)])
+def test_psd_decoder(png_check, tmp_path, channels, depth, rle):
+    rng = np.random.default_rng(8)
+    h, w = 9, 14
+    planes = rng.integers(0, 1 << depth, (channels, h, w)).astype(np.uint32)
+    planes[:, :, :5] = planes[:, :, :1]  # runs
+    if channels >= 4:
+        planes[3, 0, 0], planes[3, 1, 1] = 0, (1 << depth) - 1
+    path = str(tmp_path / "x.psd")
+    open(path, "wb").write(_psd(planes, depth, rle))
+    hi = (planes >> 8) if depth == 16 else planes
+    want = np.zeros((h, w, 4), np.uint8)
+    want[..., 3] = 255
+    for k in range(min(channels, 4)):
+        want[..., k] = hi[k]
+    if channels >= 4:
+        want = _unpremultiply(want)
+    assert np.array_equal(decode(png_check, path), want)
+    if channels == 3 and depth == 8 and not rle:
+        assert np.array_equal(decode(png_check, path), pil_rgba(path))
+
+
+def test_psd_non_rgb_is_refused(png_check, tmp_path):
+    import struct as st
+    path = str(tmp_path / "g.psd")
+    open(path, "wb").write(b"8BPS" + st.pack(">H6xHIIHH", 1, 1, 2, 2, 8, 1) + b"\x00" * 14 + b"\x00" * 4)
+    r = subprocess.run([png_check, path], capture_output=True, text=True)
+    assert r.returncode != 0 and "RGB" in r.stderr
