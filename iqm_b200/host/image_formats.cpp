@@ -1,13 +1,14 @@
-// BMP, TGA, GIF, Radiance HDR and Photoshop PSD input for the command line, written from the
-// formats' specifications (Microsoft's BITMAPINFOHEADER family; Truevision TGA 2.0; GIF89a; the
-// Radiance RGBE picture format; Adobe's PSD file format).  Output is RGBA8 like the reference's
+// BMP, TGA, GIF, Radiance HDR, Photoshop PSD and Softimage PIC input for the command line, written
+// from the formats' specifications (Microsoft's BITMAPINFOHEADER family; Truevision TGA 2.0;
+// GIF89a; the Radiance RGBE picture format; Adobe's PSD file format; Softimage's PIC format).  Output is RGBA8 like the reference's
 // stbi_load(..., 4) (src/main.cpp:37-57), including that loader's conversions where a format
 // needs one (see each decoder).  Grey expands to R = G = B, a missing alpha becomes 255.
 // Covered: BMP with 8-bit palettes, 24-bit and 32-bit pixels (BI_RGB, or BI_BITFIELDS with
 // byte-aligned 8-bit masks), bottom-up or top-down rows; TGA types 1, 2, 3 and their run-length
 // forms 9, 10, 11 with 8-, 24- or 32-bit pixels and 24- or 32-bit colour maps, either origin; the
 // first frame of a GIF; HDR with run-length or flat RGBE scanlines; RGB PSD, 8 or 16 bits, raw or
-// PackBits.  Other layouts are refused with a reason.
+// PackBits; PIC with raw, pure or mixed run-length packets of 8-bit channels.  Other layouts are refused with a reason.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
@@ -485,6 +486,80 @@ InputImage decode_psd(const std::vector<unsigned char> &f) {
             if (px[3] != 0 && px[3] != 255) {
                 const float a = px[3] / 255.0f, ra = 1.0f / a, inv_a = 255.0f * (1 - ra);
                 for (int c = 0; c < 3; c++) px[c] = (unsigned char)int(px[c] * ra + inv_a);
+            }
+        }
+    return img;
+}
+
+// Softimage PIC (as stbi_load reads it): a 104-byte header (magic 0x5380F634, "PICT" at byte 88,
+// big-endian width and height at 92 and 94), then a chain of channel packets (chained flag, bits
+// per channel -- 8 only --, coding 0 raw / 1 pure run-length / 2 mixed run-length, and a channel
+// mask R 0x80, G 0x40, B 0x20, A 0x10).  Every row holds each packet's data for that row in chain
+// order; channels no packet carries stay 255.
+InputImage decode_pic(const std::vector<unsigned char> &f) {
+    if (f.size() < 104 || be32(f, 0) != 0x5380F634u || std::memcmp(&f[88], "PICT", 4) != 0)
+        throw std::runtime_error("not a PIC file");
+    const int w = int(be16(f, 92)), h = int(be16(f, 94));
+    check_size(w, h);
+    size_t pos = 104;
+    auto byte = [&]() -> unsigned {
+        if (pos >= f.size()) throw std::runtime_error("truncated");
+        return f[pos++];
+    };
+    struct Packet {
+        unsigned type, mask;
+    };
+    std::vector<Packet> packets;
+    for (bool chained = true; chained;) {
+        if (packets.size() == 10) throw std::runtime_error("too many PIC packets");
+        chained = byte() != 0;
+        const unsigned size = byte(), type = byte(), mask = byte();
+        if (size != 8) throw std::runtime_error("PIC packet is not 8 bits per channel");
+        if (type > 2) throw std::runtime_error("unknown PIC packet coding");
+        packets.push_back({type, mask});
+    }
+    InputImage img;
+    img.width = w;
+    img.height = h;
+    img.data.assign(size_t(w) * h * 4, 255);
+    auto read_value = [&](unsigned mask, unsigned char *dst) {
+        for (int c = 0; c < 4; c++)
+            if (mask & (0x80u >> c)) dst[c] = (unsigned char)byte();
+    };
+    auto copy_value = [](unsigned mask, unsigned char *dst, const unsigned char *src) {
+        for (int c = 0; c < 4; c++)
+            if (mask & (0x80u >> c)) dst[c] = src[c];
+    };
+    for (int y = 0; y < h; y++)
+        for (const Packet &pk : packets) {
+            unsigned char *dst = &img.data[size_t(y) * w * 4];
+            int left = w;
+            if (pk.type == 0) {
+                for (int x = 0; x < w; x++, dst += 4) read_value(pk.mask, dst);
+                continue;
+            }
+            while (left > 0) {
+                unsigned char v[4] = {};
+                int count = int(byte());
+                if (pk.type == 1) {  // a count and one value per run; a run past the row is cut
+                    count = std::min(count, left);
+                    read_value(pk.mask, v);
+                    for (int i = 0; i < count; i++, dst += 4) copy_value(pk.mask, dst, v);
+                } else if (count >= 128) {  // mixed: a repeated run (128: a 16-bit count follows)
+                    if (count == 128) {
+                        count = int(be16(f, pos));
+                        pos += 2;
+                    } else {
+                        count -= 127;
+                    }
+                    if (count > left) throw std::runtime_error("PIC run past the row");
+                    read_value(pk.mask, v);
+                    for (int i = 0; i < count; i++, dst += 4) copy_value(pk.mask, dst, v);
+                } else {  // mixed: count + 1 literal values
+                    if (++count > left) throw std::runtime_error("PIC run past the row");
+                    for (int i = 0; i < count; i++, dst += 4) read_value(pk.mask, dst);
+                }
+                left -= count;
             }
         }
     return img;

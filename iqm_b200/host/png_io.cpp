@@ -217,6 +217,7 @@ InputImage load_image(const std::string &path) {
         if (starts("GIF87a") || starts("GIF89a")) return decode_gif(f);
         if (starts("8BPS")) return decode_psd(f);
         if (starts("#?RADIANCE\n") || starts("#?RGBE\n")) return decode_hdr(f);
+        if (f.size() >= 92 && starts("\x53\x80\xF6\x34") && std::memcmp(&f[88], "PICT", 4) == 0) return decode_pic(f);
         // TGA has no signature: like the reference's loader, try it when nothing else matched
         try {
             return decode_tga(f);

@@ -1,4 +1,4 @@
-// PNG, binary PNM, BMP, TGA, baseline JPEG, GIF, Radiance HDR and RGB PSD input, 8-bit grey / RGB / RGBA PNG output, for the command-line front end.
+// PNG, binary PNM, BMP, TGA, JPEG, GIF, Radiance HDR, RGB PSD and Softimage PIC input, 8-bit grey / RGB / RGBA PNG output, for the command-line front end.
 // Decoding always yields RGBA8 like the reference's stbi_load(..., 4) (src/main.cpp:37-57):
 // grey -> R=G=B, missing alpha -> 255, 16-bit samples -> their high byte, palettes expanded.
 #ifndef IQM_HOST_PNG_IO_H
@@ -26,6 +26,7 @@ InputImage decode_jpeg(const std::vector<unsigned char> &file); // jpeg_decode.c
 InputImage decode_gif(const std::vector<unsigned char> &file);  // image_formats.cpp (first frame)
 InputImage decode_hdr(const std::vector<unsigned char> &file);  // image_formats.cpp (to 8 bits)
 InputImage decode_psd(const std::vector<unsigned char> &file);  // image_formats.cpp (RGB)
+InputImage decode_pic(const std::vector<unsigned char> &file);  // image_formats.cpp (Softimage)
 std::vector<unsigned char> encode_grey_png(int width, int height, const std::vector<unsigned char> &pixels);
 }  // namespace IQM
 

@@ -472,3 +472,58 @@ def test_psd_non_rgb_is_refused(png_check, tmp_path):
     open(path, "wb").write(b"8BPS" + st.pack(">H6xHIIHH", 1, 1, 2, 2, 8, 1) + b"\x00" * 14 + b"\x00" * 4)
     r = subprocess.run([png_check, path], capture_output=True, text=True)
     assert r.returncode != 0 and "RGB" in r.stderr
+
+
+def _pic(w, h, packets, rows):
+    """Softimage PIC: header, packet chain [(coding, mask)], then per row each packet's bytes."""
+    import struct as st
+    head = st.pack(">I", 0x5380F634) + b"\x00" * 84 + b"PICT" + st.pack(">HHIHH", w, h, 0, 0, 0)
+    chain = b"".join(bytes([1 if i + 1 < len(packets) else 0, 8, t, m]) for i, (t, m) in enumerate(packets))
+    return head + chain + b"".join(rows)
+
+
+def _pic_channels(mask):
+    return [c for c in range(4) if mask & (0x80 >> c)]
+
+
+def _pic_encode_row(px, coding, mask):
+    ch = _pic_channels(mask)
+    vals = [bytes(int(px[x, c]) for c in ch) for x in range(px.shape[0])]
+    if coding == 0:
+        return b"".join(vals)
+    out, i = bytearray(), 0
+    while i < len(vals):
+        j = i
+        while j < len(vals) and vals[j] == vals[i] and j - i < (255 if coding == 1 else 300):
+            j += 1
+        n = j - i
+        if coding == 1:
+            out += bytes([n]) + vals[i]
+            i = j
+        elif n >= 2:
+            out += (bytes([128]) + n.to_bytes(2, "big") if n > 128 else bytes([n + 127])) + vals[i]
+            i = j
+        else:
+            k = i
+            while k < len(vals) and k - i < 128 and (k + 1 >= len(vals) or vals[k + 1] != vals[k]):
+                k += 1
+            k = max(k, i + 1)
+            out += bytes([k - i - 1]) + b"".join(vals[i:k])
+            i = k
+    return bytes(out)
+
+
+@pytest.mark.parametrize("codings", [(0,), (1,), (2,), (2, 1)])
+def test_pic_decoder(png_check, tmp_path, codings):
+    rng = np.random.default_rng(9)
+    h, w = 6, 150
+    img = rng.integers(0, 256, (h, w, 4)).astype(np.uint8)
+    img[:, 3:140] = img[:, 3:4]  # a run longer than 128 (a 16-bit count in mixed coding)
+    packets = [(codings[0], 0xE0)] + ([(codings[1], 0x10)] if len(codings) > 1 else [])
+    rows = [b"".join(_pic_encode_row(img[y], t, m) for t, m in packets) for y in range(h)]
+    path = str(tmp_path / "x.pic")
+    open(path, "wb").write(_pic(w, h, packets, rows))
+    want = img.copy()
+    if len(codings) == 1:
+        want[..., 3] = 255  # no packet carries alpha
+    assert np.array_equal(decode(png_check, path), want)
