@@ -771,7 +771,9 @@ struct MmaColGeom {
     static constexpr int SP = 13;
     static constexpr size_t tables = Dft::smem_bytes;
     static constexpr size_t slab_bytes = sizeof(float2) * 2 * MCW * SLAB;
-    static constexpr size_t smem = tables + slab_bytes + sizeof(__half2) * 2 * H * SP;
+    static constexpr int FLD = (H + 3) & ~3;  // per-warp filter column (floats), 16-byte aligned
+    static constexpr size_t stage_bytes = sizeof(__half2) * 2 * H * SP;
+    static constexpr size_t smem = tables + slab_bytes + stage_bytes + sizeof(float) * MCW * FLD;
     static_assert(MCW == 8 && tables % 16 == 0 && slab_bytes % 16 == 0, "16-byte aligned slab and staging");
 };
 
@@ -785,6 +787,8 @@ __global__ void __launch_bounds__(32 * MCW, Dft::P == 1 && !Dft::kRegs ? 3 : 2)
     float2 *Sl = sm + Gm::tables / sizeof(float2);                          // [img][column][SLAB]
     __half2 *stage = reinterpret_cast<__half2 *>(Sl + 2 * MCW * Gm::SLAB);  // [img][y][SP]
     const int warp = threadIdx.x >> 5;
+    // this warp's column of the current filter, read once per scale for both images
+    float *fcol = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(stage) + Gm::stage_bytes) + warp * Gm::FLD;
     Dft dft;
     dft.load(table, sm);  // complete at the item loop's first barrier
     const int ngroups = (g.w2 + MCW - 1) / MCW;
@@ -815,13 +819,15 @@ __global__ void __launch_bounds__(32 * MCW, Dft::P == 1 && !Dft::kRegs ? 3 : 2)
         for (int s = 0; s < 4; s++) {
             if (warp < nc) {  // warp-uniform
                 const float *Hz = g.filters + size_t(o * 4 + s) * g.n + size_t(x0 + warp) * H;
+                for (int i = threadIdx.x & 31; i < H; i += 32) fcol[i] = __ldg(Hz + i);
+                __syncwarp();
 #pragma unroll 1
                 for (int img = 0; img < 2; img++) {
                     const float2 *col = Sl + (img * MCW + warp) * Gm::SLAB;
                     __half2 *st = stage + img * H * Gm::SP + warp;
                     dft.run(
                         [&](int n1, int n2) {
-                            const float h = __ldg(Hz + Dft::N2 * n1 + n2);
+                            const float h = fcol[Dft::N2 * n1 + n2];
                             const float2 v = col[n1 * Gm::SEG + n2];
                             return make_float2(h * v.x, h * v.y);
                         },
