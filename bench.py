@@ -64,8 +64,8 @@ TRAFFIC = {
 # 32 inverse transforms of each of the 480 columns (270 = 15 x 18: 27 m16n8k16 tiles) and of each
 # of the 270 rows (480 = 16 x 30: 48 tiles), 2 * 16 * 8 * 16 = 4096 flops a tile, times the products
 # per tile (3 with split-precision operands, 1 with single FP16 operands).
-# The mixed SSIM forms run one CTA per 64x32 output tile: 4 warps, each with 3 x 16 horizontal and
-# 2 x 16 vertical m16n8k16 tiles (4 moments x 2 n-tiles x 2 k-steps per 16-row block).
+# The mixed SSIM forms run one CTA per 64x64 output tile: 4 warps, each with 5 x 16 horizontal and
+# 4 x 16 vertical m16n8k16 tiles (4 moments x 2 n-tiles x 2 k-steps per 16-row block).
 MMA_PRODUCTS = {"mixed": 3, "mixed_fast": 1}
 
 
@@ -75,7 +75,7 @@ def mma_tiles_per_pair(kernel, w, h):
     if kernel == "fsim_inv_rows_mma_kernel":
         return 32 * 270 * 48
     if kernel == "ssim_mma_kernel":
-        return -(-w // 64) * -(-h // 32) * 4 * (48 + 32)
+        return -(-w // 64) * -(-h // 64) * 4 * (80 + 64)
     return 0
 
 

@@ -16,34 +16,45 @@
 // B fragments of the vertical product (k = image row, n = column): the horizontal results never
 // leave registers.  The moments enter the horizontal pass from shared memory through ldmatrix.
 //
-// CTA tile: 64 output columns (4 warps x 16) x 32 output rows (two 16-row blocks); the CTA works
-// from image rows y0-8 .. y0+39 and columns x0-8 .. x0+71.  The kernel is persistent: each CTA walks
-// the tiles blockIdx.x, blockIdx.x + gridDim.x, ...  Per tile: load the RGBA8 rows and stage them
-// as FP16 moment planes (one barrier), then each warp runs
-// its three 16-row horizontal blocks and two vertical blocks (a rolled loop, so the code stays in
+// CTA tile: 64 output columns (4 warps x 16) x 64 output rows (four 16-row blocks); the CTA works
+// from image rows y0-8 .. y0+71 and columns x0-8 .. x0+71 (1.56 staged pixels per output pixel).
+// The kernel is persistent: each CTA walks the tiles blockIdx.x, blockIdx.x + gridDim.x, ...  Per
+// tile: load the RGBA8 rows and stage them as FP16 moment planes (one barrier), then each warp runs
+// its five 16-row horizontal blocks and four vertical blocks in a rolled loop (the code stays in
 // the instruction cache).  The moments are taken about the tile's centre pixel (u, v) and scaled
 // by 2^12 (largest staged magnitude 4 * 2^12, well inside FP16's range, and small values stay clear
-// of FP16's subnormals).
+// of FP16's subnormals).  Measured against 64x32 tiles, the taller tile stages a third fewer pixels
+// per output and runs 1.35x faster despite one CTA fewer per SM; taller or wider tiles were slower
+// (96 or 128 rows) or took the single-product form past its bound (128 columns).
 //
 // IQM_MIXED stages every moment as an FP16 hi + lo pair and forms each product as
 // A_hi B_hi + A_hi B_lo + A_lo B_hi (about 21 significant bits, MSSIM within ~1e-6 of FP64);
-// IQM_MIXED_FAST uses the hi parts alone (11-bit moments and taps: MSSIM within ~5e-5 of FP64 on
-// large natural and ramp images, up to ~1.1e-4 on small ones where fewer pixels average the
-// rounding; the 32-row shift tile keeps the second moments' cancellation small).  The per-pixel weight
-// normalisation uses the window as the tensor cores see it (FP16-rounded taps in the fast form).
+// IQM_MIXED_FAST uses the hi parts alone (11-bit moments and taps: MSSIM within a few 1e-5 of FP64
+// on large images, tested to 2e-4; the error grows with how far a tile's pixels lie from its
+// centre pixel, which bounds the tile's size).  The per-pixel weight normalisation uses the window
+// as the tensor cores see it (FP16-rounded taps in the fast form).
 #pragma once
 
 #include "dft_mma.cuh"
 
+#ifndef SSIM_MT_W
+#define SSIM_MT_W 64
+#endif
+#ifndef SSIM_MT_H
+#define SSIM_MT_H 64
+#endif
+
 namespace {
 
-constexpr int MT_W = 64;              // output columns per CTA tile
-constexpr int MT_H = 32;              // output rows per CTA tile
-constexpr int MT_THREADS = 128;       // 4 warps, 16 output columns each
-constexpr int MT_ROWS = MT_H + 16;    // staged rows y0-8 .. y0+39 (three 16-row horizontal blocks)
-constexpr int MT_SCOLS = MT_W + 16;   // staged columns x0-8 .. x0+71
-constexpr int MT_LD = 88;             // FP16 row stride of a staged plane: 176 bytes, so the 8 rows
-                                      // of one ldmatrix 8x8 load fall in distinct 16-byte bank groups
+constexpr int MT_W = SSIM_MT_W;       // output columns per CTA tile
+constexpr int MT_H = SSIM_MT_H;       // output rows per CTA tile (a multiple of 16)
+constexpr int MT_THREADS = 2 * MT_W;  // one warp per 16 output columns
+constexpr int MT_ROWS = MT_H + 16;    // staged rows y0-8 .. y0+MT_H+7 (MT_H/16 + 1 horizontal blocks)
+constexpr int MT_SCOLS = MT_W + 16;   // staged columns x0-8 .. x0+MT_W+7
+constexpr int MT_LD = MT_SCOLS + 8;   // FP16 row stride of a staged plane: 48 mod 128 bytes, so the 8
+                                      // rows of one ldmatrix 8x8 load fall in distinct 16-byte groups
+static_assert((2 * MT_LD) % 128 == 48, "ldmatrix rows must fall in distinct bank groups");
+constexpr int MT_MIN_CTAS_SINGLE = 512 / MT_THREADS, MT_MIN_CTAS_SPLIT = 384 / MT_THREADS > 0 ? 384 / MT_THREADS : 1;
 constexpr float MT_SCALE = 4096.f;    // staged moments are scaled by 2^12
 
 struct SsimMmaArgs {
@@ -94,9 +105,9 @@ __device__ __forceinline__ float2 luma2(uint32_t pa, uint32_t pb) {
 
 // Stage the tile's moment planes: staged row r = image row y0 - 8 + r, staged column q = image column
 // x0 - 8 + q; positions outside the image hold zero in every plane (they drop out of the sums).
-// The thread's loads are issued in two rounds of four 4-pixel chunks (eight 16-byte loads in
-// flight per thread) ahead of their conversion: two memory round trips per tile, with the code of
-// one round only.  (Prefetching the next tile into shared memory instead hides the round trips but
+// The thread's loads are issued in two rounds of up to seven 4-pixel chunks (fourteen 16-byte loads
+// in flight per thread) ahead of their conversion: two memory round trips per tile, with the code
+// of one round only.  (Prefetching the next tile into shared memory instead hides the round trips but
 // costs a CTA per SM, which measured slower.)
 template <int SPLIT>
 __device__ __forceinline__ void stage_moments(__half *pl, const SsimPairDev &P, int x0, int y0, float cu, float cv) {
@@ -269,7 +280,7 @@ __device__ __forceinline__ float ssim_px(float2 m1, float2 m2, float inv, float 
 // at the same time, so the rows they share meet in L2), keeping the band fragments and a warm
 // instruction cache across tiles.
 template <int SPLIT>
-__global__ void __launch_bounds__(MT_THREADS, SPLIT == 1 ? 4 : 3) ssim_mma_kernel(SsimMmaArgs args, int total_tiles) {
+__global__ void __launch_bounds__(MT_THREADS, SPLIT == 1 ? MT_MIN_CTAS_SINGLE : MT_MIN_CTAS_SPLIT) ssim_mma_kernel(SsimMmaArgs args, int total_tiles) {
     extern __shared__ __align__(16) unsigned char ssim_mma_smem[];
     __half *pl = reinterpret_cast<__half *>(ssim_mma_smem);
     __shared__ double red[MT_THREADS / 32];
@@ -355,7 +366,7 @@ __global__ void __launch_bounds__(MT_THREADS, SPLIT == 1 ? 4 : 3) ssim_mma_kerne
         float acc = 0.f;
         unsigned hph[4][2][2], hpl[4][2][2], hnh[4][2][2], hnl[4][2][2];
 #pragma unroll 1
-        for (int hb = 0; hb < 3; hb++) {
+        for (int hb = 0; hb < MT_ROWS / 16; hb++) {
             hpass<SPLIT>(pl, hb, warp, ah, al, hnh, hnl);
             if (hb > 0) {
                 // output rows y0 + 16 (hb - 1) + 0..15 from the window of blocks hb - 1 and hb
