@@ -15,6 +15,7 @@ pairs, no collective on the data path): weak scaling; with --batch the 256 pairs
 longest-processing-time first over the ranks: strong scaling.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -617,6 +618,22 @@ def main():
             tens[k] = {"achieved": achieved_t, "peak": tensor_peak, "unit": "TFLOP/s", "frac": achieved_t / tensor_peak,
                        "flops_per_launch": flops, "peak_source": tensor_note + " dense bf16 (burst)"}
         roof["tensor"] = tens
+    if metric == "flip":
+        # FLIP is bound by FP32 arithmetic: the SIMT fraction of its filter taps.  Per pixel pair:
+        # the CSF prefilter, 3 channels x 2 images x (horizontal + vertical) taps of 2 rc + 1, and
+        # the feature filters, per image 3 horizontal (g, edge, point) and 4 vertical outputs of
+        # 2 rf + 1 taps; a multiply-add is 2 flops.  The colour epilogue is not counted.
+        ppd = rt.L.iqm_flip_ppd(ctypes.byref(flip_args.c()))
+        rf = int(np.ceil(np.float32(3.0) * np.float32(0.5 * 0.082) * np.float32(ppd)))
+        rc = int(np.ceil(np.float32(3.0) * np.sqrt(np.float32(0.04) / np.float32(2.0 * np.pi ** 2)) * np.float32(ppd)))
+        flops_px = 2 * (12 * (2 * rc + 1) + 14 * (2 * rf + 1))
+        sm_max = (clk or {}).get("sm_max_mhz") or 1965
+        simt_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
+        simt = flops_px * W * H / (ms_per_step / 1e3 / B) / 1e12
+        roof["simt"] = {"achieved": simt, "peak": simt_peak, "unit": "TFLOP/s", "frac": simt / simt_peak,
+                        "flops_per_pixel": flops_px, "radii": {"feature": rf, "csf": rc},
+                        "scope": "whole step, filter taps only",
+                        "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 2 flops x max SM clock"}
 
     # end to end: host API with pinned host images and host scores
     e2e = None
