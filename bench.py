@@ -284,7 +284,6 @@ def run_batch(args, rank, world, local):
             flush=True)
         return
 
-    import ctypes
     import torch
     import iqm_b200
     from iqm_b200 import parallel
@@ -643,7 +642,6 @@ def main():
         pa = torch.from_numpy(a).pin_memory()
         pb = torch.from_numpy(b).pin_memory()
         pin.append((pa, pb))
-    import ctypes
     items = [(pa.data_ptr(), pb.data_ptr(), W, H, W * 4) for pa, pb in pin]
     arr = iqm_b200._pairs(items)
     out = np.empty(B * nscore, np.float64)
