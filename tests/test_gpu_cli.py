@@ -131,3 +131,18 @@ def test_cli_fsim_precision_and_energy_options(cli, rt, o64, tmp_path):
     out = run(cli, "--method", "FSIM", "--input", pa, "--ref", pb, "FSIM_ENERGY_SUM", "full")
     ff, ffc = o64.fsim(a, b, energy_full=True)
     assert abs(value(out, "FSIM") - ff) <= 2e-6 and abs(value(out, "FSIMc") - ffc) <= 2e-6
+
+
+def test_cli_ssim_precision_option(cli, rt, o64, tmp_path):
+    """--precision reaches SSIM too: the split tensor-core form within 1e-5 of the FP64 oracle, single
+    FP16 products within their 2e-4 bound; the batch mode takes the same option."""
+    a, b = synth.grey_pair(600, 700, config=0, pair=3)
+    pa, pb = save(tmp_path, "a.png", a), save(tmp_path, "b.png", b)
+    want = o64.ssim(a, b)
+    for prec, tol in (("mixed", 1e-5), ("mixed_fast", 2e-4)):
+        out = run(cli, "--method", "SSIM", "--input", pa, "--ref", pb, "--precision", prec)
+        assert abs(value(out, "MSSIM") - want) <= tol
+    lst = tmp_path / "list.txt"
+    lst.write_text("%s %s\n%s %s\n" % (pa, pb, pb, pa))
+    out = run(cli, "--method", "SSIM", "--batch", str(lst), "--precision", "mixed")
+    assert out.count("MSSIM") == 2
