@@ -205,3 +205,44 @@ def test_uneven_256_batch_as_benchmarked_matches_oracle(rt, o64):
     for i in picks:
         f, fc = o64.fsim(*rgb[i])
         assert abs(results["fsim"][2 * i] - f) <= TOL and abs(results["fsim"][2 * i + 1] - fc) <= TOL, (i, sizes[i])
+
+
+@pytest.mark.parametrize("precision,tol", [(iqm_b200.IQM_MIXED, 1e-5), (iqm_b200.IQM_MIXED_FAST, 2e-4)])
+def test_plan_with_mixed_precision_forms(rt, o64, precision, tol):
+    """A batch plan built with the tensor-core forms: SSIM (ssim->precision) and FSIM (the plan's
+    precision) replay the same scores as the per-metric calls of those forms and stay within the
+    forms' bounds of the FP64 oracle (FSIM: 1e-4 for both forms)."""
+    import torch
+    sizes = [(480, 270), (1920, 1080), (333, 121), (97, 211)]
+    pairs = _pairs(sizes, seed_pair=40)
+    bufs, items = _to_device(pairs)
+    mask = iqm_b200.METRIC_SSIM | iqm_b200.METRIC_FSIM
+    d_scores = torch.zeros(iqm_b200.scores_per_pair(mask) * len(pairs), dtype=torch.float64, device="cuda")
+    s = iqm_b200.SSIM(rt)
+    s.precision = precision
+    f = iqm_b200.FSIM(rt)
+    f.precision = precision
+    plan = iqm_b200.BatchPlan(rt, mask, items, d_scores.data_ptr(), ssim=s.params(), precision=precision,
+                              autotune=False)
+    try:
+        plan.run()
+        rt.synchronize()
+        got = iqm_b200._split_scores(mask, len(pairs), d_scores.cpu().numpy())
+    finally:
+        plan.close()
+    assert np.array_equal(got["ssim"], s.compute_batch(pairs))
+    assert np.array_equal(np.asarray(got["fsim"]).reshape(-1, 2), np.asarray(f.compute_batch(pairs)).reshape(-1, 2))
+    for (a, b), gs, gf in zip(pairs, got["ssim"], np.asarray(got["fsim"]).reshape(-1, 2)):
+        assert abs(gs - o64.ssim(a, b)) <= tol
+        assert np.abs(np.asarray(gf) - np.asarray(o64.fsim(a, b))).max() <= 1e-4
+
+
+@pytest.mark.parametrize("precision", [iqm_b200.IQM_FP32, iqm_b200.IQM_MIXED, iqm_b200.IQM_MIXED_FAST])
+@pytest.mark.parametrize("h,w", [(16, 4000), (3000, 13), (11, 70)])
+def test_ssim_extreme_aspect_ratios(rt, o64, precision, h, w):
+    """Thin and wide images: a single tile row or column of the tiled kernels, halos on both sides."""
+    a, b = synth.grey_pair(h, w, config=0, pair=7)
+    s = iqm_b200.SSIM(rt)
+    s.precision = precision
+    tol = {iqm_b200.IQM_FP32: 1e-5, iqm_b200.IQM_MIXED: 1e-5, iqm_b200.IQM_MIXED_FAST: 2e-4}[precision]
+    assert abs(s.compute_metric(a, b, want_map=False).mssim - o64.ssim(a, b)) <= tol
