@@ -37,17 +37,10 @@
 
 #include "dft_mma.cuh"
 
-#ifndef SSIM_MT_W
-#define SSIM_MT_W 64
-#endif
-#ifndef SSIM_MT_H
-#define SSIM_MT_H 64
-#endif
-
 namespace {
 
-constexpr int MT_W = SSIM_MT_W;       // output columns per CTA tile
-constexpr int MT_H = SSIM_MT_H;       // output rows per CTA tile (a multiple of 16)
+constexpr int MT_W = 64;              // output columns per CTA tile (a multiple of 16)
+constexpr int MT_H = 64;              // output rows per CTA tile (a multiple of 16)
 constexpr int MT_THREADS = 2 * MT_W;  // one warp per 16 output columns
 constexpr int MT_ROWS = MT_H + 16;    // staged rows y0-8 .. y0+MT_H+7 (MT_H/16 + 1 horizontal blocks)
 constexpr int MT_SCOLS = MT_W + 16;   // staged columns x0-8 .. x0+MT_W+7
