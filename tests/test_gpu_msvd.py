@@ -65,3 +65,27 @@ def test_msvd_rejects_tiny(rt):
     a = np.zeros((7, 20, 4), np.uint8)
     with pytest.raises(iqm_b200.IQMError):
         iqm_b200.SVD(rt).compute_metric(a, a)
+
+
+def test_msvd_constant_blocks_known_answer(rt, o64):
+    """A block of one grey value v is the rank-1 matrix v 1 1^T: singular values (8 v, 0, ..., 0).
+    Two images of constant blocks a_ij and b_ij therefore have D_ij = 8 |a_ij - b_ij| on every
+    computed block (the last block row and column of a size that is a multiple of 8 are not
+    computed), and the map is D / max D."""
+    nb = 8
+    i, j = np.meshgrid(np.arange(nb), np.arange(nb), indexing="ij")
+    a = 10 + 3 * i + 5 * j
+    b = a + (i * j) % 4 + (i == 2) * 7
+    def image(v):
+        g = np.repeat(np.repeat(v.astype(np.uint8), 8, 0), 8, 1)
+        img = np.repeat(g[..., None], 4, 2)
+        img[..., 3] = 255
+        return np.ascontiguousarray(img)
+    A, B = image(a), image(b)
+    res = iqm_b200.SVD(rt).compute_metric(A, B)
+    d = 8.0 * np.abs(a - b).astype(np.float64)
+    d[nb - 1, :] = 0.0
+    d[:, nb - 1] = 0.0
+    assert np.allclose(res.image_data.reshape(nb, nb), d / d.max(), atol=2e-5)
+    want = o64.msvd(A, B)
+    assert abs(res.msvd - want) <= 1e-5 * max(1.0, abs(want))
