@@ -61,6 +61,7 @@ struct SsimPairDev {
     int tile_base;     // first global tile index of this pair
     int ntiles;
     int vec_ok;        // 16-byte loads allowed
+    int unit_base;     // tensor-core kernel: first global work unit (column segment of tiles)
 };
 
 struct SsimArgs {
@@ -366,16 +367,16 @@ void check_params(const iqm_ssim_params &p) {
 
 // The tensor-core kernel (one 64x32 tile per CTA) for IQM_MIXED (split products) and
 // IQM_MIXED_FAST (single products).
-// Persistent launch: as many CTAs as fit on the device at once (at most one per tile).
+// Persistent launch: as many CTAs as fit on the device at once (at most one per work unit).
 template <int SPLIT>
-void launch_ssim_mma(const SsimMmaArgs &a, int total_tiles, int device, cudaStream_t s) {
+void launch_ssim_mma(const SsimMmaArgs &a, int total_units, int device, cudaStream_t s) {
     const size_t smem = SsimMmaGeom<SPLIT>::smem_bytes;
     IQM_CHECK_CUDA(cudaFuncSetAttribute(ssim_mma_kernel<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int sms = 0, per_sm = 0;
     IQM_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     IQM_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ssim_mma_kernel<SPLIT>, MT_THREADS, smem));
-    const int grid = std::max(1, std::min(total_tiles, sms * std::max(1, per_sm)));
-    ssim_mma_kernel<SPLIT><<<grid, MT_THREADS, smem, s>>>(a, total_tiles);
+    const int grid = std::max(1, std::min(total_units, sms * std::max(1, per_sm)));
+    ssim_mma_kernel<SPLIT><<<grid, MT_THREADS, smem, s>>>(a, total_units);
 }
 
 // Enqueue SSIM for device-resident pairs; `maps[i]` (device, nullable) receive the SSIM maps.
@@ -386,7 +387,8 @@ void ssim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_ss
     const bool mma = p.precision != IQM_FP32;
     const int tw = mma ? MT_W : TW, th = mma ? MT_H : strip_rows(R);
     std::vector<SsimPairDev> hd(n);
-    int total = 0;
+    int total = 0, units = 0;
+    const int segt = p.precision == IQM_MIXED ? MT_SEG_SPLIT : 1;  // tiles per column segment
     for (int i = 0; i < n; i++) {
         const iqm_pair &q = pairs[i];
         SsimPairDev &d = hd[i];
@@ -401,7 +403,9 @@ void ssim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_ss
         d.tile_base = total;
         d.vec_ok = ((reinterpret_cast<uintptr_t>(q.input) | reinterpret_cast<uintptr_t>(q.ref) |
                      uintptr_t(q.row_bytes)) & 15u) == 0;
+        d.unit_base = units;
         total += d.ntiles;
+        units += d.tiles_x * int(iqm::ceil_div(d.ntiles / d.tiles_x, segt));
     }
     auto *d_desc = static_cast<SsimPairDev *>(
         iqm::upload_bytes(ctx, ctx->desc, hd.data(), sizeof(SsimPairDev) * n));
@@ -424,8 +428,8 @@ void ssim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_ss
         for (int k = 0; k < 15; k++) a.gn[k] = float(g64[k] / gsum);
         a.c1 = p.k1 * p.k1;
         a.c2 = p.k2 * p.k2;
-        if (p.precision == IQM_MIXED) launch_ssim_mma<3>(a, total, ctx->device, ctx->stream);
-        else launch_ssim_mma<1>(a, total, ctx->device, ctx->stream);
+        if (p.precision == IQM_MIXED) launch_ssim_mma<3>(a, units, ctx->device, ctx->stream);
+        else launch_ssim_mma<1>(a, units, ctx->device, ctx->stream);
         iqm::check_launch(ctx, "ssim_mma_kernel");
         return;
     }

@@ -23,7 +23,10 @@
 // its five 16-row horizontal blocks and four vertical blocks in a rolled loop (the code stays in
 // the instruction cache).  The moments are taken about the tile's centre pixel (u, v) and scaled
 // by 2^12 (largest staged magnitude 4 * 2^12, well inside FP16's range, and small values stay clear
-// of FP16's subnormals).  Measured against 64x32 tiles, the taller tile stages a third fewer pixels
+// of FP16's subnormals).  The split form walks column segments of four tiles with one shift per
+// segment (its accuracy does not depend on the shift tile): each later tile reuses the previous
+// tile's last horizontal block from registers and stages 64 rows, not 80 (+4% measured).
+// Measured against 64x32 tiles, the taller tile stages a third fewer pixels
 // per output and runs 1.35x faster despite one CTA fewer per SM; taller or wider tiles were slower
 // (96 or 128 rows) or took the single-product form past its bound (128 columns).
 //
@@ -47,8 +50,11 @@ constexpr int MT_SCOLS = MT_W + 16;   // staged columns x0-8 .. x0+MT_W+7
 constexpr int MT_LD = MT_SCOLS + 8;   // FP16 row stride of a staged plane: 48 mod 128 bytes, so the 8
                                       // rows of one ldmatrix 8x8 load fall in distinct 16-byte groups
 static_assert((2 * MT_LD) % 128 == 48, "ldmatrix rows must fall in distinct bank groups");
-constexpr int MT_MIN_CTAS_SINGLE = 512 / MT_THREADS, MT_MIN_CTAS_SPLIT = 384 / MT_THREADS > 0 ? 384 / MT_THREADS : 1;
+// CTAs per SM the launch bounds ask for: shared memory allows 3 (single products, 56 KB a CTA) and
+// 2 (split products, 112 KB); the register budgets follow.
+constexpr int MT_MIN_CTAS_SINGLE = 512 / MT_THREADS, MT_MIN_CTAS_SPLIT = 256 / MT_THREADS > 0 ? 256 / MT_THREADS : 1;
 constexpr float MT_SCALE = 4096.f;    // staged moments are scaled by 2^12
+constexpr int MT_SEG_SPLIT = 4;       // split form: tiles per column segment (one shift per segment)
 
 struct SsimMmaArgs {
     const SsimPairDev *pairs;
@@ -103,19 +109,20 @@ __device__ __forceinline__ float2 luma2(uint32_t pa, uint32_t pb) {
 // of one round only.  (Prefetching the next tile into shared memory instead hides the round trips but
 // costs a CTA per SM, which measured slower.)
 template <int SPLIT>
-__device__ __forceinline__ void stage_moments(__half *pl, const SsimPairDev &P, int x0, int y0, float cu, float cv) {
+__device__ __forceinline__ void stage_moments(__half *pl, const SsimPairDev &P, int x0, int y0, float cu, float cv,
+                                              int row_lo) {
     using G = SsimMmaGeom<SPLIT>;
     constexpr int CH = MT_SCOLS / 4;  // 4-pixel chunks per staged row
-    constexpr int CHUNKS = MT_ROWS * CH;
-    constexpr int PER_T = (CHUNKS + MT_THREADS - 1) / MT_THREADS;
+    constexpr int PER_T = (MT_ROWS * CH + MT_THREADS - 1) / MT_THREADS;
     constexpr int HALF = (PER_T + 1) / 2;
+    const int CHUNKS = (MT_ROWS - row_lo) * CH;  // staged rows row_lo .. MT_ROWS - 1
 #pragma unroll 1
     for (int k0 = 0; k0 < PER_T; k0 += HALF) {
         uint4 ra[HALF], rb[HALF];
 #pragma unroll
         for (int kk = 0; kk < HALF; kk++) {
             const int c = threadIdx.x + (k0 + kk) * MT_THREADS;
-            const int r = c / CH, q = c - r * CH;
+            const int r = row_lo + c / CH, q = c % CH;
             const int y = y0 - 8 + r, x = x0 - 8 + 4 * q;  // x is a multiple of 4: a chunk is all in or all left of 0
             ra[kk] = make_uint4(0u, 0u, 0u, 0u);
             rb[kk] = make_uint4(0u, 0u, 0u, 0u);
@@ -141,7 +148,7 @@ __device__ __forceinline__ void stage_moments(__half *pl, const SsimPairDev &P, 
         for (int kk = 0; kk < HALF; kk++) {
             const int c = threadIdx.x + (k0 + kk) * MT_THREADS;
             if (c >= CHUNKS) break;
-            const int r = c / CH, q = c - r * CH;
+            const int r = row_lo + c / CH, q = c % CH;
             const int y = y0 - 8 + r, x = x0 - 8 + 4 * q;
             const int nv = (y >= 0 && y < P.h && x >= 0) ? min(4, P.w - x) : 0;
             const uint32_t a[4] = {ra[kk].x, ra[kk].y, ra[kk].z, ra[kk].w};
@@ -244,6 +251,16 @@ __device__ __forceinline__ void vpass(const unsigned (&ah)[2][4], const unsigned
     }
 }
 
+// The pair of a work unit (pairs sorted by unit_base).
+__device__ __forceinline__ int find_unit(const SsimPairDev *pairs, int n, int unit) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pairs[mid].unit_base <= unit) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
 // In-image sum of the effective window taps around position x of a line of length n.
 __device__ __forceinline__ float window_sum(const float *w, int R, int x, int n) {
     float s = 0.f;
@@ -273,7 +290,7 @@ __device__ __forceinline__ float ssim_px(float2 m1, float2 m2, float inv, float 
 // at the same time, so the rows they share meet in L2), keeping the band fragments and a warm
 // instruction cache across tiles.
 template <int SPLIT>
-__global__ void __launch_bounds__(MT_THREADS, SPLIT == 1 ? MT_MIN_CTAS_SINGLE : MT_MIN_CTAS_SPLIT) ssim_mma_kernel(SsimMmaArgs args, int total_tiles) {
+__global__ void __launch_bounds__(MT_THREADS, SPLIT == 1 ? MT_MIN_CTAS_SINGLE : MT_MIN_CTAS_SPLIT) ssim_mma_kernel(SsimMmaArgs args, int total_units) {
     extern __shared__ __align__(16) unsigned char ssim_mma_smem[];
     __half *pl = reinterpret_cast<__half *>(ssim_mma_smem);
     __shared__ double red[MT_THREADS / 32];
@@ -321,18 +338,25 @@ __global__ void __launch_bounds__(MT_THREADS, SPLIT == 1 ? MT_MIN_CTAS_SINGLE : 
     for (int k = 0; k <= 2 * R; k++) wsum += weff[k];
     const float inv_in = 1.0f / (wsum * wsum * MT_SCALE);
 
-    for (int gt = blockIdx.x; gt < total_tiles; gt += gridDim.x) {
-        const int pi = find_pair(args.pairs, args.npairs, gt);
+    // A work unit is a column segment of SEGT vertically adjacent tiles of one pair, walked top to
+    // bottom with one shift for the segment: each tile after the first takes its first horizontal
+    // block (image rows y0 - 8 .. y0 + 7) from the previous tile's last one, still in registers, and
+    // stages only the 64 rows below it.
+    constexpr int SEGT = SPLIT == 1 ? 1 : MT_SEG_SPLIT;
+    unsigned hph[4][2][2], hpl[4][2][2], hnh[4][2][2], hnl[4][2][2];
+    for (int unit = blockIdx.x; unit < total_units; unit += gridDim.x) {
+        const int pi = find_unit(args.pairs, args.npairs, unit);
         const SsimPairDev P = args.pairs[pi];
-        const int local = gt - P.tile_base;
-        const int x0 = (local % P.tiles_x) * MT_W;
-        const int y0 = (local / P.tiles_x) * MT_H;
         const int W = P.w, H = P.h;
+        const int local = unit - P.unit_base;
+        const int tx = local % P.tiles_x, ty0 = (local / P.tiles_x) * SEGT;
+        const int ty1 = min(ty0 + SEGT, P.ntiles / P.tiles_x);
+        const int x0 = tx * MT_W;
 
-        // shift constants: u, v of the tile's centre pixel
+        // shift constants: u, v of the segment's centre pixel
         float cu, cv;
         {
-            const int cx = min(x0 + MT_W / 2, W - 1), cy = min(y0 + MT_H / 2, H - 1);
+            const int cx = min(x0 + MT_W / 2, W - 1), cy = min((ty0 + ty1) * MT_H / 2, H - 1);
             const uint32_t pa = __ldg(reinterpret_cast<const uint32_t *>(P.a + (long long)cy * P.pitch) + cx);
             const uint32_t pb = __ldg(reinterpret_cast<const uint32_t *>(P.b + (long long)cy * P.pitch) + cx);
             const float2 l = luma2(pa, pb);
@@ -340,64 +364,70 @@ __global__ void __launch_bounds__(MT_THREADS, SPLIT == 1 ? MT_MIN_CTAS_SINGLE : 
             cv = l.x - l.y;
         }
 
-        // the previous tile's ldmatrix reads ended before the barriers of its pooling
-        stage_moments<SPLIT>(pl, P, x0, y0, cu, cv);
-        __syncthreads();
-
-        // every output pixel in the image, under the full window and pooled
-        const bool interior = x0 >= R && x0 + MT_W - 1 + R <= W - 1 && y0 >= R && y0 + MT_H - 1 + R <= H - 1;
-
-        // normalisation of the lane's rows (g, g + 8 of each output block) and columns (2t, 2t + 1 of
-        // each 8-column half): 1 / (window weight * 2^12), the weight cut at the image border
+        // normalisation of the lane's columns (2t, 2t + 1 of each 8-column half): the window weight
+        // cut at the image border, relative to the interior one
+        const bool interior_x = x0 >= R && x0 + MT_W - 1 + R <= W - 1;
         float rx[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const int x = x0 + 16 * warp + 8 * (j >> 1) + 2 * t + (j & 1);
-            rx[j] = interior ? 1.f : wsum / window_sum(weff, R, x, W);
+            rx[j] = interior_x ? 1.f : wsum / window_sum(weff, R, x, W);
         }
 
-        float acc = 0.f;
-        unsigned hph[4][2][2], hpl[4][2][2], hnh[4][2][2], hnl[4][2][2];
 #pragma unroll 1
-        for (int hb = 0; hb < MT_ROWS / 16; hb++) {
-            hpass<SPLIT>(pl, hb, warp, ah, al, hnh, hnl);
-            if (hb > 0) {
-                // output rows y0 + 16 (hb - 1) + 0..15 from the window of blocks hb - 1 and hb
-                float out[4][2][4];
-                vpass<SPLIT>(ah, al, hph, hpl, hnh, hnl, out);
-                const int yb = y0 + 16 * (hb - 1) + g;
-                float ry[2];
-#pragma unroll
-                for (int e = 0; e < 2; e++)
-                    ry[e] = interior ? inv_in : inv_in * wsum / window_sum(weff, R, yb + 8 * e, H);
-#pragma unroll
-                for (int i = 0; i < 4; i++)
-#pragma unroll
-                    for (int v = 0; v < 2; v++) {
-                        const int y = yb + 8 * (i >> 1);
-                        const int x = x0 + 16 * warp + 8 * v + 2 * t + (i & 1);
-                        const float ssim = ssim_px(make_float2(out[0][v][i], out[1][v][i]),
-                                                   make_float2(out[2][v][i], out[3][v][i]),
-                                                   ry[i >> 1] * rx[2 * v + (i & 1)], cu, cv, args.c1, args.c2);
-                        const bool valid = interior || (x < W && y < H);
-                        if (valid && P.map) P.map[(long long)y * W + x] = ssim;
-                        const bool pool = interior || (valid && x >= R && x <= W - R && y >= R && y <= H - R);
-                        acc += pool ? ssim : 0.f;
-                    }
-            }
-#pragma unroll
-            for (int p = 0; p < 4; p++)
-#pragma unroll
-                for (int v = 0; v < 2; v++)
-#pragma unroll
-                    for (int kb = 0; kb < 2; kb++) {
-                        hph[p][v][kb] = hnh[p][v][kb];
-                        hpl[p][v][kb] = hnl[p][v][kb];
-                    }
-        }
+        for (int ty = ty0; ty < ty1; ty++) {
+            const int y0 = ty * MT_H;
+            const int hb0 = ty == ty0 ? 0 : 1;  // first horizontal block computed here
 
-        pool_tiles<MT_THREADS>(acc, red, &is_last, args.partials, args.counters, args.scores, pi, P, gt,
-                               double(W - 2 * R + 1) * double(H - 2 * R + 1));
+            // the previous tile's ldmatrix reads ended before the barriers of its pooling
+            stage_moments<SPLIT>(pl, P, x0, y0, cu, cv, 16 * hb0);
+            __syncthreads();
+
+            // every output pixel in the image, under the full window and pooled
+            const bool interior = interior_x && y0 >= R && y0 + MT_H - 1 + R <= H - 1;
+
+            float acc = 0.f;
+#pragma unroll 1
+            for (int hb = hb0; hb < MT_ROWS / 16; hb++) {
+                hpass<SPLIT>(pl, hb, warp, ah, al, hnh, hnl);
+                if (hb > 0) {
+                    // output rows y0 + 16 (hb - 1) + 0..15 from the window of blocks hb - 1 and hb
+                    float out[4][2][4];
+                    vpass<SPLIT>(ah, al, hph, hpl, hnh, hnl, out);
+                    const int yb = y0 + 16 * (hb - 1) + g;
+                    float ry[2];  // 1 / (window weight * 2^12) of the lane's rows g, g + 8
+#pragma unroll
+                    for (int e = 0; e < 2; e++)
+                        ry[e] = interior ? inv_in : inv_in * wsum / window_sum(weff, R, yb + 8 * e, H);
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+#pragma unroll
+                        for (int v = 0; v < 2; v++) {
+                            const int y = yb + 8 * (i >> 1);
+                            const int x = x0 + 16 * warp + 8 * v + 2 * t + (i & 1);
+                            const float ssim = ssim_px(make_float2(out[0][v][i], out[1][v][i]),
+                                                       make_float2(out[2][v][i], out[3][v][i]),
+                                                       ry[i >> 1] * rx[2 * v + (i & 1)], cu, cv, args.c1, args.c2);
+                            const bool valid = interior || (x < W && y < H);
+                            if (valid && P.map) P.map[(long long)y * W + x] = ssim;
+                            const bool pool = interior || (valid && x >= R && x <= W - R && y >= R && y <= H - R);
+                            acc += pool ? ssim : 0.f;
+                        }
+                }
+#pragma unroll
+                for (int p = 0; p < 4; p++)
+#pragma unroll
+                    for (int v = 0; v < 2; v++)
+#pragma unroll
+                        for (int kb = 0; kb < 2; kb++) {
+                            hph[p][v][kb] = hnh[p][v][kb];
+                            hpl[p][v][kb] = hnl[p][v][kb];
+                        }
+            }
+
+            pool_tiles<MT_THREADS>(acc, red, &is_last, args.partials, args.counters, args.scores, pi, P,
+                                   P.tile_base + ty * P.tiles_x + tx, double(W - 2 * R + 1) * double(H - 2 * R + 1));
+        }
     }
 }
 
