@@ -23,9 +23,11 @@
 // its five 16-row horizontal blocks and four vertical blocks in a rolled loop (the code stays in
 // the instruction cache).  The moments are taken about the tile's centre pixel (u, v) and scaled
 // by 2^12 (largest staged magnitude 4 * 2^12, well inside FP16's range, and small values stay clear
-// of FP16's subnormals).  The split form walks column segments of four tiles with one shift per
+// of FP16's subnormals).  The split form walks column segments of six tiles with one shift per
 // segment (its accuracy does not depend on the shift tile): each later tile reuses the previous
-// tile's last horizontal block from registers and stages 64 rows, not 80 (+4% measured).
+// tile's last horizontal block from registers and stages 64 rows, not 80.  Measured at 1080p
+// (17 tiles a column) with segments of 4 / 5 / 6 / 7 / 8 tiles: 0.96 / 1.06 / 1.08 / 1.02 / 0.99x
+// the FP32 kernel.
 // Measured against 64x32 tiles, the taller tile stages a third fewer pixels
 // per output and runs 1.35x faster despite one CTA fewer per SM; taller or wider tiles were slower
 // (96 or 128 rows) or took the single-product form past its bound (128 columns).
@@ -54,7 +56,7 @@ static_assert((2 * MT_LD) % 128 == 48, "ldmatrix rows must fall in distinct bank
 // 2 (split products, 112 KB); the register budgets follow.
 constexpr int MT_MIN_CTAS_SINGLE = 512 / MT_THREADS, MT_MIN_CTAS_SPLIT = 256 / MT_THREADS > 0 ? 256 / MT_THREADS : 1;
 constexpr float MT_SCALE = 4096.f;    // staged moments are scaled by 2^12
-constexpr int MT_SEG_SPLIT = 4;       // split form: tiles per column segment (one shift per segment)
+constexpr int MT_SEG_SPLIT = 6;       // split form: tiles per column segment (one shift per segment)
 
 struct SsimMmaArgs {
     const SsimPairDev *pairs;
