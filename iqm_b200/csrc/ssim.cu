@@ -388,7 +388,7 @@ void ssim_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_ss
     const int tw = mma ? MT_W : TW, th = mma ? MT_H : strip_rows(R);
     std::vector<SsimPairDev> hd(n);
     int total = 0, units = 0;
-    const int segt = p.precision == IQM_MIXED ? MT_SEG_SPLIT : 1;  // tiles per column segment
+    const int segt = MT_SEG_SPLIT;  // tensor-core kernel: tiles per column segment (work unit)
     for (int i = 0; i < n; i++) {
         const iqm_pair &q = pairs[i];
         SsimPairDev &d = hd[i];

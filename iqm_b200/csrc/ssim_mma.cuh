@@ -56,7 +56,7 @@ static_assert((2 * MT_LD) % 128 == 48, "ldmatrix rows must fall in distinct bank
 // 2 (split products, 112 KB); the register budgets follow.
 constexpr int MT_MIN_CTAS_SINGLE = 512 / MT_THREADS, MT_MIN_CTAS_SPLIT = 256 / MT_THREADS > 0 ? 256 / MT_THREADS : 1;
 constexpr float MT_SCALE = 4096.f;    // staged moments are scaled by 2^12
-constexpr int MT_SEG_SPLIT = 6;       // split form: tiles per column segment (one shift per segment)
+constexpr int MT_SEG_SPLIT = 6;       // tiles per column segment (a work unit; the split form's shift tile)
 
 struct SsimMmaArgs {
     const SsimPairDev *pairs;
@@ -341,10 +341,12 @@ __global__ void __launch_bounds__(MT_THREADS, SPLIT == 1 ? MT_MIN_CTAS_SINGLE : 
     const float inv_in = 1.0f / (wsum * wsum * MT_SCALE);
 
     // A work unit is a column segment of SEGT vertically adjacent tiles of one pair, walked top to
-    // bottom with one shift for the segment: each tile after the first takes its first horizontal
-    // block (image rows y0 - 8 .. y0 + 7) from the previous tile's last one, still in registers, and
-    // stages only the 64 rows below it.
-    constexpr int SEGT = SPLIT == 1 ? 1 : MT_SEG_SPLIT;
+    // bottom.  The split form uses one shift for the segment, so each tile after the first takes its
+    // first horizontal block (image rows y0 - 8 .. y0 + 7) from the previous tile's last one, still
+    // in registers, and stages only the 64 rows below it.  The single-product form keeps one shift
+    // per tile (its error grows with the shift tile) and stages every tile whole.
+    constexpr int SEGT = MT_SEG_SPLIT;
+    constexpr bool SHARE = SPLIT != 1;  // one shift per segment, the boundary block reused
     unsigned hph[4][2][2], hpl[4][2][2], hnh[4][2][2], hnl[4][2][2];
     for (int unit = blockIdx.x; unit < total_units; unit += gridDim.x) {
         const int pi = find_unit(args.pairs, args.npairs, unit);
@@ -355,16 +357,18 @@ __global__ void __launch_bounds__(MT_THREADS, SPLIT == 1 ? MT_MIN_CTAS_SINGLE : 
         const int ty1 = min(ty0 + SEGT, P.ntiles / P.tiles_x);
         const int x0 = tx * MT_W;
 
-        // shift constants: u, v of the segment's centre pixel
-        float cu, cv;
-        {
-            const int cx = min(x0 + MT_W / 2, W - 1), cy = min((ty0 + ty1) * MT_H / 2, H - 1);
+        // shift constants: u, v of the segment's (SHARE) or the tile's centre pixel
+        float cu = 0.f, cv = 0.f;
+        auto shift_at = [&](int cy) {
+            const int cx = min(x0 + MT_W / 2, W - 1);
+            cy = min(cy, H - 1);
             const uint32_t pa = __ldg(reinterpret_cast<const uint32_t *>(P.a + (long long)cy * P.pitch) + cx);
             const uint32_t pb = __ldg(reinterpret_cast<const uint32_t *>(P.b + (long long)cy * P.pitch) + cx);
             const float2 l = luma2(pa, pb);
             cu = l.x + l.y;
             cv = l.x - l.y;
-        }
+        };
+        if (SHARE) shift_at((ty0 + ty1) * MT_H / 2);
 
         // normalisation of the lane's columns (2t, 2t + 1 of each 8-column half): the window weight
         // cut at the image border, relative to the interior one
@@ -379,7 +383,8 @@ __global__ void __launch_bounds__(MT_THREADS, SPLIT == 1 ? MT_MIN_CTAS_SINGLE : 
 #pragma unroll 1
         for (int ty = ty0; ty < ty1; ty++) {
             const int y0 = ty * MT_H;
-            const int hb0 = ty == ty0 ? 0 : 1;  // first horizontal block computed here
+            const int hb0 = SHARE && ty != ty0 ? 1 : 0;  // first horizontal block computed here
+            if (!SHARE) shift_at(y0 + MT_H / 2);
 
             // the previous tile's ldmatrix reads ended before the barriers of its pooling
             stage_moments<SPLIT>(pl, P, x0, y0, cu, cv, 16 * hb0);
