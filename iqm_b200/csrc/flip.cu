@@ -8,7 +8,9 @@
 // here is its mean.
 //
 // Two kernels:
-//   flip_hpass_kernel  one CTA per 512-pixel row segment of both images: RGBA8 -> linear RGB by a
+//   flip_hpass_kernel  one CTA per 512-pixel segment of 8 rows of both images, walked row by row
+//                      with each row's pixels loaded during the previous row's taps (measured
+//                      1.41x the one-row-per-CTA form at 67 ppd): RGBA8 -> linear RGB by a
 //                      256-entry table (the sRGB curve of srgb_to_ycxcz.glsl:22-28 on 8-bit inputs),
 //                      -> XYZ -> YCxCz in shared memory, then the horizontal feature taps (g, edge,
 //                      point on (Y+16)/116, feature_filter_horizontal.glsl) and the horizontal CSF
@@ -41,6 +43,8 @@ constexpr int MAXR = 32;          // largest supported filter radius (ppd up to 
 constexpr int MAXT = 2 * MAXR + 1;
 constexpr int HSEG = 512;         // pixels per row segment (hpass)
 constexpr int HT = HSEG / 4;      // hpass threads (4 pixels each)
+constexpr int HROWS = 8;          // hpass: rows one CTA walks down its segment column
+constexpr int HQ = (2 * (HSEG + 2 * MAXR) + HT - 1) / HT;  // staged pixels per thread and row, at most
 constexpr int VT_COLS = 32, VT_ROWS = 32, VT_RPT = 8;  // vpass tile and rows per thread
 constexpr int VT = VT_COLS * (VT_ROWS / VT_RPT);        // 128 threads
 constexpr int NPLANE = 12;        // per pair: [img][dx, ddx, value, Y, Cx, Cz]
@@ -64,7 +68,7 @@ struct FlipPairDev {
     int tiles_x, ntiles, tile_base;
     int vec_ok;
     long long plane_off;  // offset (floats) of this pair's 12 planes
-    long long seg_base;   // first hpass segment index of this pair
+    long long seg_base;   // first hpass work unit (HROWS rows of one 512-pixel segment) of this pair
 };
 
 struct FlipArgs {
@@ -97,27 +101,46 @@ __device__ __forceinline__ int find_tile(const FlipPairDev *p, int n, int t) {
 // RF, RC > 0: filter radii fixed at compile time (tap loops unrolled, weights as constant-bank
 // operands); 0: read from T.
 template <int RF, int RC>
-__global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __grid_constant__ FlipTaps T) {
+__global__ void __launch_bounds__(HT, 8) flip_hpass_kernel(FlipArgs args, const __grid_constant__ FlipTaps T) {
     __shared__ float lin[256];
     __shared__ float ycc[2][4][HSEG + 2 * MAXR];  // Y, Cx, Cz and (Y + 16) / 116
-    const long long seg = blockIdx.x;
-    const int pi = find_seg(args.pairs, args.npairs, seg);
+    const long long unit = blockIdx.x;
+    const int pi = find_seg(args.pairs, args.npairs, unit);
     const FlipPairDev P = args.pairs[pi];
     const int segs_x = (P.w + HSEG - 1) / HSEG;
-    const long long local = seg - P.seg_base;
-    const int y = int(local / segs_x);
+    const long long local = unit - P.seg_base;
+    const int y_first = int(local / segs_x) * HROWS;
+    const int y_end = min(y_first + HROWS, P.h);
     const int x0 = int(local % segs_x) * HSEG;
     const int rf = RF ? RF : T.rf, rc = RC ? RC : T.rc;
     const int R = max(rf, rc);
     for (int i = threadIdx.x; i < 256; i += HT) lin[i] = T.lin[i];
-    __syncthreads();
-    // stage YCxCz of columns x0-R .. x0+HSEG+R-1 (clamped to the image), both images
+    // columns x0-R .. x0+HSEG+R-1 (clamped to the image) of both images; each thread's share of a
+    // row's pixels is loaded a row ahead, so the loads run under the previous row's taps
     const int ncols = HSEG + 2 * R;
-#pragma unroll 4
-    for (int q = threadIdx.x; q < 2 * ncols; q += HT) {
+    uint32_t raw[HQ];
+    auto load_row = [&](int yy) {
+#pragma unroll
+        for (int k = 0; k < HQ; k++) {
+            const int q = threadIdx.x + k * HT;
+            if (q < 2 * ncols) {
+                const int img = q / ncols, c = q - img * ncols;
+                const int x = min(max(x0 - R + c, 0), P.w - 1);
+                raw[k] = __ldg(reinterpret_cast<const uint32_t *>((img ? P.b : P.a) + (long long)yy * P.pitch) + x);
+            }
+        }
+    };
+    load_row(y_first);
+    __syncthreads();  // the sRGB table
+#pragma unroll 1
+    for (int y = y_first; y < y_end; y++) {
+    // stage YCxCz of the row, both images
+#pragma unroll
+    for (int k = 0; k < HQ; k++) {
+        const int q = threadIdx.x + k * HT;
+        if (q >= 2 * ncols) break;
         const int img = q / ncols, c = q - img * ncols;
-        const int x = min(max(x0 - R + c, 0), P.w - 1);
-        const uint32_t px = __ldg(reinterpret_cast<const uint32_t *>((img ? P.b : P.a) + (long long)y * P.pitch) + x);
+        const uint32_t px = raw[k];
         const float r = lin[px & 0xffu], g = lin[(px >> 8) & 0xffu], b = lin[(px >> 16) & 0xffu];
         float X = fmaf(T.rgb2xyz[0], r, fmaf(T.rgb2xyz[1], g, T.rgb2xyz[2] * b));
         float Y = fmaf(T.rgb2xyz[3], r, fmaf(T.rgb2xyz[4], g, T.rgb2xyz[5] * b));
@@ -131,6 +154,7 @@ __global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __g
         ycc[img][3][c] = (ycc[img][0][c] + 16.0f) / 116.0f;
     }
     __syncthreads();
+    if (y + 1 < y_end) load_row(y + 1);
     const int n = P.w * P.h;
     float *planes = args.planes + P.plane_off;
     const int xl = 4 * threadIdx.x;  // first of this thread's 4 segment columns
@@ -217,6 +241,8 @@ __global__ void __launch_bounds__(HT) flip_hpass_kernel(FlipArgs args, const __g
                 }
             }
         }
+    }
+    __syncthreads();  // the row's taps are read before the next row is staged
     }
 }
 
@@ -638,7 +664,7 @@ void flip_enqueue(iqm_ctx *ctx, const std::vector<iqm_pair> &pairs, const iqm_fl
         d.plane_off = plane_floats;
         d.seg_base = segs;
         tiles += d.ntiles;
-        segs += (long long)iqm::ceil_div(q.w, HSEG) * q.h;
+        segs += (long long)iqm::ceil_div(q.w, HSEG) * iqm::ceil_div(q.h, HROWS);
         plane_floats += (long long)NPLANE * q.w * q.h;
     }
     IQM_REQUIRE(segs < (1LL << 31) && tiles < (1 << 30), "batch too large");
