@@ -424,19 +424,44 @@ fsim_inv_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int 
         }
     };
     if (PN > 0 && nbw > 0) load_filter(o * 4);
-    for (int idx = threadIdx.x; idx < cols * h2; idx += blockDim.x) {
-        const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
-        if (c >= nc) continue;
-        float2 v = make_float2(1.f, 0.f);
-        if (!consts_mode) {
-            const int x = x0 + c;
-            // Z = F(Y_img + i Y_ref): F(Y_img) = (Z(k) + conj Z(-k)) / 2, F(Y_ref) = (Z(k) - conj Z(-k)) / 2i
-            const float2 z = src[size_t(y) * g.w2 + x];
-            const float2 m = src[size_t(y ? h2 - y : 0) * g.w2 + (x ? g.w2 - x : 0)];
-            v = img == 0 ? make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y))
-                         : make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
+    // Z = F(Y_img + i Y_ref): F(Y_img) = (Z(k) + conj Z(-k)) / 2, F(Y_ref) = (Z(k) - conj Z(-k)) / 2i
+    auto separate = [&](float2 z, float2 m) {
+        return img == 0 ? make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y))
+                        : make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
+    };
+    if constexpr (PN > 0) {
+        // fixed length: each thread's NB * PN / 32 slab entries, all loads in flight before the stores
+        // (blockDim.x = 32 nw threads cover cols * PN = NB nw PN entries)
+        constexpr int KS = (NB * PN + 31) / 32;
+        float2 zv[KS], mv[KS];
+#pragma unroll
+        for (int k = 0; k < KS; k++) {
+            const int idx = threadIdx.x + k * blockDim.x;
+            const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
+            zv[k] = mv[k] = make_float2(1.f, 0.f);
+            if (idx < cols * h2 && c < nc && !consts_mode) {
+                const int x = x0 + c;
+                zv[k] = __ldcg(src + size_t(y) * g.w2 + x);
+                mv[k] = __ldcg(src + size_t(y ? h2 - y : 0) * g.w2 + (x ? g.w2 - x : 0));
+            }
         }
-        Sl[size_t(c) * h2 + y] = v;
+#pragma unroll
+        for (int k = 0; k < KS; k++) {
+            const int idx = threadIdx.x + k * blockDim.x;
+            const int c = idx & (cols - 1), y = idx >> lw;
+            if (idx < cols * h2 && c < nc) Sl[size_t(c) * h2 + y] = consts_mode ? make_float2(1.f, 0.f) : separate(zv[k], mv[k]);
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < cols * h2; idx += blockDim.x) {
+            const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
+            if (c >= nc) continue;
+            float2 v = make_float2(1.f, 0.f);
+            if (!consts_mode) {
+                const int x = x0 + c;
+                v = separate(src[size_t(y) * g.w2 + x], src[size_t(y ? h2 - y : 0) * g.w2 + (x ? g.w2 - x : 0)]);
+            }
+            Sl[size_t(c) * h2 + y] = v;
+        }
     }
     __syncthreads();
     for (int s = 0; s < 4; s++) {
@@ -569,9 +594,22 @@ __global__ void __launch_bounds__(FT, engine_len<Eng>::value ? 4 : 1) fsim_inv_r
         const int y = y0 + r;
         if (r < rr && y < g.h2) {
             float2 *a = warp_area<Eng>(work, warp, wl);
+            constexpr int PN = engine_len<Eng>::value;
             for (int t = 0; t < NB; t++) {
                 const float2 *src = g.T + (size_t(plane) * 16 + o * 4 + h * NB + t) * g.n + size_t(y) * w2;
-                for (int x = lane; x < w2; x += 32) a[t * wl + x] = src[x];
+                if constexpr (PN > 0) {
+                    // fixed length: every load of the row is in flight before the first store
+                    constexpr int PV = (PN + 31) / 32;
+                    float2 v[PV];
+#pragma unroll
+                    for (int i = 0; i < PV; i++)
+                        if (lane + 32 * i < PN) v[i] = __ldcg(src + lane + 32 * i);
+#pragma unroll
+                    for (int i = 0; i < PV; i++)
+                        if (lane + 32 * i < PN) a[t * wl + lane + 32 * i] = v[i];
+                } else {
+                    for (int x = lane; x < w2; x += 32) a[t * wl + x] = src[x];
+                }
             }
             float2 *res = Eng::run(a, a + NB * wl, L, sm, 1.f, wl);
             if (warp == 0 && lane == 0) parity = slab_parity(res, a);
