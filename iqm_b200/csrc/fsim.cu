@@ -339,9 +339,25 @@ __global__ void __launch_bounds__(FT, engine_len<Eng>::value ? 4 : 1) fsim_fwd_r
     float2 *a = warp_area<Eng>(work, warp, wl), *b = a + NB * wl;
     const float *Y1 = g.yiq + (size_t(pair * 2) * 3 + 2) * g.n + size_t(y0) * g.w2;
     const float *Y2 = Y1 + size_t(3) * g.n;  // the pair's second image
-    for (int t = 0; t < nb; t++)
-        for (int x = lane; x < g.w2; x += 32)
-            a[t * wl + x] = make_float2(Y1[size_t(t) * g.w2 + x], Y2[size_t(t) * g.w2 + x]);
+    constexpr int PN = engine_len<Eng>::value;
+    for (int t = 0; t < nb; t++) {
+        if constexpr (PN > 0) {  // fixed length: the row's loads all in flight before the stores
+            constexpr int PV = (PN + 31) / 32;
+            float v1[PV], v2[PV];
+#pragma unroll
+            for (int i = 0; i < PV; i++)
+                if (lane + 32 * i < PN) {
+                    v1[i] = __ldcg(Y1 + size_t(t) * g.w2 + lane + 32 * i);
+                    v2[i] = __ldcg(Y2 + size_t(t) * g.w2 + lane + 32 * i);
+                }
+#pragma unroll
+            for (int i = 0; i < PV; i++)
+                if (lane + 32 * i < PN) a[t * wl + lane + 32 * i] = make_float2(v1[i], v2[i]);
+        } else {
+            for (int x = lane; x < g.w2; x += 32)
+                a[t * wl + x] = make_float2(Y1[size_t(t) * g.w2 + x], Y2[size_t(t) * g.w2 + x]);
+        }
+    }
     const float2 *res = Eng::run(a, b, L, sm, -1.f, wl);
     float2 *S = g.spec + size_t(pair) * g.n + size_t(y0) * g.w2;
     for (int t = 0; t < nb; t++)
@@ -368,9 +384,27 @@ fsim_fwd_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int 
     const int nc = min(cols, g.w2 - x0);
     float2 *S = g.spec + size_t(pair) * g.n;
     // column c lives in warp c / NB, slot c % NB
-    for (int idx = threadIdx.x; idx < cols * g.h2; idx += blockDim.x) {
-        const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
-        if (c < nc) warp_area<Eng>(work, c / NB, wl)[(c % NB) * wl + y] = S[size_t(y) * g.w2 + x0 + c];
+    constexpr int PN = engine_len<Eng>::value;
+    if constexpr (PN > 0) {  // fixed length: each thread's slab loads all in flight before the stores
+        constexpr int KS = (NB * PN + 31) / 32;
+        float2 v[KS];
+#pragma unroll
+        for (int k = 0; k < KS; k++) {
+            const int idx = threadIdx.x + k * blockDim.x;
+            const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
+            if (idx < cols * g.h2 && c < nc) v[k] = __ldcg(S + size_t(y) * g.w2 + x0 + c);
+        }
+#pragma unroll
+        for (int k = 0; k < KS; k++) {
+            const int idx = threadIdx.x + k * blockDim.x;
+            const int c = idx & (cols - 1), y = idx >> lw;
+            if (idx < cols * g.h2 && c < nc) warp_area<Eng>(work, c / NB, wl)[(c % NB) * wl + y] = v[k];
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < cols * g.h2; idx += blockDim.x) {
+            const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
+            if (c < nc) warp_area<Eng>(work, c / NB, wl)[(c % NB) * wl + y] = S[size_t(y) * g.w2 + x0 + c];
+        }
     }
     __syncthreads();
     const int nbw = min(NB, nc - warp * NB);
