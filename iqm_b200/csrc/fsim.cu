@@ -320,6 +320,25 @@ __device__ __forceinline__ float2 *warp_area(float2 *base, int warp, int wl) {
 using Engine270 = FixedEngine<iqm::FixedPlan<270, 9, 3, 10>>;
 using Engine480 = FixedEngine<iqm::FixedPlanIP<480, 15, 8, 4>>;
 
+// Strided copy with up to 8 independent loads in flight per thread: ld(i) for i = first, first +
+// step, ... < n, in batches of 8 loads before their 8 stores st(i, v) (runtime-length paths, whose
+// plain loops would wait for each load before issuing the next).
+template <class T, class Ld, class St>
+__device__ __forceinline__ void batched_copy(int first, int n, int step, Ld ld, St st) {
+    for (int i0 = first; i0 < n; i0 += 8 * step) {
+        T v[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if (i0 + k * step < n) v[k] = ld(i0 + k * step);
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if (i0 + k * step < n) st(i0 + k * step, v[k]);
+    }
+}
+struct F2x2 {
+    float2 z, m;
+};
+
 // forward transform (src/gpu/fsim/fsim.cpp:270-368: luma as complex (Y, 0), sign -1, unscaled),
 // NB rows per warp.
 template <class Eng>
@@ -354,8 +373,9 @@ __global__ void __launch_bounds__(FT, engine_len<Eng>::value ? 4 : 1) fsim_fwd_r
             for (int i = 0; i < PV; i++)
                 if (lane + 32 * i < PN) a[t * wl + lane + 32 * i] = make_float2(v1[i], v2[i]);
         } else {
-            for (int x = lane; x < g.w2; x += 32)
-                a[t * wl + x] = make_float2(Y1[size_t(t) * g.w2 + x], Y2[size_t(t) * g.w2 + x]);
+            batched_copy<float2>(
+                lane, g.w2, 32, [&](int x) { return make_float2(Y1[size_t(t) * g.w2 + x], Y2[size_t(t) * g.w2 + x]); },
+                [&](int x, float2 v) { a[t * wl + x] = v; });
         }
     }
     const float2 *res = Eng::run(a, b, L, sm, -1.f, wl);
@@ -401,10 +421,16 @@ fsim_fwd_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int 
             if (idx < cols * g.h2 && c < nc) warp_area<Eng>(work, c / NB, wl)[(c % NB) * wl + y] = v[k];
         }
     } else {
-        for (int idx = threadIdx.x; idx < cols * g.h2; idx += blockDim.x) {
-            const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
-            if (c < nc) warp_area<Eng>(work, c / NB, wl)[(c % NB) * wl + y] = S[size_t(y) * g.w2 + x0 + c];
-        }
+        batched_copy<float2>(
+            threadIdx.x, cols * g.h2, blockDim.x,
+            [&](int idx) {
+                const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
+                return c < nc ? S[size_t(y) * g.w2 + x0 + c] : make_float2(0.f, 0.f);
+            },
+            [&](int idx, float2 v) {
+                const int c = idx & (cols - 1), y = idx >> lw;
+                if (c < nc) warp_area<Eng>(work, c / NB, wl)[(c % NB) * wl + y] = v;
+            });
     }
     __syncthreads();
     const int nbw = min(NB, nc - warp * NB);
@@ -486,16 +512,22 @@ fsim_inv_cols_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, int 
             if (idx < cols * h2 && c < nc) Sl[size_t(c) * h2 + y] = consts_mode ? make_float2(1.f, 0.f) : separate(zv[k], mv[k]);
         }
     } else {
-        for (int idx = threadIdx.x; idx < cols * h2; idx += blockDim.x) {
-            const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
-            if (c >= nc) continue;
-            float2 v = make_float2(1.f, 0.f);
-            if (!consts_mode) {
-                const int x = x0 + c;
-                v = separate(src[size_t(y) * g.w2 + x], src[size_t(y ? h2 - y : 0) * g.w2 + (x ? g.w2 - x : 0)]);
-            }
-            Sl[size_t(c) * h2 + y] = v;
-        }
+        batched_copy<F2x2>(
+            threadIdx.x, cols * h2, blockDim.x,
+            [&](int idx) {
+                const int c = idx & (cols - 1), y = idx >> lw;  // cols = 1 << lw
+                F2x2 p{make_float2(1.f, 0.f), make_float2(1.f, 0.f)};
+                if (c < nc && !consts_mode) {
+                    const int x = x0 + c;
+                    p.z = src[size_t(y) * g.w2 + x];
+                    p.m = src[size_t(y ? h2 - y : 0) * g.w2 + (x ? g.w2 - x : 0)];
+                }
+                return p;
+            },
+            [&](int idx, F2x2 p) {
+                const int c = idx & (cols - 1), y = idx >> lw;
+                if (c < nc) Sl[size_t(c) * h2 + y] = consts_mode ? make_float2(1.f, 0.f) : separate(p.z, p.m);
+            });
     }
     __syncthreads();
     for (int s = 0; s < 4; s++) {
@@ -554,24 +586,30 @@ fsim_inv_cols_seq_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, 
     float2 *a = Sl + size_t(cb) * h2;  // nc x wl
     float2 *b = a + size_t(cb) * wl;   // nc x wl
     const float2 *src = g.spec + size_t(g.pair0 + (plane >> 1)) * g.n;  // the pair's packed spectrum
-    for (int idx = threadIdx.x; idx < nc * h2; idx += blockDim.x) {
-        const int y = idx / nc, c = idx - y * nc;
-        const int x = x0 + c;
-        const float2 z = src[size_t(y) * w2 + x];
-        const float2 m = src[size_t(y ? h2 - y : 0) * w2 + (x ? w2 - x : 0)];
-        Sl[size_t(c) * h2 + y] = img == 0 ? make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y))
-                                          : make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
-    }
+    batched_copy<F2x2>(
+        threadIdx.x, nc * h2, blockDim.x,
+        [&](int idx) {
+            const int y = idx / nc, c = idx - y * nc;
+            const int x = x0 + c;
+            return F2x2{src[size_t(y) * w2 + x], src[size_t(y ? h2 - y : 0) * w2 + (x ? w2 - x : 0)]};
+        },
+        [&](int idx, F2x2 p) {
+            const int y = idx / nc, c = idx - y * nc;
+            const float2 z = p.z, m = p.m;
+            Sl[size_t(c) * h2 + y] = img == 0 ? make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y))
+                                              : make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
+        });
     __syncthreads();
     for (int s = 0; s < 4; s++) {
         const int z = o * 4 + s;
         const float *H = g.filters + size_t(z) * g.n + size_t(x0) * h2;  // column-major filter plane
-        for (int idx = threadIdx.x; idx < nc * h2; idx += blockDim.x) {
-            const int c = idx / h2, y = idx - c * h2;
-            const float hv = __ldg(H + idx);
-            const float2 v = Sl[idx];
-            a[size_t(c) * wl + y] = make_float2(hv * v.x, hv * v.y);
-        }
+        batched_copy<float>(
+            threadIdx.x, nc * h2, blockDim.x, [&](int idx) { return __ldg(H + idx); },
+            [&](int idx, float hv) {
+                const int c = idx / h2, y = idx - c * h2;
+                const float2 v = Sl[idx];
+                a[size_t(c) * wl + y] = make_float2(hv * v.x, hv * v.y);
+            });
         __syncthreads();
         const float2 *res = iqm::fft_run(a, b, L, 1.f, nc, wl);
         float2 *dst = g.T + (size_t(plane) * 16 + z) * g.n;
@@ -642,7 +680,8 @@ __global__ void __launch_bounds__(FT, engine_len<Eng>::value ? 4 : 1) fsim_inv_r
                     for (int i = 0; i < PV; i++)
                         if (lane + 32 * i < PN) a[t * wl + lane + 32 * i] = v[i];
                 } else {
-                    for (int x = lane; x < w2; x += 32) a[t * wl + x] = src[x];
+                    batched_copy<float2>(lane, w2, 32, [&](int x) { return src[x]; },
+                                         [&](int x, float2 v) { a[t * wl + x] = v; });
                 }
             }
             float2 *res = Eng::run(a, a + NB * wl, L, sm, 1.f, wl);
@@ -756,10 +795,16 @@ __global__ void __launch_bounds__(FT, 1) fsim_inv_rows_seq_kernel(FsimGroup g, c
     float2 *keep = sm;  // 4 x w2
     float2 *a = sm + 4 * w2, *b = a + size_t(sb) * wl;  // sb x wl each
     for (int s0 = 0; s0 < 4; s0 += sb) {
-        for (int idx = threadIdx.x; idx < sb * w2; idx += FT) {
-            const int t = idx / w2, x = idx - t * w2;
-            a[size_t(t) * wl + x] = src[size_t(s0 + t) * g.n + x];
-        }
+        batched_copy<float2>(
+            threadIdx.x, sb * w2, FT,
+            [&](int idx) {
+                const int t = idx / w2, x = idx - t * w2;
+                return src[size_t(s0 + t) * g.n + x];
+            },
+            [&](int idx, float2 v) {
+                const int t = idx / w2, x = idx - t * w2;
+                a[size_t(t) * wl + x] = v;
+            });
         const float2 *res = iqm::fft_run(a, b, L, 1.f, sb, wl);
         for (int idx = threadIdx.x; idx < sb * w2; idx += FT) {
             const int t = idx / w2, x = idx - t * w2;
