@@ -27,8 +27,9 @@
 //                      (combine_error_maps.glsl:28) and FP64 pooling; the last CTA of a pair writes
 //                      the mean.
 // Filter taps depend only on pixels-per-degree: computed on the host in double, normalised once.
-// Both images go through the same compiled code (the per-pixel colour math is one non-inlined
-// function, the row pass one loop), so identical images give exactly 0.
+// Both images go through the same compiled code (the per-pixel colour math works on float2 pairs
+// {input, reference} with packed FP32x2 instructions, the row pass is one loop), so identical
+// images give exactly 0.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -57,6 +58,7 @@ struct FlipTaps {
     float lin[256];       // sRGB byte -> linear
     float rgb2xyz[9], xyz2rgb[9], white[3], inv_white[3];
     float cmax;           // HyAB(Hunt(green), Hunt(blue))^0.7
+    float pcc, dec_lo, dec_inv_span;  // 0.4 cmax, 0.95 / pcc, 1 / (cmax - pcc)
 };
 
 struct FlipPairDev {
@@ -97,6 +99,14 @@ __device__ __forceinline__ int find_tile(const FlipPairDev *p, int n, int t) {
     }
     return lo;
 }
+
+// Packed FP32x2 arithmetic for the per-pixel colour terms, whose two halves are the two images:
+// each half rounds exactly like the scalar operation.
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
 
 // RF, RC > 0: filter radii fixed at compile time (tap loops unrolled, weights as constant-bank
 // operands); 0: read from T.
@@ -151,7 +161,7 @@ __global__ void __launch_bounds__(HT, 8) flip_hpass_kernel(FlipArgs args, const 
         ycc[img][0][c] = fmaf(116.0f, Y, -16.0f);
         ycc[img][1][c] = 500.0f * (X - Y);
         ycc[img][2][c] = 200.0f * (Y - Z);
-        ycc[img][3][c] = (ycc[img][0][c] + 16.0f) / 116.0f;
+        ycc[img][3][c] = (ycc[img][0][c] + 16.0f) * (1.0f / 116.0f);
     }
     __syncthreads();
     if (y + 1 < y_end) load_row(y + 1);
@@ -246,89 +256,95 @@ __global__ void __launch_bounds__(HT, 8) flip_hpass_kernel(FlipArgs args, const 
     }
 }
 
-// x^y for the non-negative bases FLIP raises to powers: exp2(y log2 x) for x > 0 (a few ulp from
-// powf, well inside the score tolerance), powf itself for x = 0 so 0^0 and 0^-y keep their values.
-__device__ __forceinline__ float pow_nonneg(float x, float y) {
-    return x > 0.0f ? exp2f(y * log2f(x)) : powf(x, y);
+// The per-pixel colour terms use the SFU approximations (lg2.approx through __log2f, ex2.approx,
+// rsqrtf: a few ulp), far inside the score tolerance; the reference's shaders leave the accuracy of
+// pow and sqrt to the implementation as well.
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
 }
 
-// L*a*b* of normalised XYZ (shaders/flip/spatial_prefilter.glsl:86-96); the shader's
-// pow(v, 1/3) is a cube root
-__device__ __forceinline__ void xyzn_to_lab(float x, float y, float z, float lab[3]) {
+// x^y for the non-negative bases FLIP raises to powers: exp2(y log2 x) for x > 0; for x = 0 the
+// values of pow(0, y): 0 for y > 0, 1 for y = 0, +inf for y < 0.
+__device__ __forceinline__ float pow_nonneg(float x, float y) {
+    return x > 0.0f ? ex2_approx(y * __log2f(x)) : (y > 0.0f ? 0.0f : y == 0.0f ? 1.0f : __int_as_float(0x7f800000));
+}
+
+// square root of v >= 0 as v * rsqrt(v) (0 for v = 0)
+__device__ __forceinline__ float sqrt_nonneg(float v) { return v * rsqrtf(fmaxf(v, 1e-30f)); }
+
+// cube root of v > 0: exp2(log2(v) / 3), then one Newton-Raphson step on y^3 = v,
+// y <- y - (y^3 - v) / (3 y^2), which squares the estimate's relative error
+__device__ __forceinline__ float cbrt_pos(float v) {
+    const float y = ex2_approx(__log2f(v) * (1.0f / 3.0f));
+    const float y2 = y * y;
+    return y - __fdividef(fmaf(y2, y, -v), 3.0f * y2);
+}
+
+// the L*a*b* companding of one normalised XYZ component (shaders/flip/spatial_prefilter.glsl:86-96);
+// the shader's pow(v, 1/3) is a cube root
+__device__ __forceinline__ float lab_f(float v) {
     const float delta = 6.0f / 29.0f, limit = 0.008856f;
     const float k = 1.0f / (3.0f * delta * delta), o = 4.0f / 29.0f;
-    const float cx = x > limit ? cbrtf(x) : fmaf(x, k, o);
-    const float cy = y > limit ? cbrtf(y) : fmaf(y, k, o);
-    const float cz = z > limit ? cbrtf(z) : fmaf(z, k, o);
-    lab[0] = fmaf(116.0f, cy, -16.0f);
-    lab[1] = 500.0f * (cx - cy);
-    lab[2] = 200.0f * (cy - cz);
+    return v > limit ? cbrt_pos(v) : fmaf(v, k, o);
 }
+__device__ __forceinline__ float2 lab_f2(float2 v) { return make_float2(lab_f(v.x), lab_f(v.y)); }
 
-// filtered YCxCz -> Hunt-adjusted L*a*b* (shaders/flip/spatial_prefilter.glsl:74-99)
-__device__ __forceinline__ void ycxcz_to_hunt_lab(const FlipTaps &T, float Y, float Cx, float Cz, float lab[3]) {
-    const float yy = (Y + 16.0f) * (1.0f / 116.0f), cx = Cx * (1.0f / 500.0f), cz = Cz * (1.0f / 200.0f);
-    const float X = (yy + cx) * T.white[0], Yw = yy * T.white[1], Z = (yy - cz) * T.white[2];
-    float rgb[3];
+// filtered YCxCz -> Hunt-adjusted L*a*b* (shaders/flip/spatial_prefilter.glsl:74-99) of both
+// images at once
+__device__ __forceinline__ void ycxcz_to_hunt_lab2(const FlipTaps &T, float2 Y, float2 Cx, float2 Cz, float2 lab[3]) {
+    const float2 yy = mul2(add2(Y, dup2(16.0f)), dup2(1.0f / 116.0f));
+    const float2 cx = mul2(Cx, dup2(1.0f / 500.0f)), cz = mul2(Cz, dup2(1.0f / 200.0f));
+    const float2 X = mul2(add2(yy, cx), dup2(T.white[0])), Yw = mul2(yy, dup2(T.white[1]));
+    const float2 Z = mul2(sub2(yy, cz), dup2(T.white[2]));
+    float2 rgb[3];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-        const float v = fmaf(T.xyz2rgb[3 * i], X, fmaf(T.xyz2rgb[3 * i + 1], Yw, T.xyz2rgb[3 * i + 2] * Z));
-        rgb[i] = fminf(fmaxf(v, 0.0f), 1.0f);
+        const float2 v = fma2(dup2(T.xyz2rgb[3 * i]), X,
+                              fma2(dup2(T.xyz2rgb[3 * i + 1]), Yw, mul2(dup2(T.xyz2rgb[3 * i + 2]), Z)));
+        rgb[i] = make_float2(fminf(fmaxf(v.x, 0.0f), 1.0f), fminf(fmaxf(v.y, 0.0f), 1.0f));
     }
-    float xyz[3];
+    float2 c[3];
 #pragma unroll
     for (int i = 0; i < 3; i++)
-        xyz[i] = fmaf(T.rgb2xyz[3 * i], rgb[0], fmaf(T.rgb2xyz[3 * i + 1], rgb[1], T.rgb2xyz[3 * i + 2] * rgb[2])) *
-                 T.inv_white[i];
-    xyzn_to_lab(xyz[0], xyz[1], xyz[2], lab);
-    lab[1] *= 0.01f * lab[0];
-    lab[2] *= 0.01f * lab[0];
+        c[i] = lab_f2(mul2(fma2(dup2(T.rgb2xyz[3 * i]), rgb[0],
+                                fma2(dup2(T.rgb2xyz[3 * i + 1]), rgb[1], mul2(dup2(T.rgb2xyz[3 * i + 2]), rgb[2]))),
+                           dup2(T.inv_white[i])));
+    lab[0] = fma2(dup2(116.0f), c[1], dup2(-16.0f));
+    lab[1] = mul2(dup2(500.0f), sub2(c[0], c[1]));
+    lab[2] = mul2(dup2(200.0f), sub2(c[1], c[2]));
+    const float2 s = mul2(dup2(0.01f), lab[0]);
+    lab[1] = mul2(lab[1], s);
+    lab[2] = mul2(lab[2], s);
 }
 
-// Everything one image contributes to a pixel, from its seven filtered sums: gradient and
-// second-derivative magnitudes and the Hunt-adjusted L*a*b* colour.  Not inlined: both images run
-// the one compiled copy, so identical inputs round identically and FLIP(a, a) is exactly 0.
-// Arguments and result travel by value (registers).
-struct ImgTerms {
-    float L, a, b, dl, ddl;
-};
-
-__device__ __noinline__ ImgTerms per_image(const FlipTaps &T, float d0, float d1, float dd0, float dd1, float cY,
-                                           float cCx, float cCz) {
-    ImgTerms o;
-    o.dl = sqrtf(fmaf(d0, d0, d1 * d1));
-    o.ddl = sqrtf(fmaf(dd0, dd0, dd1 * dd1));
-    float lab[3];
-    ycxcz_to_hunt_lab(T, cY, cCx, cCz, lab);
-    o.L = lab[0];
-    o.a = lab[1];
-    o.b = lab[2];
-    return o;
-}
-
-// Per-pixel FLIP value from the vertically filtered terms of both images, f[img] = (dx*g,
-// value*edge, ddx*g, value*point, Y*csf0, Cx*csf1, Cz*csf2): feature error
+// Per-pixel FLIP value from the vertically filtered terms of both images, f[q] = {input,
+// reference} of (dx*g, value*edge, ddx*g, value*point, Y*csf0, Cx*csf1, Cz*csf2): feature error
 // (feature_detection.glsl:48-53), HyAB colour error of the Hunt-adjusted L*a*b* values
-// (spatial_detection.glsl:67-82) and their combination (combine_error_maps.glsl:28).
-__device__ __forceinline__ float flip_pixel(const FlipTaps &T, const float (&f)[2][7]) {
-    float lab[2][3], dl[2], ddl[2];
-#pragma unroll
-    for (int m = 0; m < 2; m++) {
-        const ImgTerms t = per_image(T, f[m][0], f[m][1], f[m][2], f[m][3], f[m][4], f[m][5], f[m][6]);
-        lab[m][0] = t.L;
-        lab[m][1] = t.a;
-        lab[m][2] = t.b;
-        dl[m] = t.dl;
-        ddl[m] = t.ddl;
-    }
-    const float ed = fabsf(dl[0] - dl[1]), pd = fabsf(ddl[0] - ddl[1]);
-    const float def = sqrtf(rsqrtf(2.0f) * fmaxf(ed, pd));
-    const float d0 = lab[0][0] - lab[1][0], d1 = lab[0][1] - lab[1][1], d2 = lab[0][2] - lab[1][2];
-    const float hy = fabsf(d0) + sqrtf(fmaf(d1, d1, d2 * d2));
+// (spatial_detection.glsl:67-82) and their combination (combine_error_maps.glsl:28).  Each image's
+// terms are one half of a packed operation or the same scalar code, so identical images give
+// exactly 0.
+__device__ __forceinline__ float flip_pixel2(const FlipTaps &T, const float2 (&f)[7]) {
+    const float2 g2 = fma2(f[0], f[0], mul2(f[1], f[1])), p2 = fma2(f[2], f[2], mul2(f[3], f[3]));
+    float2 lab[3];
+    ycxcz_to_hunt_lab2(T, f[4], f[5], f[6], lab);
+    const float ed = fabsf(sqrt_nonneg(g2.x) - sqrt_nonneg(g2.y));
+    const float pd = fabsf(sqrt_nonneg(p2.x) - sqrt_nonneg(p2.y));
+    const float def = sqrt_nonneg(0.70710678f * fmaxf(ed, pd));
+    const float d0 = lab[0].x - lab[0].y, d1 = lab[1].x - lab[1].y, d2 = lab[2].x - lab[2].y;
+    const float hy = fabsf(d0) + sqrt_nonneg(fmaf(d1, d1, d2 * d2));
     const float de = pow_nonneg(hy, 0.7f);
-    const float pcc = 0.4f * T.cmax;
-    const float dec = de < pcc ? (0.95f / pcc) * de : 0.95f + ((de - pcc) / (T.cmax - pcc)) * (1.0f - 0.95f);
+    const float dec = de < T.pcc ? T.dec_lo * de : 0.95f + ((de - T.pcc) * T.dec_inv_span) * (1.0f - 0.95f);
     return pow_nonneg(dec, 1.0f - def);
+}
+
+// the 7 filtered terms of both images from per-image accumulators
+__device__ __forceinline__ float flip_pixel(const FlipTaps &T, const float (&f)[2][7]) {
+    float2 v[7];
+#pragma unroll
+    for (int q = 0; q < 7; q++) v[q] = make_float2(f[0][q], f[1][q]);
+    return flip_pixel2(T, v);
 }
 
 // Pools the CTA's FP64 partial sum; the last CTA of a pair writes the pair's mean.
@@ -622,6 +638,9 @@ void make_taps(double ppd, FlipTaps &T) {
     lab_of(0, 0, 1, lb);
     const double hy = std::fabs(lg[0] - lb[0]) + std::sqrt((lg[1] - lb[1]) * (lg[1] - lb[1]) + (lg[2] - lb[2]) * (lg[2] - lb[2]));
     T.cmax = float(std::pow(hy, 0.7));
+    T.pcc = 0.4f * T.cmax;
+    T.dec_lo = 0.95f / T.pcc;
+    T.dec_inv_span = 1.0f / (T.cmax - T.pcc);
 }
 
 iqm_flip_params resolve(const iqm_flip_params *p) {
