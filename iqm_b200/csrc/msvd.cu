@@ -84,9 +84,9 @@ __device__ __forceinline__ void load_block(const uint8_t *img, long long pitch, 
 // Singular values (descending) of the 8x8 matrix whose columns are c[0..7]; c is destroyed.
 // One-sided Jacobi: each (i, j) column pair is rotated so the columns become orthogonal.  Inner
 // products, rotations and the squared column norms (recomputed from the rotated columns) are FP32;
-// the rotation test |<ci,cj>|^2 > eps^2 |ci|^2 |cj|^2 is evaluated in FP64 (eps = 4 FLT_EPSILON,
-// above FP32 rounding noise, so sweeps stop: at most 6 on the OpenCV fixture blocks), and the final
-// norms are accumulated in FP64.
+// the rotation test |<ci,cj>|^2 > eps^2 |ci|^2 |cj|^2 is FP32 too (eps = 4 FLT_EPSILON, above FP32
+// rounding noise, so sweeps stop: at most 6 on the OpenCV fixture blocks), and the final norms are
+// accumulated in FP64 like OpenCV's Jacobi SVD.
 __device__ __forceinline__ void svd8_values(float c[8][8], float s[8]) {
     float nrm[8];
 #pragma unroll
@@ -96,7 +96,7 @@ __device__ __forceinline__ void svd8_values(float c[8][8], float s[8]) {
         for (int r = 0; r < 8; r++) q = fmaf(c[i][r], c[i][r], q);
         nrm[i] = q;
     }
-    const double eps2 = 16.0 * double(FLT_EPSILON) * double(FLT_EPSILON);
+    const float eps2 = 16.0f * FLT_EPSILON * FLT_EPSILON;
     for (int sweep = 0; sweep < 60; sweep++) {
         bool changed = false;
 #pragma unroll
@@ -106,14 +106,19 @@ __device__ __forceinline__ void svd8_values(float c[8][8], float s[8]) {
                 float p = 0.f;
 #pragma unroll
                 for (int r = 0; r < 8; r++) p = fmaf(c[i][r], c[j][r], p);
-                const double pd = double(p);
-                if (pd * pd > eps2 * double(nrm[i]) * double(nrm[j])) {
+                // all three products stay far inside FP32's range (norms < 2^20); pairs whose inner
+                // product is below 1e-15 count as orthogonal, so columns that shrink to rounding
+                // noise do not keep the sweeps going through denormal products
+                if (p * p > fmaxf(eps2 * nrm[i] * nrm[j], 1e-30f)) {
                     // |p| <= |ci||cj| < 2^20 here, so the fast quotient is accurate to a few ulp; the
                     // angle only steers the sweep, later rotations remove what it leaves
                     const float zeta = __fdividef(nrm[j] - nrm[i], 2.0f * p);
                     const float az = fabsf(zeta);
-                    // tan(theta): smaller root of t^2 + 2 zeta t - 1 = 0 (1/(2 zeta) once zeta^2 overflows)
-                    const float t = copysignf(1.0f, zeta) / (az < 1e18f ? az + sqrtf(fmaf(zeta, zeta, 1.0f)) : 2.0f * az);
+                    // tan(theta): smaller root of t^2 + 2 zeta t - 1 = 0 (1/(2 zeta) once zeta^2
+                    // overflows); sqrt(z) as z rsqrt(z) for z = zeta^2 + 1 >= 1, and the fast
+                    // quotient for a denominator in [1, 2^61)
+                    const float z = fmaf(zeta, zeta, 1.0f);
+                    const float t = __fdividef(copysignf(1.0f, zeta), az < 1e18f ? az + z * rsqrtf(z) : 2.0f * az);
                     const float cs = rsqrtf(fmaf(t, t, 1.0f));
                     const float sn = cs * t;
                     float ni = 0.f, nj = 0.f;
