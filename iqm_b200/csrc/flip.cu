@@ -256,23 +256,14 @@ __global__ void __launch_bounds__(HT, 8) flip_hpass_kernel(FlipArgs args, const 
     }
 }
 
-// The per-pixel colour terms use the SFU approximations (lg2.approx through __log2f, ex2.approx,
-// rsqrtf: a few ulp), far inside the score tolerance; the reference's shaders leave the accuracy of
-// pow and sqrt to the implementation as well.
-__device__ __forceinline__ float ex2_approx(float x) {
-    float y;
-    asm("ex2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
+using iqm::ex2_approx;
+using iqm::sqrt_nonneg;
 
 // x^y for the non-negative bases FLIP raises to powers: exp2(y log2 x) for x > 0; for x = 0 the
 // values of pow(0, y): 0 for y > 0, 1 for y = 0, +inf for y < 0.
 __device__ __forceinline__ float pow_nonneg(float x, float y) {
     return x > 0.0f ? ex2_approx(y * __log2f(x)) : (y > 0.0f ? 0.0f : y == 0.0f ? 1.0f : __int_as_float(0x7f800000));
 }
-
-// square root of v >= 0 as v * rsqrt(v) (0 for v = 0)
-__device__ __forceinline__ float sqrt_nonneg(float v) { return v * rsqrtf(fmaxf(v, 1e-30f)); }
 
 // cube root of v > 0: exp2(log2(v) / 3), then one Newton-Raphson step on y^3 = v,
 // y <- y - (y^3 - v) / (3 y^2), which squares the estimate's relative error

@@ -622,7 +622,8 @@ fsim_inv_cols_seq_kernel(FsimGroup g, const __grid_constant__ FftLen L, int wl, 
 }
 
 // Per-pixel response sums of one orientation from its 4 scales (scaled by 1/N here), as
-// shaders/fsim/fsim_sum_filter_responses.glsl:43-80 and fsim_pack_for_median.glsl:39-43.
+// shaders/fsim/fsim_sum_filter_responses.glsl:43-80 and fsim_pack_for_median.glsl:39-43; square
+// roots and the reciprocal from the SFU approximations.
 __device__ __forceinline__ void response_sums(const float2 v[4], float invN, float &sA, float &en, float &e0) {
     float re[4], im[4];
     float sE = 0.f, sO = 0.f;
@@ -631,11 +632,11 @@ __device__ __forceinline__ void response_sums(const float2 v[4], float invN, flo
     for (int s = 0; s < 4; s++) {
         re[s] = v[s].x * invN;
         im[s] = v[s].y * invN;
-        sA += sqrtf(re[s] * re[s] + im[s] * im[s]);
+        sA += iqm::sqrt_nonneg(re[s] * re[s] + im[s] * im[s]);
         sE += re[s];
         sO += im[s];
     }
-    const float rxe = 1.0f / (sqrtf(sE * sE + sO * sO) + 0.0001f);
+    const float rxe = __fdividef(1.0f, iqm::sqrt_nonneg(sE * sE + sO * sO) + 0.0001f);
     const float mE = sE * rxe, mO = sO * rxe;
     en = 0.f;
 #pragma unroll

@@ -253,4 +253,18 @@ void enqueue_msvd_dev(iqm_ctx *ctx, const iqm_pair *pairs, int n, double *d_scor
 
 inline unsigned ceil_div(long a, long b) { return unsigned((a + b - 1) / b); }
 
+// Per-pixel transcendentals from the SFU approximations (a few ulp, far inside the 1e-5 score
+// bounds; the reference's shaders leave the accuracy of sqrt, pow and division to the implementation
+// as well).
+#ifdef __CUDACC__
+// 2^x by the PTX ex2.approx instruction
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+// sqrt(v) for v >= 0 as v * rsqrt(v); 0 for v = 0
+__device__ __forceinline__ float sqrt_nonneg(float v) { return v * rsqrtf(fmaxf(v, 1e-30f)); }
+#endif
+
 }  // namespace iqm
