@@ -636,7 +636,7 @@ __device__ __forceinline__ void response_sums(const float2 v[4], float invN, flo
         sE += re[s];
         sO += im[s];
     }
-    const float rxe = __fdividef(1.0f, iqm::sqrt_nonneg(sE * sE + sO * sO) + 0.0001f);
+    const float rxe = iqm::rcp_approx(iqm::sqrt_nonneg(sE * sE + sO * sO) + 0.0001f);
     const float mE = sE * rxe, mO = sO * rxe;
     en = 0.f;
 #pragma unroll

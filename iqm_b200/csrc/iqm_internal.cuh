@@ -255,16 +255,31 @@ inline unsigned ceil_div(long a, long b) { return unsigned((a + b - 1) / b); }
 
 // Per-pixel transcendentals from the SFU approximations (a few ulp, far inside the 1e-5 score
 // bounds; the reference's shaders leave the accuracy of sqrt, pow and division to the implementation
-// as well).
+// as well).  The PTX .ftz forms are single SFU operations; every argument they get here is a normal
+// number (or 0 / inf where stated), so flushing subnormals changes nothing.
 #ifdef __CUDACC__
-// 2^x by the PTX ex2.approx instruction
-__device__ __forceinline__ float ex2_approx(float x) {
+__device__ __forceinline__ float ex2_approx(float x) {  // 2^x
     float y;
-    asm("ex2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float lg2_approx(float x) {  // log2 x (-inf for 0)
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rsqrt_approx(float x) {  // 1 / sqrt(x)
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {  // 1 / x
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
 // sqrt(v) for v >= 0 as v * rsqrt(v); 0 for v = 0
-__device__ __forceinline__ float sqrt_nonneg(float v) { return v * rsqrtf(fmaxf(v, 1e-30f)); }
+__device__ __forceinline__ float sqrt_nonneg(float v) { return v * rsqrt_approx(fmaxf(v, 1e-30f)); }
 #endif
 
 }  // namespace iqm

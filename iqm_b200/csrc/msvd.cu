@@ -110,16 +110,16 @@ __device__ __forceinline__ void svd8_values(float c[8][8], float s[8]) {
                 // product is below 1e-15 count as orthogonal, so columns that shrink to rounding
                 // noise do not keep the sweeps going through denormal products
                 if (p * p > fmaxf(eps2 * nrm[i] * nrm[j], 1e-30f)) {
-                    // |p| <= |ci||cj| < 2^20 here, so the fast quotient is accurate to a few ulp; the
-                    // angle only steers the sweep, later rotations remove what it leaves
-                    const float zeta = __fdividef(nrm[j] - nrm[i], 2.0f * p);
+                    // 1e-15 < |p| <= |ci||cj| < 2^20 here, so the SFU reciprocal is accurate to a few
+                    // ulp; the angle only steers the sweep, later rotations remove what it leaves
+                    const float zeta = (nrm[j] - nrm[i]) * iqm::rcp_approx(2.0f * p);
                     const float az = fabsf(zeta);
                     // tan(theta): smaller root of t^2 + 2 zeta t - 1 = 0 (1/(2 zeta) once zeta^2
-                    // overflows); sqrt(z) as z rsqrt(z) for z = zeta^2 + 1 >= 1, and the fast
-                    // quotient for a denominator in [1, 2^61)
+                    // overflows); sqrt(z) as z rsqrt(z) for z = zeta^2 + 1 >= 1, and the SFU
+                    // reciprocal of a denominator in [1, 2^61)
                     const float z = fmaf(zeta, zeta, 1.0f);
-                    const float t = __fdividef(copysignf(1.0f, zeta), az < 1e18f ? az + z * rsqrtf(z) : 2.0f * az);
-                    const float cs = rsqrtf(fmaf(t, t, 1.0f));
+                    const float t = copysignf(1.0f, zeta) * iqm::rcp_approx(az < 1e18f ? az + z * iqm::rsqrt_approx(z) : 2.0f * az);
+                    const float cs = iqm::rsqrt_approx(fmaf(t, t, 1.0f));
                     const float sn = cs * t;
                     float ni = 0.f, nj = 0.f;
 #pragma unroll
