@@ -1111,7 +1111,7 @@ __device__ __forceinline__ float grad_at(const float *Y, int x, int y, int w2, i
             }
         }
     const float a = vs / 16.0f, b = hs / 16.0f;
-    return sqrtf(a * a + b * b);
+    return iqm::sqrt_nonneg(a * a + b * b);
 }
 
 // Similarity terms of one pixel from the two images' phase congruency, gradient magnitude and
@@ -1119,12 +1119,13 @@ __device__ __forceinline__ float grad_at(const float *Y, int x, int y, int w2, i
 __device__ __forceinline__ void similarity_terms(float pc1, float pc2, float g1, float g2, float i1, float i2, float q1,
                                                  float q2, double &s_pcm, double &s_sim, double &s_simc) {
     const float pcm = fmaxf(pc1, pc2);
-    const float pcsim = (2.0f * pc1 * pc2 + 0.85f) / (pc1 * pc1 + pc2 * pc2 + 0.85f);
-    const float gsim = (2.0f * g1 * g2 + 160.0f) / (g1 * g1 + g2 * g2 + 160.0f);
-    const float isim = (2.0f * i1 * i2 + 200.0f) / (i1 * i1 + i2 * i2 + 200.0f);
-    const float qsim = (2.0f * q1 * q2 + 200.0f) / (q1 * q1 + q2 * q2 + 200.0f);
+    // denominators >= 0.85: SFU reciprocals; |SI SQ|^0.03 as exp2(0.03 log2 |SI SQ|) (0 for 0)
+    const float pcsim = (2.0f * pc1 * pc2 + 0.85f) * iqm::rcp_approx(pc1 * pc1 + pc2 * pc2 + 0.85f);
+    const float gsim = (2.0f * g1 * g2 + 160.0f) * iqm::rcp_approx(g1 * g1 + g2 * g2 + 160.0f);
+    const float isim = (2.0f * i1 * i2 + 200.0f) * iqm::rcp_approx(i1 * i1 + i2 * i2 + 200.0f);
+    const float qsim = (2.0f * q1 * q2 + 200.0f) * iqm::rcp_approx(q1 * q1 + q2 * q2 + 200.0f);
     const float sim = gsim * pcsim * pcm;
-    const float simc = gsim * pcsim * powf(fabsf(isim * qsim), 0.03f) * pcm;
+    const float simc = gsim * pcsim * iqm::ex2_approx(0.03f * iqm::lg2_approx(fabsf(isim * qsim))) * pcm;
     s_pcm += pcm;
     s_sim += sim;
     s_simc += simc;
@@ -1202,7 +1203,7 @@ __global__ void __launch_bounds__(FT) fsim_final_kernel(FsimGroup g) {
                             hs += v * hor[idx];
                         }
                     const float a = vs / 16.0f, b = hs / 16.0f;
-                    gm[img][q] = sqrtf(a * a + b * b);
+                    gm[img][q] = iqm::sqrt_nonneg(a * a + b * b);
                 }
             }
 #pragma unroll

@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(NT, 8) ssim_kernel(SsimArgs args) {
                             const float mu2 = mu * mu, mv2 = mv * mv;
                             const float num = (0.5f * (mu2 - mv2) + args.c1) * (0.5f * (varu - varv) + args.c2);
                             const float den = (0.5f * (mu2 + mv2) + args.c1) * (0.5f * (varu + varv) + args.c2);
-                            const float ssim = __fdividef(num, den);
+                            const float ssim = num * iqm::rcp_approx(den);  // den >= c1 c2 > 0
                             if (P.map) P.map[(long long)y * W + x] = ssim;
                             if (pool_y && x >= R && x <= W - R) acc += ssim;
                         }

@@ -285,7 +285,7 @@ __device__ __forceinline__ float ssim_px(float2 m1, float2 m2, float inv, float 
     const float2 X = make_float2(mu2.x, var.x), Y = make_float2(mu2.y, var.y), C = make_float2(c1, c2);
     const float2 plus = __ffma2_rn(__fadd2_rn(X, Y), make_float2(0.5f, 0.5f), C);
     const float2 minus = __ffma2_rn(__ffma2_rn(Y, make_float2(-1.f, -1.f), X), make_float2(0.5f, 0.5f), C);
-    return __fdividef(minus.x * minus.y, plus.x * plus.y);
+    return (minus.x * minus.y) * iqm::rcp_approx(plus.x * plus.y);  // plus.x plus.y >= c1 c2 > 0
 }
 
 // Persistent: each CTA walks tiles blockIdx.x, blockIdx.x + gridDim.x, ... (neighbouring tiles run
