@@ -100,13 +100,12 @@ __device__ __forceinline__ int find_tile(const FlipPairDev *p, int n, int t) {
     return lo;
 }
 
-// Packed FP32x2 arithmetic for the per-pixel colour terms, whose two halves are the two images:
-// each half rounds exactly like the scalar operation.
-__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+// Packed FP32x2 arithmetic for the per-pixel colour terms, whose two halves are the two images.
+using iqm::add2;
+using iqm::dup2;
+using iqm::fma2;
+using iqm::mul2;
+using iqm::sub2;
 
 // RF, RC > 0: filter radii fixed at compile time (tap loops unrolled, weights as constant-bank
 // operands); 0: read from T.

@@ -7,11 +7,12 @@
 // msvd = sum |D - median| / n with n = (W/8)*(H/8) (skipped slots count as D = 0).
 //
 // Here everything runs on the device in two kernels:
-//   msvd_block_kernel  one thread per block slot: 8 rows x 8 RGBA8 pixels of both images straight
-//                      into registers (two 16-byte loads per row and image, coalesced across a
-//                      warp of horizontally adjacent blocks), OpenCV's 15-bit fixed-point grey,
-//                      one-sided Jacobi SVD in registers (FP32 rotations and inner products, FP64
-//                      convergence test and final norms), D in FP32 as the shader does;
+//   msvd_block_kernel  two lanes per block slot (one per image): 8 rows x 8 RGBA8 pixels straight
+//                      into registers (two 16-byte loads per row, coalesced across a warp of
+//                      horizontally adjacent blocks), OpenCV's 15-bit fixed-point grey, one-sided
+//                      Jacobi SVD in registers (FP32 rotations, inner products and rotation test,
+//                      two rows per packed FP32x2 instruction; FP64 final norms), D in FP32 as the
+//                      shader does;
 //   msvd_pool_kernel   one CTA per pair: exact median by radix select (select.cuh), then the mean
 //                      absolute deviation summed in FP64, and the optional D/max(D) map.
 #include <cfloat>
@@ -60,9 +61,9 @@ __device__ __forceinline__ int find_pair(const MsvdPairDev *p, int n, int slot) 
     return lo;
 }
 
-// Loads one 8x8 grey block (column-major in registers: c[col][row]).
+// Loads one 8x8 grey block, column-major in registers as row pairs: c[col][k] = (row 2k, row 2k + 1).
 __device__ __forceinline__ void load_block(const uint8_t *img, long long pitch, int x, int y, bool vec,
-                                           float c[8][8]) {
+                                           float2 c[8][4]) {
 #pragma unroll
     for (int r = 0; r < 8; r++) {
         const uint8_t *row = img + (long long)(y + r) * pitch + 4LL * x;
@@ -77,25 +78,33 @@ __device__ __forceinline__ void load_block(const uint8_t *img, long long pitch, 
             for (int q = 0; q < 8; q++) px[q] = __ldg(reinterpret_cast<const uint32_t *>(row) + q);
         }
 #pragma unroll
-        for (int q = 0; q < 8; q++) c[q][r] = gray_u8(px[q]);
+        for (int q = 0; q < 8; q++) {
+            if (r & 1) c[q][r >> 1].y = gray_u8(px[q]);
+            else c[q][r >> 1].x = gray_u8(px[q]);
+        }
     }
+}
+
+// <ci, cj> over the 8 rows: the even and odd rows as the two halves of packed FMAs, then their sum
+__device__ __forceinline__ float dot8(const float2 (&ci)[4], const float2 (&cj)[4]) {
+    float2 q = iqm::mul2(ci[0], cj[0]);
+#pragma unroll
+    for (int k = 1; k < 4; k++) q = iqm::fma2(ci[k], cj[k], q);
+    return q.x + q.y;
 }
 
 // Singular values (descending) of the 8x8 matrix whose columns are c[0..7]; c is destroyed.
 // One-sided Jacobi: each (i, j) column pair is rotated so the columns become orthogonal.  Inner
-// products, rotations and the squared column norms (recomputed from the rotated columns) are FP32;
-// the rotation test |<ci,cj>|^2 > eps^2 |ci|^2 |cj|^2 is FP32 too (eps = 4 FLT_EPSILON, above FP32
-// rounding noise, so sweeps stop: at most 6 on the OpenCV fixture blocks), and the final norms are
-// accumulated in FP64 like OpenCV's Jacobi SVD.
-__device__ __forceinline__ void svd8_values(float c[8][8], float s[8]) {
+// products, rotations and the squared column norms (recomputed from the rotated columns) are FP32,
+// two rows per packed FP32x2 instruction (half the instructions and half the unrolled code of the
+// sweep, which otherwise overflows the instruction cache); the rotation test
+// |<ci,cj>|^2 > eps^2 |ci|^2 |cj|^2 is FP32 too (eps = 4 FLT_EPSILON, above FP32 rounding noise, so
+// sweeps stop: at most 6 on the OpenCV fixture blocks), and the final norms are accumulated in FP64
+// like OpenCV's Jacobi SVD.
+__device__ __forceinline__ void svd8_values(float2 c[8][4], float s[8]) {
     float nrm[8];
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-        float q = 0.f;
-#pragma unroll
-        for (int r = 0; r < 8; r++) q = fmaf(c[i][r], c[i][r], q);
-        nrm[i] = q;
-    }
+    for (int i = 0; i < 8; i++) nrm[i] = dot8(c[i], c[i]);
     const float eps2 = 16.0f * FLT_EPSILON * FLT_EPSILON;
     for (int sweep = 0; sweep < 60; sweep++) {
         bool changed = false;
@@ -103,9 +112,7 @@ __device__ __forceinline__ void svd8_values(float c[8][8], float s[8]) {
         for (int i = 0; i < 7; i++) {
 #pragma unroll
             for (int j = i + 1; j < 8; j++) {
-                float p = 0.f;
-#pragma unroll
-                for (int r = 0; r < 8; r++) p = fmaf(c[i][r], c[j][r], p);
+                const float p = dot8(c[i], c[j]);
                 // all three products stay far inside FP32's range (norms < 2^20); pairs whose inner
                 // product is below 1e-15 count as orthogonal, so columns that shrink to rounding
                 // noise do not keep the sweeps going through denormal products
@@ -121,18 +128,20 @@ __device__ __forceinline__ void svd8_values(float c[8][8], float s[8]) {
                     const float t = copysignf(1.0f, zeta) * iqm::rcp_approx(az < 1e18f ? az + z * iqm::rsqrt_approx(z) : 2.0f * az);
                     const float cs = iqm::rsqrt_approx(fmaf(t, t, 1.0f));
                     const float sn = cs * t;
-                    float ni = 0.f, nj = 0.f;
+                    const float2 cs2 = iqm::dup2(cs), sn2 = iqm::dup2(sn), msn2 = iqm::dup2(-sn);
+                    float2 ni = iqm::dup2(0.f), nj = iqm::dup2(0.f);
 #pragma unroll
-                    for (int r = 0; r < 8; r++) {
-                        const float xi = c[i][r], xj = c[j][r];
-                        const float yi = fmaf(cs, xi, -sn * xj), yj = fmaf(sn, xi, cs * xj);
-                        c[i][r] = yi;
-                        c[j][r] = yj;
-                        ni = fmaf(yi, yi, ni);
-                        nj = fmaf(yj, yj, nj);
+                    for (int k = 0; k < 4; k++) {
+                        const float2 xi = c[i][k], xj = c[j][k];
+                        const float2 yi = iqm::fma2(cs2, xi, iqm::mul2(msn2, xj));
+                        const float2 yj = iqm::fma2(sn2, xi, iqm::mul2(cs2, xj));
+                        c[i][k] = yi;
+                        c[j][k] = yj;
+                        ni = iqm::fma2(yi, yi, ni);
+                        nj = iqm::fma2(yj, yj, nj);
                     }
-                    nrm[i] = ni;
-                    nrm[j] = nj;
+                    nrm[i] = ni.x + ni.y;
+                    nrm[j] = nj.x + nj.y;
                     changed = true;
                 }
             }
@@ -143,7 +152,10 @@ __device__ __forceinline__ void svd8_values(float c[8][8], float s[8]) {
     for (int i = 0; i < 8; i++) {
         double q = 0.0;
 #pragma unroll
-        for (int r = 0; r < 8; r++) q = fma(double(c[i][r]), double(c[i][r]), q);
+        for (int k = 0; k < 4; k++) {
+            q = fma(double(c[i][k].x), double(c[i][k].x), q);
+            q = fma(double(c[i][k].y), double(c[i][k].y), q);
+        }
         s[i] = float(sqrt(q));
     }
     // descending order (sorting network on 8 registers)
@@ -167,8 +179,9 @@ __device__ __forceinline__ void svd8_values(float c[8][8], float s[8]) {
 // Two lanes per block slot: the even lane takes the block of the distorted image, the odd lane the
 // same block of the reference; the odd lane's singular values reach the even lane by shuffle.  One
 // copy of the SVD code serves both images and twice as many blocks are in flight.
-// Six CTAs per SM (80 registers, a few spilled to L1): measured 2.6% faster than five at 87.
-__global__ void __launch_bounds__(BLOCK_THREADS, 6) msvd_block_kernel(MsvdArgs args) {
+// Five CTAs per SM (90 registers, no spills): with the packed row pairs, six CTAs at 80 registers
+// spill the columns and measured 16% slower.
+__global__ void __launch_bounds__(BLOCK_THREADS, 5) msvd_block_kernel(MsvdArgs args) {
     const int slot = (blockIdx.x * BLOCK_THREADS + threadIdx.x) >> 1;
     const int img = threadIdx.x & 1;
     const bool in_range = slot < args.total_slots;  // both lanes of a slot agree
@@ -186,7 +199,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 6) msvd_block_kernel(MsvdArgs a
     const unsigned mask = __ballot_sync(0xffffffffu, computed);
     if (computed) {
         {  // one 8x8 block of one image
-            float c[8][8];
+            float2 c[8][4];
             load_block(img ? P.b : P.a, P.pitch, 8 * bx, 8 * by, P.vec_ok, c);
             float s[8];
             svd8_values(c, s);
