@@ -35,6 +35,7 @@
 #include <vector>
 
 #include "iqm_internal.cuh"
+#include "packed_f32x2.cuh"
 
 #define GLSL_PI 3.141592653589
 

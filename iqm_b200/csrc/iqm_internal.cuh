@@ -280,13 +280,6 @@ __device__ __forceinline__ float rcp_approx(float x) {  // 1 / x
 }
 // sqrt(v) for v >= 0 as v * rsqrt(v); 0 for v = 0
 __device__ __forceinline__ float sqrt_nonneg(float v) { return v * rsqrt_approx(fmaxf(v, 1e-30f)); }
-
-// Packed FP32x2 arithmetic: each half rounds exactly like the scalar operation.
-__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
 #endif
 
 }  // namespace iqm

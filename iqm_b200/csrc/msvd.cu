@@ -19,6 +19,7 @@
 #include <cmath>
 
 #include "iqm_internal.cuh"
+#include "packed_f32x2.cuh"
 #include "select.cuh"
 
 namespace {
