@@ -21,7 +21,7 @@ def is_prime(p):
 def planner(tmp_path_factory):
     exe = str(tmp_path_factory.mktemp("native") / "fft_plan_check")
     csrc = os.path.join(ROOT, "iqm_b200", "csrc")
-    subprocess.run(["/usr/local/cuda/bin/nvcc", "-std=c++17", "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"),
+    subprocess.run(["/usr/local/cuda/bin/nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"),
                     "-I", csrc, "-o", exe, os.path.join(ROOT, "tests", "native", "fft_plan_check.cu"),
                     os.path.join(csrc, "fft.cu")], check=True)
     return exe
