@@ -280,6 +280,18 @@ __device__ __forceinline__ float rcp_approx(float x) {  // 1 / x
 }
 // sqrt(v) for v >= 0 as v * rsqrt(v); 0 for v = 0
 __device__ __forceinline__ float sqrt_nonneg(float v) { return v * rsqrt_approx(fmaxf(v, 1e-30f)); }
+// x^y for x >= 0: exp2(y log2 x) for x > 0; for x = 0 the values of pow(0, y): 0 for y > 0, 1 for
+// y = 0, +inf for y < 0
+__device__ __forceinline__ float pow_nonneg(float x, float y) {
+    return x > 0.0f ? ex2_approx(y * lg2_approx(x)) : (y > 0.0f ? 0.0f : y == 0.0f ? 1.0f : __int_as_float(0x7f800000));
+}
+// cube root of a normal v > 0: exp2(log2(v) / 3), then one Newton-Raphson step on y^3 = v,
+// y <- y - (y^3 - v) / (3 y^2), which squares the estimate's relative error
+__device__ __forceinline__ float cbrt_pos(float v) {
+    const float y = ex2_approx(lg2_approx(v) * (1.0f / 3.0f));
+    const float y2 = y * y;
+    return y - fmaf(y2, y, -v) * rcp_approx(3.0f * y2);
+}
 #endif
 
 }  // namespace iqm
