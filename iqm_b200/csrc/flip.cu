@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(HT, 8) flip_hpass_kernel(FlipArgs args, const 
         for (int k = 0; k < HQ; k++) {
             const int q = threadIdx.x + k * HT;
             if (q < 2 * ncols) {
-                const int img = q / ncols, c = q - img * ncols;
+                const int img = q >= ncols, c = q - img * ncols;  // q < 2 ncols
                 const int x = min(max(x0 - R + c, 0), P.w - 1);
                 raw[k] = __ldg(reinterpret_cast<const uint32_t *>((img ? P.b : P.a) + (long long)yy * P.pitch) + x);
             }
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(HT, 8) flip_hpass_kernel(FlipArgs args, const 
     for (int k = 0; k < HQ; k++) {
         const int q = threadIdx.x + k * HT;
         if (q >= 2 * ncols) break;
-        const int img = q / ncols, c = q - img * ncols;
+        const int img = q >= ncols, c = q - img * ncols;  // q < 2 ncols
         const uint32_t px = raw[k];
         const float r = lin[px & 0xffu], g = lin[(px >> 8) & 0xffu], b = lin[(px >> 16) & 0xffu];
         float X = fmaf(T.rgb2xyz[0], r, fmaf(T.rgb2xyz[1], g, T.rgb2xyz[2] * b));
