@@ -255,8 +255,10 @@ inline unsigned ceil_div(long a, long b) { return unsigned((a + b - 1) / b); }
 
 // Per-pixel transcendentals from the SFU approximations (a few ulp, far inside the 1e-5 score
 // bounds; the reference's shaders leave the accuracy of sqrt, pow and division to the implementation
-// as well).  The PTX .ftz forms are single SFU operations; every argument they get here is a normal
-// number (or 0 / inf where stated), so flushing subnormals changes nothing.
+// as well).  The PTX .ftz forms are single SFU operations.  Flushing subnormals changes nothing for
+// the kernels' arguments: square roots and reciprocals get clamped or bounded-below values, and the
+// bases of the powers (colour and feature differences, products of similarity ratios) are either
+// exactly 0 or at least an ulp of their FP32 operands, far above the subnormal range.
 #ifdef __CUDACC__
 __device__ __forceinline__ float ex2_approx(float x) {  // 2^x
     float y;
