@@ -3,10 +3,10 @@
 // GIF89a; the Radiance RGBE picture format; Adobe's PSD file format; Softimage's PIC format).  Output is RGBA8 like the reference's
 // stbi_load(..., 4) (src/main.cpp:37-57), including that loader's conversions where a format
 // needs one (see each decoder).  Grey expands to R = G = B, a missing alpha becomes 255.
-// Covered: BMP with 8-bit palettes, 24-bit and 32-bit pixels (BI_RGB, or BI_BITFIELDS with
-// byte-aligned 8-bit masks), bottom-up or top-down rows; TGA types 1, 2, 3 and their run-length
-// forms 9, 10, 11 with 8-, 24- or 32-bit pixels and 24- or 32-bit colour maps, either origin; the
-// first frame of a GIF; HDR with run-length or flat RGBE scanlines; RGB PSD, 8 or 16 bits, raw or
+// Covered: BMP with the OS/2 core or Windows headers, 1/4/8-bit palettes, 16, 24 and 32-bit pixels
+// (BI_RGB, or BI_BITFIELDS of up to 8 bits a channel), bottom-up or top-down rows; TGA types 1, 2, 3
+// and their run-length forms 9, 10, 11 with 8, 15, 16, 24 or 32-bit pixels or 8/16-bit indices into
+// 8, 15, 16, 24 or 32-bit colour maps; the first frame of a GIF; HDR with run-length or flat RGBE scanlines; RGB PSD, 8 or 16 bits, raw or
 // PackBits; PIC with raw, pure or mixed run-length packets of 8-bit channels.  Other layouts are refused with a reason.
 #include <algorithm>
 #include <cmath>
@@ -39,75 +39,176 @@ uint32_t be32(const std::vector<unsigned char> &f, size_t o) {
     return be16(f, o) << 16 | be16(f, o + 2);
 }
 
-// Position (0-7, 8-bit lanes) of an 8-bit channel mask, -1 for an absent channel.
-int mask_shift(uint32_t m) {
-    if (m == 0) return -1;
-    for (int s = 0; s < 32; s += 8)
-        if (m == (0xffu << s)) return s;
-    throw std::runtime_error("BMP channel masks other than whole bytes are not supported");
-}
-
 void check_size(int64_t w, int64_t h) {
     if (w <= 0 || h <= 0 || w > 65536 || h > 65536 || w * h >= (int64_t(1) << 31))
         throw std::runtime_error("image size out of range");
 }
 
+// An n-bit channel value (1 <= n <= 8) widened to 8 bits by repeating its bit pattern (abc ->
+// abcabcab): stb_image's expansion of BMP bit-field channels.
+unsigned widen_bits(unsigned v, int n) {
+    if (n <= 0) return 0;
+    unsigned r = 0;
+    int have = 0;
+    while (have < 8) {
+        r = r << n | v;
+        have += n;
+    }
+    return (r >> (have - 8)) & 0xffu;
+}
+
+// One BMP bit-field channel: the mask's top bit lands on bit 7 of a byte, the byte keeps the mask's
+// bit count (at most 8) from its top, and the value is widened to 8 bits (stb_image's reading; for a
+// contiguous mask it is the field's value).
+struct BmpField {
+    uint32_t mask = 0;
+    int high = 0, bits = 0;
+    explicit BmpField(uint32_t m) : mask(m) {
+        for (uint32_t t = m; t; t &= t - 1) bits++;
+        for (int b = 31; b >= 0; b--)
+            if (m >> b & 1u) {
+                high = b;
+                break;
+            }
+    }
+    unsigned operator()(uint32_t px) const {
+        uint32_t v = px & mask;
+        v = high >= 7 ? v >> (high - 7) : v << (7 - high);
+        return widen_bits((v & 0xffu) >> (8 - bits), bits);
+    }
+};
+
 }  // namespace
 
+// BMP as stb_image reads it: the OS/2 core header (12 bytes) and the 40, 56, 108 and 124-byte
+// Windows headers; 1, 4 and 8-bit palettes (3-byte entries in the core header, 4-byte ones
+// otherwise), 16-bit pixels (5-5-5 unless bit fields are given), 24-bit, 32-bit (B, G, R and an alpha
+// byte that is used unless it is 0 everywhere, or bit fields); bit fields of at most 8 bits per
+// channel, widened by repeating their bit pattern; no run-length or embedded JPEG/PNG compression.
+// Rows are bottom-up unless the height is negative.  A palette index beyond the file's palette reads
+// black (the reference's loader reads an unset table entry there).
 InputImage decode_bmp(const std::vector<unsigned char> &f) {
     if (f.size() < 26 || f[0] != 'B' || f[1] != 'M') throw std::runtime_error("not a BMP file");
-    const uint32_t data_off = le32(f, 10), hdr = le32(f, 14);
-    if (hdr < 40) throw std::runtime_error("BMP core headers are not supported");
-    const int32_t w = int32_t(le32(f, 18)), hs = int32_t(le32(f, 22));
-    const uint32_t bpp = le16(f, 28), comp = le32(f, 30);
+    const uint32_t data_off = le32(f, 10), hsz = le32(f, 14);
+    if (hsz != 12 && hsz != 40 && hsz != 56 && hsz != 108 && hsz != 124)
+        throw std::runtime_error("BMP header size " + std::to_string(hsz) + " is not supported");
+    int64_t w, hs;
+    uint32_t bpp, comp = 0;
+    if (hsz == 12) {
+        w = le16(f, 18);
+        hs = le16(f, 20);
+        if (le16(f, 22) != 1) throw std::runtime_error("bad BMP");
+        bpp = le16(f, 24);
+    } else {
+        w = int32_t(le32(f, 18));
+        hs = int32_t(le32(f, 22));
+        if (le16(f, 26) != 1) throw std::runtime_error("bad BMP");
+        bpp = le16(f, 28);
+        comp = le32(f, 30);
+    }
+    if (comp == 1 || comp == 2) throw std::runtime_error("run-length BMP is not supported");
+    if (comp > 3) throw std::runtime_error("compressed BMP is not supported");
+    if (comp == 3 && bpp != 16 && bpp != 32) throw std::runtime_error("bad BMP");
+    if (bpp != 1 && bpp != 4 && bpp != 8 && bpp != 16 && bpp != 24 && bpp != 32)
+        throw std::runtime_error("BMP bit depth " + std::to_string(bpp) + " is not supported");
     const bool top_down = hs < 0;
-    const int64_t h = top_down ? -int64_t(hs) : hs;
+    const int64_t h = top_down ? -hs : hs;
     check_size(w, h);
-    uint32_t masks[4] = {0x00ff0000u, 0x0000ff00u, 0x000000ffu, 0u};  // R, G, B, A of BI_RGB 32-bit
-    if (comp == 3) {
-        if (bpp != 32) throw std::runtime_error("BMP bit fields other than 32-bit are not supported");
-        const size_t mo = hdr >= 52 ? 54 : 14 + hdr;  // masks inside the header, or right after it
-        for (int i = 0; i < (hdr >= 56 ? 4 : 3); i++) masks[i] = le32(f, mo + 4 * i);
-    } else if (comp != 0) {
-        throw std::runtime_error("compressed BMP is not supported");
-    }
-    if (bpp != 8 && bpp != 24 && bpp != 32) throw std::runtime_error("BMP bit depth " + std::to_string(bpp) + " is not supported");
-    std::vector<unsigned char> pal;
-    if (bpp == 8) {
-        uint32_t ncol = le32(f, 46);
-        if (ncol == 0 || ncol > 256) ncol = 256;
-        const size_t po = 14 + hdr;
-        if (po + 4 * size_t(ncol) > f.size()) throw std::runtime_error("truncated");
-        pal.assign(f.begin() + po, f.begin() + po + 4 * ncol);  // B, G, R, reserved
-    }
-    const int sh[4] = {mask_shift(masks[0]), mask_shift(masks[1]), mask_shift(masks[2]), mask_shift(masks[3])};
-    const size_t stride = (size_t(w) * bpp / 8 + 3) & ~size_t(3);
-    if (data_off + stride * size_t(h) > f.size()) throw std::runtime_error("truncated");
-    InputImage img;
-    img.width = w;
-    img.height = int(h);
-    img.data.resize(size_t(w) * h * 4);
-    for (int64_t y = 0; y < h; y++) {
-        const unsigned char *row = f.data() + data_off + stride * size_t(top_down ? y : h - 1 - y);
-        unsigned char *o = img.data.data() + size_t(y) * w * 4;
-        for (int32_t x = 0; x < w; x++, o += 4) {
-            if (bpp == 8) {
-                const size_t i = size_t(row[x]) * 4;
-                if (i + 3 > pal.size()) throw std::runtime_error("BMP palette index out of range");
-                o[0] = pal[i + 2], o[1] = pal[i + 1], o[2] = pal[i], o[3] = 255;
-            } else if (bpp == 24) {
-                o[0] = row[3 * x + 2], o[1] = row[3 * x + 1], o[2] = row[3 * x], o[3] = 255;
-            } else {
-                const uint32_t v = uint32_t(row[4 * x]) | uint32_t(row[4 * x + 1]) << 8 | uint32_t(row[4 * x + 2]) << 16 |
-                                   uint32_t(row[4 * x + 3]) << 24;
-                for (int c = 0; c < 3; c++) o[c] = sh[c] < 0 ? 0 : (v >> sh[c]) & 0xffu;
-                o[3] = sh[3] < 0 ? 255 : (v >> sh[3]) & 0xffu;
+    // channel masks R, G, B, A; BI_RGB 32-bit pixels carry an alpha byte that counts only if some
+    // pixel's alpha is not 0
+    uint32_t m[4] = {0, 0, 0, 0};
+    bool alpha_if_any = false;
+    auto default_masks = [&]() {
+        if (bpp == 16) {
+            m[0] = 31u << 10, m[1] = 31u << 5, m[2] = 31u;
+        } else if (bpp == 32) {
+            m[0] = 0xffu << 16, m[1] = 0xffu << 8, m[2] = 0xffu, m[3] = 0xffu << 24;
+            alpha_if_any = true;
+        } else {
+            m[0] = m[1] = m[2] = m[3] = 0;
+        }
+    };
+    if (hsz == 40 || hsz == 56) {
+        if (bpp == 16 || bpp == 32) {
+            if (comp == 0) {
+                default_masks();
+            } else {  // R, G, B masks after the header
+                for (int i = 0; i < 3; i++) m[i] = le32(f, 14 + hsz + 4 * i);
+                if (m[0] == m[1] && m[1] == m[2]) throw std::runtime_error("bad BMP");
             }
         }
+    } else if (hsz >= 108) {  // R, G, B, A masks in the header; BI_RGB replaces them by the defaults
+        for (int i = 0; i < 4; i++) m[i] = le32(f, 54 + 4 * i);
+        if (comp != 3) default_masks();
     }
+    InputImage img;
+    img.width = int(w);
+    img.height = int(h);
+    img.data.resize(size_t(w) * h * 4);
+    const size_t row_bytes = (size_t(w) * bpp + 7) / 8, stride = (row_bytes + 3) & ~size_t(3);
+    if (size_t(data_off) + stride * size_t(h) > f.size()) throw std::runtime_error("truncated");
+    auto row_of = [&](int64_t y) { return f.data() + data_off + stride * size_t(top_down ? y : h - 1 - y); };
+    if (bpp <= 8) {
+        const size_t esz = hsz == 12 ? 3 : 4, pal_off = 14 + hsz;
+        const size_t nent = data_off > pal_off ? (data_off - pal_off) / esz : 0;
+        if (nent == 0 || nent > 256) throw std::runtime_error("bad BMP palette");
+        for (int64_t y = 0; y < h; y++) {
+            const unsigned char *row = row_of(y);
+            unsigned char *o = img.data.data() + size_t(y) * w * 4;
+            for (int64_t x = 0; x < w; x++, o += 4) {
+                unsigned idx;
+                if (bpp == 8) idx = row[x];
+                else if (bpp == 4) idx = x & 1 ? row[x >> 1] & 15u : row[x >> 1] >> 4;
+                else idx = row[x >> 3] >> (7 - (x & 7)) & 1u;
+                if (idx < nent) {
+                    const unsigned char *e = &f[pal_off + idx * esz];  // B, G, R
+                    o[0] = e[2], o[1] = e[1], o[2] = e[0];
+                } else {
+                    o[0] = o[1] = o[2] = 0;
+                }
+                o[3] = 255;
+            }
+        }
+        return img;
+    }
+    const bool plain32 = bpp == 32 && m[0] == 0xff0000u && m[1] == 0xff00u && m[2] == 0xffu && m[3] == 0xff000000u;
+    if (bpp != 24 && !plain32) {
+        if (!m[0] || !m[1] || !m[2]) throw std::runtime_error("bad BMP channel masks");
+        for (uint32_t mk : m) {
+            int bits = 0;
+            for (uint32_t t = mk; t; t &= t - 1) bits++;
+            if (bits > 8) throw std::runtime_error("BMP channel masks wider than 8 bits are not supported");
+        }
+    }
+    const BmpField fr(m[0]), fg(m[1]), fb(m[2]), fa(m[3]);
+    unsigned alpha_or = 0;
+    for (int64_t y = 0; y < h; y++) {
+        const unsigned char *row = row_of(y);
+        unsigned char *o = img.data.data() + size_t(y) * w * 4;
+        for (int64_t x = 0; x < w; x++, o += 4) {
+            if (bpp == 24) {
+                o[0] = row[3 * x + 2], o[1] = row[3 * x + 1], o[2] = row[3 * x], o[3] = 255;
+                continue;
+            }
+            const unsigned char *p = row + (bpp == 16 ? 2 : 4) * x;
+            const uint32_t v = bpp == 16 ? uint32_t(p[0]) | uint32_t(p[1]) << 8
+                                         : uint32_t(p[0]) | uint32_t(p[1]) << 8 | uint32_t(p[2]) << 16 | uint32_t(p[3]) << 24;
+            o[0] = (unsigned char)fr(v), o[1] = (unsigned char)fg(v), o[2] = (unsigned char)fb(v);
+            o[3] = m[3] ? (unsigned char)fa(v) : 255;
+            alpha_or |= o[3];
+        }
+    }
+    if (alpha_if_any && alpha_or == 0)
+        for (size_t i = 3; i < img.data.size(); i += 4) img.data[i] = 255;
     return img;
 }
 
+// TGA as stb_image reads it: types 1, 2, 3 and their run-length forms 9, 10, 11.  True colour of 15
+// or 16 bits (5-5-5, each channel widened as v * 255 / 31, no alpha), 24 or 32 bits (B, G, R, A);
+// grey of 8 bits, or 16 (grey and alpha); colour-mapped pixels of 8 or 16-bit indices into a map of
+// 8-bit grey, 15/16, 24 or 32-bit entries, read after skipping as many bytes as the map's first-entry
+// field holds, an index beyond the map taking entry 0.  Only the top-left-origin bit of the
+// descriptor counts (rows are never mirrored left to right).
 InputImage decode_tga(const std::vector<unsigned char> &f) {
     if (f.size() < 18) throw std::runtime_error("not a TGA file");
     const unsigned id_len = f[0], cmap_type = f[1], type = f[2];
@@ -119,31 +220,48 @@ InputImage decode_tga(const std::vector<unsigned char> &f) {
     if (base < 1 || base > 3 || (type > 3 && type < 9) || type > 11) throw std::runtime_error("not a TGA file");
     check_size(w, h);
     const bool mapped = base == 1, grey = base == 3;
-    if (mapped ? (bpp != 8 || cmap_type != 1 || (cmap_bits != 24 && cmap_bits != 32)) :
-                 grey ? bpp != 8 : (bpp != 24 && bpp != 32))
+    auto depth_ok = [](unsigned b) { return b == 8 || b == 15 || b == 16 || b == 24 || b == 32; };
+    if (mapped ? (cmap_type != 1 || (bpp != 8 && bpp != 16) || !depth_ok(cmap_bits) || cmap_len == 0)
+               : grey ? (bpp != 8 && bpp != 16) : !depth_ok(bpp))
         throw std::runtime_error("TGA pixel depth " + std::to_string(bpp) + " is not supported");
+    // one pixel (or map entry) of `bits` bits to RGBA; `as_grey`: 8 bits grey, 16 bits grey + alpha
+    auto to_rgba = [](const unsigned char *p, unsigned bits, bool as_grey, unsigned char *o) {
+        if (bits == 8 || (as_grey && bits == 16)) {
+            o[0] = o[1] = o[2] = p[0];
+            o[3] = bits == 16 ? p[1] : 255;
+        } else if (bits == 15 || bits == 16) {
+            const unsigned v = unsigned(p[0]) | unsigned(p[1]) << 8;
+            o[0] = (unsigned char)(((v >> 10) & 31u) * 255 / 31);
+            o[1] = (unsigned char)(((v >> 5) & 31u) * 255 / 31);
+            o[2] = (unsigned char)((v & 31u) * 255 / 31);
+            o[3] = 255;
+        } else {
+            o[0] = p[2], o[1] = p[1], o[2] = p[0], o[3] = bits == 32 ? p[3] : 255;
+        }
+    };
     size_t pos = 18 + id_len;
-    std::vector<unsigned char> cmap;
-    if (cmap_type == 1) {
-        const size_t bytes = size_t(cmap_len) * ((cmap_bits + 7) / 8);
-        if (pos + bytes > f.size()) throw std::runtime_error("truncated");
-        if (mapped) cmap.assign(f.begin() + pos, f.begin() + pos + bytes);
-        pos += bytes;
+    std::vector<unsigned char> cmap;  // RGBA per entry
+    if (mapped) {
+        pos += cmap_first;
+        const unsigned eb = (cmap_bits + 7) / 8;
+        if (pos + size_t(cmap_len) * eb > f.size()) throw std::runtime_error("truncated");
+        cmap.resize(size_t(cmap_len) * 4);
+        for (uint32_t i = 0; i < cmap_len; i++) to_rgba(&f[pos + size_t(i) * eb], cmap_bits, false, &cmap[4 * i]);
+        pos += size_t(cmap_len) * eb;
+    } else if (cmap_type == 1) {  // a colour map on an unmapped image is skipped
+        pos += size_t(cmap_len) * ((cmap_bits + 7) / 8);
     }
-    const unsigned pb = bpp / 8, cb = cmap_bits / 8;
+    const unsigned pb = (bpp + 7) / 8;
     // decode to RGBA in file order (rows bottom-up unless descriptor bit 5 marks a top-left origin)
     std::vector<unsigned char> px(size_t(w) * h * 4);
     auto put = [&](size_t i, const unsigned char *p) {
         unsigned char *o = &px[4 * i];
         if (mapped) {
-            const uint32_t idx = p[0];
-            if (idx < cmap_first || idx - cmap_first >= cmap_len) throw std::runtime_error("TGA colour index out of range");
-            const unsigned char *e = &cmap[size_t(idx - cmap_first) * cb];
-            o[0] = e[2], o[1] = e[1], o[2] = e[0], o[3] = cb == 4 ? e[3] : 255;
-        } else if (grey) {
-            o[0] = o[1] = o[2] = p[0], o[3] = 255;
+            uint32_t idx = pb == 1 ? p[0] : uint32_t(p[0]) | uint32_t(p[1]) << 8;
+            if (idx >= cmap_len) idx = 0;
+            std::memcpy(o, &cmap[4 * size_t(idx)], 4);
         } else {
-            o[0] = p[2], o[1] = p[1], o[2] = p[0], o[3] = pb == 4 ? p[3] : 255;
+            to_rgba(p, bpp, grey, o);
         }
     };
     const size_t n = size_t(w) * h;
@@ -155,8 +273,8 @@ InputImage decode_tga(const std::vector<unsigned char> &f) {
             continue;
         }
         if (pos >= f.size()) throw std::runtime_error("truncated");
-        const unsigned head = f[pos++], count = (head & 0x7f) + 1;
-        if (i + count > n) throw std::runtime_error("TGA run past the image");
+        const unsigned head = f[pos++];
+        const unsigned count = unsigned(std::min<size_t>((head & 0x7f) + 1, n - i));  // a run ends with the image
         if (head & 0x80) {  // one pixel repeated
             if (pos + pb > f.size()) throw std::runtime_error("truncated");
             for (unsigned k = 0; k < count; k++) put(i++, &f[pos]);
@@ -170,12 +288,9 @@ InputImage decode_tga(const std::vector<unsigned char> &f) {
     img.width = w;
     img.height = h;
     img.data.resize(n * 4);
-    const bool top_left = desc & 0x20, right_left = desc & 0x10;
+    const bool top_left = desc & 0x20;
     for (int32_t y = 0; y < h; y++)
-        for (int32_t x = 0; x < w; x++) {
-            const size_t src = size_t(top_left ? y : h - 1 - y) * w + (right_left ? w - 1 - x : x);
-            for (int c = 0; c < 4; c++) img.data[(size_t(y) * w + x) * 4 + c] = px[src * 4 + c];
-        }
+        std::memcpy(&img.data[size_t(y) * w * 4], &px[size_t(top_left ? y : h - 1 - y) * w * 4], size_t(w) * 4);
     return img;
 }
 

@@ -527,3 +527,202 @@ def test_pic_decoder(png_check, tmp_path, codings):
     if len(codings) == 1:
         want[..., 3] = 255  # no packet carries alpha
     assert np.array_equal(decode(png_check, path), want)
+
+
+# ---- BMP and TGA layouts beyond what PIL writes: files built here, expected pixels from the rules
+# stb_image applies (bit-field channels widened by repeating their bits, 15/16-bit TGA channels as
+# v * 255 / 31, TGA colour maps read after skipping the first-entry field's bytes).
+
+def _bmp(w, h, bpp, pixels_rows, hsz=40, comp=0, masks=None, palette=None, top_down=False):
+    """A BMP file: rows given top to bottom as bytes (unpadded); stored bottom-up unless top_down."""
+    stride = ((w * bpp + 7) // 8 + 3) & ~3
+    rows = [r + b"\0" * (stride - len(r)) for r in pixels_rows]
+    data = b"".join(rows if top_down else rows[::-1])
+    pal = b""
+    if palette is not None:
+        pal = b"".join(bytes([b, g, r]) + (b"" if hsz == 12 else b"\0") for r, g, b in palette)
+    extra = b""
+    if hsz == 12:
+        info = struct.pack("<IHHHH", 12, w, h, 1, bpp)
+    else:
+        info = struct.pack("<IiiHHIIiiII", hsz, w, -h if top_down else h, 1, bpp, comp, len(data), 2835, 2835, 0, 0)
+        if hsz >= 108:
+            m = list(masks or (0, 0, 0, 0))
+            info += struct.pack("<IIII", *m) + b"\0" * (hsz - 56)
+        elif masks is not None and comp == 3:
+            extra = struct.pack("<III", *masks[:3])
+    off = 14 + len(info) + len(extra) + len(pal)
+    return b"BM" + struct.pack("<IHHI", off + len(data), 0, 0, off) + info + extra + pal + data
+
+
+def _widen(v, n):
+    r, have = 0, 0
+    while have < 8:
+        r, have = (r << n) | v, have + n
+    return (r >> (have - 8)) & 0xff
+
+
+def _field(v, mask):
+    lo = (mask & -mask).bit_length() - 1
+    n = bin(mask).count("1")
+    return _widen((v & mask) >> lo, n)
+
+
+def test_bmp_1_bit_matches_pil(png_check, tmp_path):
+    from PIL import Image
+    arr = (np.random.default_rng(3).random((13, 21)) > 0.5).astype(np.uint8) * 255
+    path = str(tmp_path / "b1.bmp")
+    Image.fromarray(arr).convert("1").save(path)
+    got = decode(png_check, path)
+    assert np.array_equal(got[..., :3], np.asarray(Image.open(path).convert("RGB")))
+    assert (got[..., 3] == 255).all()
+
+
+@pytest.mark.parametrize("hsz", [12, 40, 124])
+@pytest.mark.parametrize("bpp", [4, 8])
+def test_bmp_palettes_and_headers(png_check, tmp_path, hsz, bpp):
+    rng = np.random.default_rng(hsz + bpp)
+    w, h, ncol = 11, 7, (16 if bpp == 4 else 200)
+    pal = [tuple(int(x) for x in rng.integers(0, 256, 3)) for _ in range(ncol)]
+    idx = rng.integers(0, ncol, (h, w))
+    rows = []
+    for y in range(h):
+        if bpp == 8:
+            rows.append(bytes(int(i) for i in idx[y]))
+        else:
+            v = list(idx[y]) + [0]
+            rows.append(bytes((int(v[2 * k]) << 4) | int(v[2 * k + 1]) for k in range((w + 1) // 2)))
+    path = tmp_path / "p.bmp"
+    path.write_bytes(_bmp(w, h, bpp, rows, hsz=hsz, palette=pal))
+    got = decode(png_check, str(path))
+    want = np.array(pal, np.uint8)[idx]
+    assert np.array_equal(got[..., :3], want) and (got[..., 3] == 255).all()
+
+
+def test_bmp_index_past_palette_reads_black(png_check, tmp_path):
+    rows = [bytes([0, 1, 5])]
+    path = tmp_path / "i.bmp"
+    path.write_bytes(_bmp(3, 1, 8, rows, palette=[(10, 20, 30), (40, 50, 60)]))
+    got = decode(png_check, str(path))
+    assert got[0, :, :3].tolist() == [[10, 20, 30], [40, 50, 60], [0, 0, 0]]
+
+
+@pytest.mark.parametrize("masks", [None, (0xF800, 0x07E0, 0x001F), (0x7C00, 0x03E0, 0x001F), (0x0F00, 0x00F0, 0x000F)])
+@pytest.mark.parametrize("top_down", [False, True])
+def test_bmp_16_bit(png_check, tmp_path, masks, top_down):
+    rng = np.random.default_rng(16)
+    w, h = 9, 5
+    px = rng.integers(0, 1 << 16, (h, w))
+    rows = [b"".join(struct.pack("<H", int(v)) for v in px[y]) for y in range(h)]
+    path = tmp_path / "s.bmp"
+    path.write_bytes(_bmp(w, h, 16, rows, comp=3 if masks else 0, masks=masks, top_down=top_down))
+    got = decode(png_check, str(path))
+    m = masks or (0x7C00, 0x03E0, 0x001F)
+    want = np.array([[[_field(int(v), m[c]) for c in range(3)] for v in row] for row in px], np.uint8)
+    assert np.array_equal(got[..., :3], want) and (got[..., 3] == 255).all()
+
+
+@pytest.mark.parametrize("alpha", ["zero", "mixed"])
+def test_bmp_32_bit_alpha_rule(png_check, tmp_path, alpha):
+    rng = np.random.default_rng(32)
+    w, h = 6, 4
+    bgra = rng.integers(0, 256, (h, w, 4), dtype=np.uint8)
+    if alpha == "zero":
+        bgra[..., 3] = 0
+    path = tmp_path / "a.bmp"
+    path.write_bytes(_bmp(w, h, 32, [bgra[y].tobytes() for y in range(h)]))
+    got = decode(png_check, str(path))
+    assert np.array_equal(got[..., :3], bgra[..., 2::-1])
+    assert np.array_equal(got[..., 3], np.full((h, w), 255, np.uint8) if alpha == "zero" else bgra[..., 3])
+
+
+def test_bmp_v5_bitfields_with_alpha(png_check, tmp_path):
+    rng = np.random.default_rng(5)
+    w, h = 5, 3
+    masks = (0x0000FF00, 0x00FF0000, 0xFF000000, 0x000000FF)  # R, G, B, A
+    px = rng.integers(0, 1 << 32, (h, w), dtype=np.uint64)
+    rows = [b"".join(struct.pack("<I", int(v)) for v in px[y]) for y in range(h)]
+    path = tmp_path / "v5.bmp"
+    path.write_bytes(_bmp(w, h, 32, rows, hsz=124, comp=3, masks=masks))
+    got = decode(png_check, str(path))
+    want = np.array([[[_field(int(v), masks[c]) for c in range(4)] for v in row] for row in px], np.uint8)
+    assert np.array_equal(got, want)
+
+
+def test_bmp_run_length_is_refused(png_check, tmp_path):
+    path = tmp_path / "r.bmp"
+    data = bytearray(_bmp(2, 2, 8, [b"\0\0", b"\0\0"], palette=[(0, 0, 0)]))
+    data[30:34] = struct.pack("<I", 1)  # BI_RLE8
+    path.write_bytes(bytes(data))
+    assert subprocess.run([png_check, str(path)], capture_output=True).returncode != 0
+
+
+def _tga(w, h, img_type, bpp, body, desc=0, cmap=None, cmap_first=0, cmap_bits=0, skip=b""):
+    cmap_len = 0 if cmap is None else len(cmap) // ((cmap_bits + 7) // 8)
+    head = struct.pack("<BBBHHBHHHHBB", 0, 1 if cmap is not None else 0, img_type, cmap_first, cmap_len, cmap_bits,
+                       0, 0, w, h, bpp, desc)
+    return head + skip + (cmap or b"") + body
+
+
+def _rgb16(v):
+    return [((v >> 10) & 31) * 255 // 31, ((v >> 5) & 31) * 255 // 31, (v & 31) * 255 // 31]
+
+
+@pytest.mark.parametrize("bpp", [15, 16])
+def test_tga_16_bit_true_colour(png_check, tmp_path, bpp):
+    rng = np.random.default_rng(bpp)
+    w, h = 7, 3
+    px = rng.integers(0, 1 << 16, (h, w))
+    body = b"".join(struct.pack("<H", int(v)) for v in px[::-1].ravel())  # bottom-up
+    path = tmp_path / "t16.tga"
+    path.write_bytes(_tga(w, h, 2, bpp, body))
+    got = decode(png_check, str(path))
+    want = np.array([[_rgb16(int(v)) for v in row] for row in px], np.uint8)
+    assert np.array_equal(got[..., :3], want) and (got[..., 3] == 255).all()
+
+
+def test_tga_grey_with_alpha(png_check, tmp_path):
+    w, h = 4, 2
+    ga = np.arange(w * h * 2, dtype=np.uint8).reshape(h, w, 2) * 7
+    path = tmp_path / "ga.tga"
+    path.write_bytes(_tga(w, h, 3, 16, ga[::-1].tobytes()))
+    got = decode(png_check, str(path))
+    assert np.array_equal(got[..., 0], ga[..., 0]) and np.array_equal(got[..., 2], ga[..., 0])
+    assert np.array_equal(got[..., 3], ga[..., 1])
+
+
+@pytest.mark.parametrize("cmap_bits,index_bits", [(16, 8), (24, 16), (32, 8), (8, 8)])
+def test_tga_colour_maps(png_check, tmp_path, cmap_bits, index_bits):
+    rng = np.random.default_rng(cmap_bits + index_bits)
+    w, h, n = 6, 3, 40
+    eb = (cmap_bits + 7) // 8
+    cmap = rng.integers(0, 256, n * eb, dtype=np.uint8).tobytes()
+    idx = rng.integers(0, n + 5, (h, w))  # indices past the map take entry 0
+    body = b"".join((struct.pack("<H", int(i)) if index_bits == 16 else bytes([int(i)])) for i in idx[::-1].ravel())
+    path = tmp_path / "cm.tga"
+    path.write_bytes(_tga(w, h, 1, index_bits, body, cmap=cmap, cmap_bits=cmap_bits, cmap_first=3, skip=b"\x11" * 3))
+
+    def entry(i):
+        i = i if i < n else 0
+        e = cmap[i * eb:(i + 1) * eb]
+        if cmap_bits == 8:
+            return [e[0]] * 3 + [255]
+        if cmap_bits == 16:
+            return _rgb16(e[0] | e[1] << 8) + [255]
+        return [e[2], e[1], e[0], e[3] if cmap_bits == 32 else 255]
+    want = np.array([[entry(int(i)) for i in row] for row in idx], np.uint8)
+    got = decode(png_check, str(path))
+    assert np.array_equal(got, want)
+
+
+def test_tga_right_to_left_bit_is_ignored_and_runs_end_with_the_image(png_check, tmp_path):
+    w, h = 3, 2
+    px = np.arange(w * h * 3, dtype=np.uint8).reshape(h, w, 3)
+    body = px[::-1, :, ::-1].tobytes()  # bottom-up BGR
+    path = tmp_path / "rl.tga"
+    path.write_bytes(_tga(w, h, 2, 24, body, desc=0x10))
+    assert np.array_equal(decode(png_check, str(path))[..., :3], px)
+    # a run-length packet of 128 repeats covers the 6 pixels and ends with the image
+    path.write_bytes(_tga(w, h, 10, 24, bytes([0xFF, 1, 2, 3])))
+    got = decode(png_check, str(path))
+    assert (got[..., :3] == np.array([3, 2, 1], np.uint8)).all()
