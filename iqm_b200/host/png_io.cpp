@@ -168,14 +168,17 @@ InputImage decode_png(const std::vector<unsigned char> &f) {
 }
 
 InputImage decode_pnm(const std::vector<unsigned char> &f) {
-    // binary P5 (grey) / P6 (RGB), maxval <= 255
+    // binary P5 (grey) / P6 (RGB) as stb_image reads them: samples taken as they are (no rescaling
+    // by maxval); for maxval > 255 two bytes a sample, of which the loader keeps the second (it reads
+    // the big-endian samples into host-order 16-bit words and keeps their high byte); comments run
+    // to the end of the line (LF or CR)
     size_t pos = 0;
     auto token = [&]() -> std::string {
         std::string t;
         while (pos < f.size()) {
             const char c = char(f[pos]);
             if (c == '#') {
-                while (pos < f.size() && f[pos] != '\n') pos++;
+                while (pos < f.size() && f[pos] != '\n' && f[pos] != '\r') pos++;
             } else if (std::isspace((unsigned char)c)) {
                 if (!t.empty()) break;
                 pos++;
@@ -190,12 +193,13 @@ InputImage decode_pnm(const std::vector<unsigned char> &f) {
     if (magic != "P5" && magic != "P6") throw std::runtime_error("unsupported PNM type");
     const int w = std::stoi(token()), h = std::stoi(token()), maxv = std::stoi(token());
     pos++;  // the single whitespace after maxval
-    if (w <= 0 || h <= 0 || maxv <= 0 || maxv > 255) throw std::runtime_error("unsupported PNM header");
-    const int ch = magic == "P5" ? 1 : 3;
-    if (f.size() < pos + size_t(w) * h * ch) throw std::runtime_error("truncated PNM");
+    if (w <= 0 || h <= 0 || maxv < 0 || maxv > 65535) throw std::runtime_error("unsupported PNM header");
+    if (int64_t(w) * h >= (int64_t(1) << 31)) throw std::runtime_error("image size out of range");
+    const int ch = magic == "P5" ? 1 : 3, bytes = maxv > 255 ? 2 : 1;
+    if (f.size() < pos + size_t(w) * h * ch * bytes) throw std::runtime_error("truncated PNM");
     InputImage img{w, h, std::vector<unsigned char>(size_t(w) * h * 4)};
     for (size_t i = 0; i < size_t(w) * h; i++) {
-        for (int c = 0; c < 3; c++) img.data[i * 4 + c] = f[pos + i * ch + (ch == 3 ? c : 0)];
+        for (int c = 0; c < 3; c++) img.data[i * 4 + c] = f[pos + (i * ch + (ch == 3 ? c : 0)) * bytes + bytes - 1];
         img.data[i * 4 + 3] = 255;
     }
     return img;

@@ -726,3 +726,22 @@ def test_tga_right_to_left_bit_is_ignored_and_runs_end_with_the_image(png_check,
     path.write_bytes(_tga(w, h, 10, 24, bytes([0xFF, 1, 2, 3])))
     got = decode(png_check, str(path))
     assert (got[..., :3] == np.array([3, 2, 1], np.uint8)).all()
+
+
+@pytest.mark.parametrize("magic,ch", [(b"P5", 1), (b"P6", 3)])
+def test_pnm_16_bit_and_small_maxval(png_check, tmp_path, magic, ch):
+    """maxval > 255: two bytes a sample, the loader keeps the second; maxval < 255: samples as they
+    are, not rescaled; comments end at CR or LF."""
+    rng = np.random.default_rng(ch)
+    w, h = 5, 4
+    s16 = rng.integers(0, 65536, (h, w, ch)).astype(">u2")
+    path = tmp_path / "d.pnm"
+    path.write_bytes(magic + b"\n# made here\r%d %d\n65535\n" % (w, h) + s16.tobytes())
+    got = decode(png_check, str(path))
+    low = (s16.astype(np.uint32) & 0xFF).astype(np.uint8)
+    want = np.repeat(low, 3, axis=2) if ch == 1 else low
+    assert np.array_equal(got[..., :3], want) and (got[..., 3] == 255).all()
+    s8 = rng.integers(0, 16, (h, w, ch), dtype=np.uint8)
+    path.write_bytes(magic + b" %d %d 15\n" % (w, h) + s8.tobytes())
+    got = decode(png_check, str(path))
+    assert np.array_equal(got[..., :3], np.repeat(s8, 3, axis=2) if ch == 1 else s8)
