@@ -2,9 +2,9 @@
 // sequential DCT with Huffman coding, 8-bit samples; JFIF colour).  Output is RGBA8 like the
 // reference's stbi_load(..., 4) (src/main.cpp:37-57).  A lossy format decodes to slightly different
 // bytes in different decoders (IDCT arithmetic, chroma upsampling, colour rounding): this one uses a
-// separable floating-point IDCT, the triangle ("fancy") filter for 2x horizontal and vertical
-// chroma upsampling (replication for other factors) and the JFIF YCbCr->RGB equations, which keeps
-// it within a few levels of other decoders.  Progressive files (T.81 Annex G: spectral selection
+// separable floating-point IDCT, the reference loader's integer triangle filters for 2x chroma
+// upsampling (including its edge rule; the nearest sample for other factors) and the JFIF
+// YCbCr->RGB equations, which keeps it within a few levels of the reference's loader.  Progressive files (T.81 Annex G: spectral selection
 // and successive approximation, Huffman coded) keep every block's coefficients across their scans
 // and are transformed after the last one.  Arithmetic-coded and lossless files, 12-bit samples and
 // 4-component (CMYK) images are refused with a reason.
@@ -415,19 +415,36 @@ InputImage decode_jpeg(const std::vector<unsigned char> &f) {
     img.width = width;
     img.height = height;
     img.data.resize(size_t(width) * height * 4);
-    // component sample at full resolution: triangle filter for factor 2, replication otherwise
+    // Component sample at full resolution, as the reference's loader upsamples chroma (integer
+    // triangle filters, each output rounded to a byte):
+    //   2x across:       (3 a + b + 2) >> 2 with b the neighbour on the output's side; the row's
+    //                    first output is a[0], its last a[w-1], and the output before the last
+    //                    weighs the second-to-last sample by 3 -- the loader's own edge rule;
+    //   2x down:         (3 near + far + 2) >> 2 with the neighbouring row (clamped) as far;
+    //   2x both ways:    t = 3 near + far per column, then (3 t + t' + 8) >> 4 with the neighbouring
+    //                    column's t', and (t + 2) >> 2 at the row's first and last output;
+    //   other factors:   the nearest sample.
     auto sample = [&](const Component &c, int x, int y) -> float {
         const int fx = hmax / c.h, fy = vmax / c.v, stride = c.bw * 8;
         const int pw = (width * c.h + hmax - 1) / hmax, ph = (height * c.v + vmax - 1) / vmax;  // real extent
         auto at = [&](int xx, int yy) {
-            return float(c.plane[size_t(std::clamp(yy, 0, ph - 1)) * stride + std::clamp(xx, 0, pw - 1)]);
+            return int(c.plane[size_t(std::clamp(yy, 0, ph - 1)) * stride + std::clamp(xx, 0, pw - 1)]);
         };
         const int cx = x / fx, cy = y / fy;
-        if (fx == 1 && fy == 1) return at(cx, cy);
-        const int nx = fx == 2 ? ((x & 1) ? cx + 1 : cx - 1) : cx;  // nearer neighbour along x
-        const int ny = fy == 2 ? ((y & 1) ? cy + 1 : cy - 1) : cy;
-        const float wx = fx == 2 ? 0.75f : 1.f, wy = fy == 2 ? 0.75f : 1.f;
-        return wy * (wx * at(cx, cy) + (1 - wx) * at(nx, cy)) + (1 - wy) * (wx * at(cx, ny) + (1 - wx) * at(nx, ny));
+        if (fy == 2 && fx <= 2) {
+            const int far_row = (y & 1) ? cy + 1 : cy - 1;  // clamped by at()
+            auto t = [&](int xx) { return 3 * at(xx, cy) + at(xx, far_row); };
+            if (fx == 1) return float((t(cx) + 2) >> 2);
+            if (pw == 1 || x == 0 || x == 2 * pw - 1) return float((t(cx) + 2) >> 2);
+            return float((x & 1) ? (3 * t(cx) + t(cx + 1) + 8) >> 4 : (3 * t(cx) + t(cx - 1) + 8) >> 4);
+        }
+        if (fx == 2 && fy == 1) {
+            if (pw == 1 || x == 0) return float(at(cx, cy));
+            if (x & 1) return float(cx == pw - 1 ? at(cx, cy) : (3 * at(cx, cy) + at(cx + 1, cy) + 2) >> 2);
+            if (cx == pw - 1) return float((3 * at(cx - 1, cy) + at(cx, cy) + 2) >> 2);
+            return float((3 * at(cx, cy) + at(cx - 1, cy) + 2) >> 2);
+        }
+        return float(at(cx, cy));
     };
     for (int y = 0; y < height; y++)
         for (int x = 0; x < width; x++) {

@@ -111,7 +111,9 @@ def test_tga_decoder_matches_pil(png_check, tmp_path, mode, rle, origin):
 @pytest.mark.parametrize("size", [(48, 64), (37, 53)])
 def test_jpeg_decoder_close_to_pil(png_check, tmp_path, subsampling, size):
     """Baseline JPEG (4:4:4, 4:2:2, 4:2:0; odd sizes): a lossy format decodes to slightly different
-    bytes in different decoders, so the bound is a few levels per channel."""
+    bytes in different decoders, so the bound is a few levels per channel.  With 4:2:2 the column
+    before the last chroma pair's second output follows the reference loader's edge rule, not PIL's
+    filter, and is left out here (tests/test_loader_vs_reference.py holds it to the loader)."""
     from PIL import Image
     from iqm_b200 import synth
     h, w = size
@@ -120,6 +122,10 @@ def test_jpeg_decoder_close_to_pil(png_check, tmp_path, subsampling, size):
     Image.fromarray(a[..., :3]).save(path, quality=90, subsampling=subsampling)
     got = decode(png_check, path)[..., :3].astype(int)
     want = np.asarray(Image.open(path).convert("RGB")).astype(int)
+    if subsampling == 1:
+        keep = np.ones(w, bool)
+        keep[2 * ((w + 1) // 2 - 1)] = False
+        got, want = got[:, keep], want[:, keep]
     d = np.abs(got - want)
     assert d.max() <= 4 and d.mean() <= 0.6, (d.max(), d.mean())
 
