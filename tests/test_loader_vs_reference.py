@@ -4,7 +4,7 @@ ref` builds that call from the reference's tree into oracle/_ref/ref_loader (tes
 never part of the product); these tests skip where the reference tree is absent.
 
 Lossless formats (PNG in every colour type, bit depth and interlace; PNM; BMP and TGA layouts;
-GIF; Radiance HDR) must decode to the same RGBA bytes, alpha included.  JPEG is lossy, and the
+GIF; Radiance HDR; PSD; Softimage PIC) must decode to the same RGBA bytes, alpha included.  JPEG is lossy, and the
 loader's integer IDCT and fixed-point colour conversion are its own: the bound there is 3 levels
 per channel and a mean below 0.15 (chroma upsampling, including the loader's 4:2:2 edge rule,
 follows the loader)."""
@@ -148,3 +148,37 @@ def test_jpeg_within_three_levels_of_the_loader(ref_loader, ours, tmp_path, subs
     Image.fromarray(noise(*size, 2)).save(p, quality=90, subsampling=subsampling, progressive=progressive)
     d = np.abs(run(ours, p).astype(int) - run(ref_loader, p).astype(int))
     assert d.max() <= 3 and d.mean() < 0.15, (d.max(), d.mean())
+
+
+def test_gif_hdr_psd_pic_layouts_decode_to_the_loaders_bytes(ref_loader, ours, tmp_path):
+    """The hand-built files of tests/test_cli.py: a GIF frame inside a larger screen with a
+    transparent index and a background entry; flat and run-length HDR scanlines; PSD with 3 to 5
+    channels, 8 and 16 bits, raw and PackBits (alpha un-premultiplied); PIC with raw, pure and mixed
+    run-length packets."""
+    import test_cli as t
+    rng = np.random.default_rng(11)
+    files = []
+    pal = [tuple(int(v) for v in rng.integers(0, 256, 3)) for _ in range(8)]
+    frame = rng.integers(0, 8, (5, 6)).astype(np.uint8)
+    files.append(("t.gif", t._gif(11, 9, pal, 2, frame, x0=3, y0=2, transparent=6)))
+    for w, rle in ((5, False), (40, True)):
+        rgbe = rng.integers(0, 256, (7, w, 4)).astype(np.uint8)
+        rgbe[..., 0] |= 0x80
+        rgbe[:, :w // 3, :] = rgbe[:, :1, :]
+        body = b"".join(t._hdr_rle_scanline(rgbe[y]) for y in range(7)) if rle else rgbe.tobytes()
+        files.append(("x%d.hdr" % w, b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n-Y 7 +X %d\n" % w + body))
+    for channels, depth, rle in [(3, 8, False), (3, 8, True), (4, 8, False), (4, 8, True), (3, 16, False),
+                                 (5, 16, False)]:
+        planes = rng.integers(0, 1 << depth, (channels, 9, 14)).astype(np.uint32)
+        planes[:, :, :5] = planes[:, :, :1]
+        files.append(("p%d%d%d.psd" % (channels, depth, rle), t._psd(planes, depth, rle)))
+    img = rng.integers(0, 256, (6, 150, 4)).astype(np.uint8)
+    img[:, 3:140] = img[:, 3:4]
+    for codings in [(0,), (1,), (2,), (2, 1)]:
+        packets = [(codings[0], 0xE0)] + ([(codings[1], 0x10)] if len(codings) > 1 else [])
+        rows = [b"".join(t._pic_encode_row(img[y], c, m) for c, m in packets) for y in range(6)]
+        files.append(("x%s.pic" % "".join(map(str, codings)), t._pic(150, 6, packets, rows)))
+    for name, data in files:
+        p = tmp_path / name
+        p.write_bytes(data)
+        assert np.array_equal(run(ours, str(p)), run(ref_loader, str(p))), name
